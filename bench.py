@@ -1,0 +1,337 @@
+"""Benchmark: zone-updates/s of the moving-mesh relativistic hydro step on B200.
+
+Workload (one GPU): 4096 independent planar relativistic shock tubes
+(cartesian + rel_cart, Gamma = 5/3, NUM_Q = 6, no regrid), each with a seeded
+cell count drawn log-uniformly from 256-8192, rho_L = 10 and p_L = 13.33 with
++-20 % jitter, rho_R = 1, p_R = 1e-7 and one initial velocity U(-0.5, 0.5)
+applied to both states.  A step is one RK3 step of every tube, each with its own
+dt, in one persistent launch.  Synthetic inputs stand in for the reference's
+problem setups; the state (~1.4 GB) is larger than L2, so every step streams it
+from HBM.
+
+Arms:
+  (default)          the CUDA path: `value` times steps on device-resident state;
+                     `e2e` times the C-ABI job from pinned host buffers (upload,
+                     steps, download).
+  --impl reference   the reference's own CPU implementation of the step
+                     (oracle/_ref, compiled from the reference sources; the C
+                     restatement if that build is absent) on a bounded sample of
+                     tubes, one process per host core.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NTUBES = 4096
+SEED = 20241203
+B_ZU_NQ6 = 8 * (8 * (6 + 1) + 1)  # algorithmic bytes per zone-update (456 for NUM_Q = 6)
+METRIC = "zone-updates/s on 1 B200: plain vs batched+learned c2p at L1<=1e-8; HBM % peak"
+
+
+def tube_setups(ntubes=NTUBES, seed=SEED):
+    from gamma_b200 import problems
+    rng = np.random.default_rng(seed)
+    n = np.floor(np.exp(rng.uniform(math.log(256), math.log(8192), ntubes))).astype(int)
+    jr = rng.uniform(-0.2, 0.2, ntubes)
+    jp = rng.uniform(-0.2, 0.2, ntubes)
+    v = rng.uniform(-0.5, 0.5, ntubes)
+    return [problems.TubeSetup(ncell=int(n[i]), rhoL=10. * (1. + jr[i]), pL=13.33 * (1. + jp[i]), vL=float(v[i]),
+                               vR=float(v[i]), rhoR=1.0, pR=1.e-7) for i in range(ntubes)]
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle-reason samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in self.rows for j in range(4) if r[3 + j].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_zone():
+    """DRAM bytes per zone-update of the step kernel from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["track_step_cart_dram_bytes_per_zone_update"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+# CPU arms (the reference's own code, or the restatement)
+
+def _cpu_worker(args):
+    kind, tubes, steps, warmup = args
+    sys.path.insert(0, ROOT)
+    zones = 0
+    t_total = 0.0
+    for t in tubes:
+        if kind == "reference":  # one process-wide Simu per library: re-initialised per tube
+            from oracle.refsim import RefSim
+            s = RefSim("tube")
+            s.set_params(**t)
+            s.init()
+        else:
+            from oracle import port
+            s = port.PortSim(port.tube_config(**t))
+            s.init()
+        s.step(warmup)
+        t0 = time.perf_counter()
+        s.step(steps)
+        t_total += time.perf_counter() - t0
+        zones += steps * int(t["ncell"])
+    return zones, t_total
+
+
+def cpu_run(setups, steps, warmup, sample, cores, budget_zones):
+    """Time the CPU step on a sample of tubes, one process per core; returns (zone-updates/s, info)."""
+    import multiprocessing as mp
+
+    kind = "reference" if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_tube.so")) else "port"
+    rng = np.random.default_rng(SEED + 1)
+    idx = rng.choice(len(setups), size=min(sample, len(setups)), replace=False)
+    tubes = []
+    for i in idx:
+        s = setups[i]
+        tubes.append(dict(ncell=s.ncell, nmax=s.ncell, rhoL=s.rhoL, pL=s.pL, vL=s.vL, vR=s.vR, rhoR=s.rhoR, pR=s.pR))
+    # bound the work: scale the step count so the sample is ~budget_zones zone-updates
+    zsum = sum(t["ncell"] for t in tubes)
+    steps = max(1, min(steps, int(budget_zones // max(zsum, 1))))
+    chunks = [tubes[k::cores] for k in range(cores)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_cpu_worker, [(kind, ch, steps, warmup) for ch in chunks if ch])
+    wall = time.perf_counter() - t0
+    zones = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    value = zones / busy
+    info = {"kind": kind, "cores": cores,
+            "sample": f"{len(tubes)} of the {len(setups)} tubes (seeded), {steps} timed RK3 steps each after "
+                      f"{warmup} warm-up steps, {cores} processes; value = sample zone-updates / slowest process"}
+    return value, info, wall
+
+
+# ---------------------------------------------------------------------------
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    setups = tube_setups()
+    cores = os.cpu_count() or 1
+    steps = max(1, args.steps)
+    value, info, wall = cpu_run(setups, steps, args.warmup, sample=max(64, cores * 2), cores=cores,
+                                budget_zones=float(os.environ.get("GAMMA_REF_ZONES", 4.0e7)))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "4096 cartesian relativistic shock tubes, 256-8192 cells (log-uniform), "
+                                   "Gamma=5/3, NUM_Q=6, one RK3 step per step", "tubes": NTUBES, "seed": SEED},
+            "cpu_baseline": dict(info, value=value, unit="zone-updates/s"),
+            "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_gpu_arm(args):
+    import torch
+
+    from gamma_b200 import gpu, problems
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    setups = tube_setups(args.ntubes)
+    states = [s.initial_state() for s in setups]
+    g = gpu.GammaGPU(gpu.config_cart(), [s.capacity for s in setups])
+    pk = problems.pack(states, g.offsets, g.total, 6)
+    zones_per_step = sum(s.ncell for s in setups)
+
+    # pinned host buffers for the end-to-end arm
+    host = {k: torch.from_numpy(np.ascontiguousarray(pk[k])).pin_memory() for k in ("prim", "x", "dx", "dt_loc", "xI")}
+    out_prim = torch.empty_like(host["prim"]).pin_memory()
+    h2d_bytes = sum(v.numel() * 8 for k, v in host.items()) - host["prim"].numel() * 8 // 6  # slot 3 is not sent
+    d2h_bytes = out_prim.numel() * 8 * 5 // 6
+
+    def upload():
+        g.upload_ptrs(pk["ntrack"], pk["t"], pk["it"], host["prim"].data_ptr(), host["x"].data_ptr(),
+                      host["dx"].data_ptr(), host["dt_loc"].data_ptr(), host["xI"].data_ptr())
+
+    stream = torch.cuda.ExternalStream(g.stream)
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    upload()
+    for _ in range(args.warmup):
+        g.step(1, stats=False)
+    torch.cuda.synchronize()
+    stats0 = g.step(1)  # one step with statistics, outside the timed region
+    assert stats0["status"] == 0, stats0
+
+    # ---- device-resident timing: K launches, one RK3 step each
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            ev[0].record(stream)
+            for k in range(args.steps):
+                g.step(1, stats=False)
+                ev[k + 1].record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    per_launch = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    ms_total = max_over_ranks(sum(per_launch))
+    ms_step = ms_total / args.steps
+    value = ws * zones_per_step * args.steps / (ms_total / 1e3)
+
+    # ---- end to end through the C ABI from pinned host memory: upload, K steps, download
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        upload()
+        for _ in range(args.steps):
+            g.step(1, stats=False)
+        g.download_ptrs(out_prim.data_ptr())
+        e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = ws * zones_per_step * args.steps / (e2e_ms / 1e3)
+
+    peak, peak_kind = measured_peak_hbm()
+    achieved = B_ZU_NQ6 * zones_per_step / (statistics.mean(per_launch) / 1e3) / 1e9
+    tz = traffic_per_zone()
+    line = {
+        "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.ntubes} cartesian relativistic shock tubes, 256-8192 cells (log-uniform), "
+                               "Gamma=5/3, NUM_Q=6, one RK3 step of every tube per launch", "tubes": args.ntubes,
+                   "zones_per_step": zones_per_step, "seed": SEED, "l2": "state 1.4 GB > L2 (no flush needed)",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+        "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d_bytes / args.steps,
+                "d2h_bytes_per_step": d2h_bytes / args.steps,
+                "definition": "pinned-host upload of the initial state, K steps, download of the final "
+                              "primitives, through gamma_gpu_upload/step/download"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "bytes_per_zone_update": B_ZU_NQ6,
+                     "traffic": None if tz is None else tz * zones_per_step},
+        "clocks": clk.summary(),
+        "gpu_launches": args.steps,
+        "c2p": {"mean_newton_iters": stats0["c2p_iters"] / max(stats0["c2p_calls"], 1),
+                "max_newton_iters": stats0["c2p_max_iters"], "fallbacks": stats0["c2p_fallbacks"]},
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        setups_cpu = setups
+        cores = os.cpu_count() or 1
+        v, info, _ = cpu_run(setups_cpu, 50, 2, sample=max(64, cores * 2), cores=cores,
+                             budget_zones=float(os.environ.get("GAMMA_CPU_ZONES", 3.0e7)))
+        line["cpu_baseline"] = dict(info, value=v, unit="zone-updates/s")
+    if rank == 0:
+        print(json.dumps(line))
+    g.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gamma", choices=["gamma", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ntubes", type=int, default=NTUBES, help="smaller batches for profiling captures")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,428 @@
+// C-ABI of the B200 moving-mesh hydro step (include/gamma_gpu.h).
+#include "gamma_gpu.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "track_step.cuh"
+
+namespace {
+
+enum Kind { KIND_CART = 0, KIND_SPH = 1 };
+
+constexpr int kBlock = 128;
+
+}  // namespace
+
+struct gamma_ctx {
+  gamma_config_t cfg{};
+  int kind = KIND_CART;
+  int nq = 0, nqs = 0;
+  int nruns = 0;
+  int max_cap = 0;
+  std::vector<int> cap;
+  std::vector<long long> off;
+  long long N = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<void *> allocs;
+  gb::Tracks T{};
+  int *d_order = nullptr;
+  int *d_queue = nullptr;
+  gb::StepStats *d_stats = nullptr;
+  int grid = 0;
+  size_t smem = 0;
+  std::string err;
+};
+
+namespace {
+
+int fail_cuda(gamma_ctx *c, cudaError_t e, const char *what) {
+  if (c) c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return GAMMA_ERR_CUDA;
+}
+
+#define GB_CUDA(ctx, call)                                   \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) return fail_cuda(ctx, e_, #call); \
+  } while (0)
+
+int check_cfg(const gamma_config_t *cfg, int *kind) {
+  if (!cfg) return GAMMA_ERR_INVALID;
+  if (cfg->ngst != 2) return GAMMA_ERR_INVALID;
+  if (!(cfg->gamma_ad > 1.) || !(cfg->cfl > 0.)) return GAMMA_ERR_INVALID;
+  if (cfg->geometry == GAMMA_GEOM_SPHERICAL1D && cfg->hydro == GAMMA_HYDRO_REL_SPH && cfg->nq == 10 &&
+      cfg->shock_detection && cfg->local_synchrotron && cfg->problem == GAMMA_PROBLEM_BM1D) {
+    *kind = KIND_SPH;
+    return GAMMA_OK;
+  }
+  if (cfg->geometry == GAMMA_GEOM_CARTESIAN && cfg->hydro == GAMMA_HYDRO_REL_CART && cfg->nq == 6 &&
+      !cfg->shock_detection && !cfg->local_synchrotron && cfg->problem == GAMMA_PROBLEM_TUBE &&
+      cfg->eos == GAMMA_EOS_IDEAL) {
+    *kind = KIND_CART;
+    return GAMMA_OK;
+  }
+  return GAMMA_ERR_INVALID;
+}
+
+gb::Phys phys_of(const gamma_config_t &c) {
+  gb::Phys p;
+  p.gamma_ad = c.gamma_ad;
+  p.cfl = c.cfl;
+  p.vi = c.vi;
+  p.eos = c.eos;
+  p.ngst = c.ngst;
+  return p;
+}
+
+template <class Cfg>
+size_t smem_bytes(int max_cap) {
+  using TS = gb::TrackStep<Cfg, kBlock>;
+  return sizeof(typename TS::Smem) + 4u * 4u * (size_t)gb::regrid_words(max_cap);
+}
+
+template <class Cfg>
+int configure_launch(gamma_ctx *c) {
+  auto kern = gb::track_step_kernel<Cfg, kBlock>;
+  c->smem = smem_bytes<Cfg>(c->max_cap);
+  GB_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem));
+  int dev = 0, nsm = 0, occ = 0;
+  GB_CUDA(c, cudaGetDevice(&dev));
+  GB_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  GB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlock, c->smem));
+  if (occ < 1) occ = 1;
+  c->grid = std::min(c->nruns, nsm * occ);
+  return GAMMA_OK;
+}
+
+template <class Cfg>
+int launch_step(gamma_ctx *c, int nsteps, int regrid_only) {
+  gb::track_step_kernel<Cfg, kBlock><<<c->grid, kBlock, c->smem, c->stream>>>(
+      c->T, phys_of(c->cfg), nsteps, c->d_order, c->nruns, c->d_queue, c->d_stats, regrid_only);
+  GB_CUDA(c, cudaGetLastError());
+  return GAMMA_OK;
+}
+
+template <class Cfg>
+__global__ void cons2prim_kernel(gb::Phys ph, double *cons, double *prim, int n, int *iters) {
+  constexpr int NQ = Cfg::NQ;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    double c[NQ], p[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      c[q] = cons[(long long)q * n + k];
+      p[q] = prim[(long long)q * n + k];
+    }
+    gb::C2PStats st;
+    gb::cons2prim<Cfg>(ph, c, p, &st);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      cons[(long long)q * n + k] = c[q];
+      prim[(long long)q * n + k] = p[q];
+    }
+    if (iters) iters[k] = st.iters;
+  }
+}
+
+}  // namespace
+
+#define GAMMA_API __attribute__((visibility("default")))
+
+extern "C" {
+
+GAMMA_API const char *gamma_gpu_strerror(int code) {
+  switch (code) {
+    case GAMMA_OK: return "ok";
+    case GAMMA_ERR_INVALID: return "invalid argument or unsupported module combination";
+    case GAMMA_ERR_CUDA: return "CUDA error";
+    case GAMMA_ERR_CAPACITY: return "track exceeds its capacity";
+    case GAMMA_ERR_NO_DEVICE: return "no usable sm_100 CUDA device";
+    case GAMMA_ERR_NEG_DT: return "negative CFL time-step candidate (reference exit code 30)";
+    default: return "unknown error";
+  }
+}
+
+GAMMA_API const char *gamma_gpu_last_error(const gamma_ctx_t *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+GAMMA_API void *gamma_gpu_stream(gamma_ctx_t *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+GAMMA_API int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *capacity, gamma_ctx_t **out) {
+  if (!out || nruns <= 0 || !capacity) return GAMMA_ERR_INVALID;
+  *out = nullptr;
+  int kind;
+  if (check_cfg(cfg, &kind) != GAMMA_OK) return GAMMA_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GAMMA_ERR_NO_DEVICE;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess || prop.major != 10) return GAMMA_ERR_NO_DEVICE;
+
+  gamma_ctx *c = new gamma_ctx();
+  c->cfg = *cfg;
+  c->kind = kind;
+  c->nq = cfg->nq;
+  c->nqs = cfg->nq - 1;
+  c->nruns = nruns;
+  c->cap.assign(capacity, capacity + nruns);
+  c->off.resize(nruns);
+  long long N = 0;
+  for (int r = 0; r < nruns; ++r) {
+    if (c->cap[r] < 2 * cfg->ngst + 3) {
+      delete c;
+      return GAMMA_ERR_INVALID;
+    }
+    c->off[r] = N;
+    N += (c->cap[r] + 1) & ~1;  // keep every run 16-byte aligned
+    c->max_cap = std::max(c->max_cap, c->cap[r]);
+  }
+  c->N = N;
+
+  auto fail = [&](cudaError_t e, const char *what) {
+    int rc = fail_cuda(c, e, what);
+    std::string keep = c->err;
+    gamma_gpu_destroy(c);
+    (void)keep;
+    return rc;
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+  if ((e = cudaEventCreate(&c->ev0)) != cudaSuccess) return fail(e, "event");
+  if ((e = cudaEventCreate(&c->ev1)) != cudaSuccess) return fail(e, "event");
+
+  auto alloc = [&](size_t bytes, void **p) -> cudaError_t {
+    cudaError_t ee = cudaMalloc(p, std::max<size_t>(bytes, 16));
+    if (ee == cudaSuccess) {
+      c->allocs.push_back(*p);
+      ee = cudaMemsetAsync(*p, 0, std::max<size_t>(bytes, 16), c->stream);
+    }
+    return ee;
+  };
+  const size_t d = sizeof(double);
+  gb::Tracks &T = c->T;
+  T.N = N;
+  const size_t nqs = (size_t)c->nqs;
+#define GB_ALLOC(ptr, bytes)                                               \
+  if ((e = alloc((bytes), (void **)&(ptr))) != cudaSuccess) return fail(e, "cudaMalloc " #ptr)
+  GB_ALLOC(T.prim, nqs * N * d);
+  GB_ALLOC(T.x, N * d);
+  GB_ALLOC(T.dx, N * d);
+  GB_ALLOC(T.dtl, N * d);
+  GB_ALLOC(T.xI, N * d);
+  GB_ALLOC(T.u0, nqs * N * d);
+  GB_ALLOC(T.xI0, N * d);
+  if (kind == KIND_SPH) {
+    GB_ALLOC(T.sd, N * d);
+    GB_ALLOC(T.pspec, N * d);
+    GB_ALLOC(T.shocked, (size_t)N);
+    gb::RegridScratch &S = T.rg;
+    S.N = N;
+    GB_ALLOC(S.nprim, nqs * 2 * N * d);
+    GB_ALLOC(S.nx, 2 * N * d);
+    GB_ALLOC(S.ndx, 2 * N * d);
+    GB_ALLOC(S.ndtl, 2 * N * d);
+    GB_ALLOC(S.nrifx, 2 * N * d);
+    GB_ALLOC(S.nrif, 2 * N * sizeof(int));
+    GB_ALLOC(S.seg_start, 4 * N * sizeof(int));
+    GB_ALLOC(S.seg_src, 4 * N * sizeof(int));
+    GB_ALLOC(S.tprim, nqs * N * d);
+    GB_ALLOC(S.tx, N * d);
+    GB_ALLOC(S.tdx, N * d);
+    GB_ALLOC(S.tdtl, N * d);
+    GB_ALLOC(S.txI, N * d);
+  }
+  long long *d_off;
+  int *d_cap;
+  gb::RunState *d_run;
+  gb::RunParams *d_par;
+  GB_ALLOC(d_off, nruns * sizeof(long long));
+  GB_ALLOC(d_cap, nruns * sizeof(int));
+  GB_ALLOC(d_run, nruns * sizeof(gb::RunState));
+  GB_ALLOC(d_par, nruns * sizeof(gb::RunParams));
+  GB_ALLOC(c->d_order, nruns * sizeof(int));
+  GB_ALLOC(c->d_queue, sizeof(int));
+  GB_ALLOC(c->d_stats, sizeof(gb::StepStats));
+#undef GB_ALLOC
+  T.off = d_off;
+  T.cap = d_cap;
+  T.run = d_run;
+  T.par = d_par;
+  if ((e = cudaMemcpyAsync(d_off, c->off.data(), nruns * sizeof(long long), cudaMemcpyHostToDevice, c->stream)) !=
+      cudaSuccess)
+    return fail(e, "copy offsets");
+  if ((e = cudaMemcpyAsync(d_cap, c->cap.data(), nruns * sizeof(int), cudaMemcpyHostToDevice, c->stream)) !=
+      cudaSuccess)
+    return fail(e, "copy capacities");
+  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return fail(e, "sync");
+  int rc = kind == KIND_SPH ? configure_launch<gb::CfgSph>(c) : configure_launch<gb::CfgCart>(c);
+  if (rc != GAMMA_OK) {
+    gamma_gpu_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_gpu_layout(const gamma_ctx_t *ctx, long long *offsets, long long *total) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  if (offsets) std::copy(ctx->off.begin(), ctx->off.end(), offsets);
+  if (total) *total = ctx->N;
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_gpu_set_params(gamma_ctx_t *ctx, const gamma_run_params_t *params) {
+  if (!ctx || !params) return GAMMA_ERR_INVALID;
+  static_assert(sizeof(gamma_run_params_t) == sizeof(gb::RunParams), "run parameter record layout");
+  GB_CUDA(ctx, cudaMemcpyAsync((void *)ctx->T.par, params, ctx->nruns * sizeof(gb::RunParams),
+                               cudaMemcpyHostToDevice, ctx->stream));
+  GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_gpu_upload(gamma_ctx_t *ctx, const int *ntrack, const double *t, const long long *it, const double *prim,
+                     const double *x, const double *dx, const double *dt_loc, const double *xI) {
+  if (!ctx || !ntrack || !prim || !x || !dx || !xI) return GAMMA_ERR_INVALID;
+  const int R = ctx->nruns;
+  std::vector<gb::RunState> rs(R);
+  for (int r = 0; r < R; ++r) {
+    if (ntrack[r] > ctx->cap[r]) return GAMMA_ERR_CAPACITY;
+    if (ntrack[r] < 2 * ctx->cfg.ngst + 3) return GAMMA_ERR_INVALID;
+    rs[r].ntrack = ntrack[r];
+    rs[r].status = 0;
+    rs[r].t = t ? t[r] : 0.;
+    rs[r].dt = 0.;
+    rs[r].it = it ? it[r] : 0;
+  }
+  // work-queue order: longest tracks first
+  std::vector<int> order(R);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ntrack[a] > ntrack[b]; });
+  const size_t row = (size_t)ctx->N * sizeof(double);
+  const gb::Tracks &T = ctx->T;
+  for (int s = 0; s < ctx->nqs; ++s) {
+    const int q = s < 3 ? s : s + 1;
+    GB_CUDA(ctx, cudaMemcpyAsync(T.prim + (size_t)s * ctx->N, prim + (size_t)q * ctx->N, row,
+                                 cudaMemcpyHostToDevice, ctx->stream));
+  }
+  GB_CUDA(ctx, cudaMemcpyAsync(T.x, x, row, cudaMemcpyHostToDevice, ctx->stream));
+  GB_CUDA(ctx, cudaMemcpyAsync(T.dx, dx, row, cudaMemcpyHostToDevice, ctx->stream));
+  GB_CUDA(ctx, cudaMemcpyAsync(T.xI, xI, row, cudaMemcpyHostToDevice, ctx->stream));
+  if (dt_loc) {
+    GB_CUDA(ctx, cudaMemcpyAsync(T.dtl, dt_loc, row, cudaMemcpyHostToDevice, ctx->stream));
+  } else {
+    std::vector<double> inf((size_t)ctx->N, gb::DT_INF);
+    GB_CUDA(ctx, cudaMemcpyAsync(T.dtl, inf.data(), row, cudaMemcpyHostToDevice, ctx->stream));
+    GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  GB_CUDA(ctx, cudaMemcpyAsync(T.run, rs.data(), R * sizeof(gb::RunState), cudaMemcpyHostToDevice, ctx->stream));
+  GB_CUDA(ctx, cudaMemcpyAsync(ctx->d_order, order.data(), R * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // rs/order are stack buffers
+  return GAMMA_OK;
+}
+
+namespace {
+int run_steps(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats, int regrid_only) {
+  if (!ctx || nsteps < 0) return GAMMA_ERR_INVALID;
+  GB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(int), ctx->stream));
+  GB_CUDA(ctx, cudaMemsetAsync(ctx->d_stats, 0, sizeof(gb::StepStats), ctx->stream));
+  GB_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  int rc = ctx->kind == KIND_SPH ? launch_step<gb::CfgSph>(ctx, nsteps, regrid_only)
+                                 : launch_step<gb::CfgCart>(ctx, nsteps, regrid_only);
+  if (rc != GAMMA_OK) return rc;
+  GB_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  if (stats) {
+    gb::StepStats h;
+    GB_CUDA(ctx, cudaMemcpyAsync(&h, ctx->d_stats, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    GB_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    stats->c2p_calls = h.c2p_calls;
+    stats->c2p_iters = h.c2p_iters;
+    stats->c2p_fallbacks = h.c2p_fallbacks;
+    stats->zone_updates = h.zone_updates;
+    stats->splits = h.splits;
+    stats->merges = h.merges;
+    stats->c2p_max_iters = h.c2p_max_iters;
+    stats->status = h.status == 30 ? GAMMA_ERR_NEG_DT : (h.status ? GAMMA_ERR_INVALID : GAMMA_OK);
+    stats->device_ms = ms;
+  }
+  return GAMMA_OK;
+}
+}  // namespace
+
+GAMMA_API int gamma_gpu_step(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats) {
+  return run_steps(ctx, nsteps, stats, 0);
+}
+
+GAMMA_API int gamma_gpu_regrid(gamma_ctx_t *ctx, gamma_step_stats_t *stats) {
+  if (ctx && ctx->kind != KIND_SPH) return GAMMA_OK;  // problems without a regrid criterion
+  return run_steps(ctx, 1, stats, 1);
+}
+
+GAMMA_API int gamma_gpu_download(gamma_ctx_t *ctx, int *ntrack, double *t, double *dt, long long *it, int *status, double *prim,
+                       double *x, double *dx, double *dt_loc, double *xI) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  const int R = ctx->nruns;
+  const size_t row = (size_t)ctx->N * sizeof(double);
+  const gb::Tracks &T = ctx->T;
+  std::vector<gb::RunState> rs(R);
+  GB_CUDA(ctx, cudaMemcpyAsync(rs.data(), T.run, R * sizeof(gb::RunState), cudaMemcpyDeviceToHost, ctx->stream));
+  if (prim) {
+    for (int s = 0; s < ctx->nqs; ++s) {
+      const int q = s < 3 ? s : s + 1;
+      GB_CUDA(ctx, cudaMemcpyAsync(prim + (size_t)q * ctx->N, T.prim + (size_t)s * ctx->N, row,
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    std::fill(prim + 3 * (size_t)ctx->N, prim + 4 * (size_t)ctx->N, 0.);
+  }
+  if (x) GB_CUDA(ctx, cudaMemcpyAsync(x, T.x, row, cudaMemcpyDeviceToHost, ctx->stream));
+  if (dx) GB_CUDA(ctx, cudaMemcpyAsync(dx, T.dx, row, cudaMemcpyDeviceToHost, ctx->stream));
+  if (dt_loc) GB_CUDA(ctx, cudaMemcpyAsync(dt_loc, T.dtl, row, cudaMemcpyDeviceToHost, ctx->stream));
+  if (xI) GB_CUDA(ctx, cudaMemcpyAsync(xI, T.xI, row, cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int r = 0; r < R; ++r) {
+    if (ntrack) ntrack[r] = rs[r].ntrack;
+    if (t) t[r] = rs[r].t;
+    if (dt) dt[r] = rs[r].dt;
+    if (it) it[r] = rs[r].it;
+    if (status) status[r] = rs[r].status == 30 ? GAMMA_ERR_NEG_DT : (rs[r].status ? GAMMA_ERR_INVALID : GAMMA_OK);
+  }
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_gpu_cons2prim(const gamma_config_t *cfg, double *cons, double *prim, int n, int *iters, void *stream) {
+  int kind;
+  if (check_cfg(cfg, &kind) != GAMMA_OK || !cons || !prim || n < 0) return GAMMA_ERR_INVALID;
+  if (n == 0) return GAMMA_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int bs = 128;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::min((n + bs - 1) / bs, nsm * 16);
+  if (kind == KIND_SPH)
+    cons2prim_kernel<gb::CfgSph><<<grid, bs, 0, s>>>(phys_of(*cfg), cons, prim, n, iters);
+  else
+    cons2prim_kernel<gb::CfgCart><<<grid, bs, 0, s>>>(phys_of(*cfg), cons, prim, n, iters);
+  if (cudaGetLastError() != cudaSuccess) return GAMMA_ERR_CUDA;
+  return GAMMA_OK;
+}
+
+GAMMA_API void gamma_gpu_destroy(gamma_ctx_t *ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (void *p : ctx->allocs) cudaFree(p);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+}  // extern "C"

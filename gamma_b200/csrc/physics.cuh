@@ -1,0 +1,569 @@
+// Device physics of the 1D moving-mesh relativistic hydro step (FP64).
+//
+// Each function restates one member of the GAMMA reference and keeps its
+// floating-point operation order, so that with -fmad=false the only
+// differences to the CPU reference come from libm (pow, tanh) and from the
+// pressure root finder (Newton-Raphson here, GSL Brent there).
+//
+// Variable slots follow src/environment.h:33-82.  Slot 3 (the theta momentum /
+// 4-velocity) is identically zero in 1D: it is only ever multiplied by r
+// (rel_sph.cpp:78,108,441) starting from zero, so it is neither stored nor
+// computed here.
+#pragma once
+
+#include <cstdint>
+#include <math.h>
+
+#ifndef GB_HD
+#define GB_HD __device__ __forceinline__
+#endif
+
+namespace gb {
+
+enum { RHO = 0, PPP = 1, UU1 = 2, UU2 = 3 };
+enum { DEN = 0, TAU = 1, SS1 = 2, SS2 = 3 };
+enum { TR1 = 4, GMN = 6, GMX = 7, GMD = 8, PSN = 9 };
+enum { SKIP = 0, MERGE = 1, SPLIT = 2 };
+
+// src/constants.h:6-28
+constexpr double P_FLOOR = 1.e-10;
+constexpr double PI_ = 3.14159265358979323846;
+constexpr double MP = 1.6726219e-24;
+constexpr double ME = 9.1093835e-28;
+constexpr double C_LIGHT = 2.99792458e10;
+constexpr double ALPHA_SYN = 1.29251816e-09;
+constexpr double P_SPEC = 2.22;
+constexpr double EPS_E = 0.1;
+constexpr double EPS_B = 0.01;
+constexpr double ZETA = 1.;
+constexpr double GAMMA_MAX_INIT = 1.e8;
+constexpr double DETECT_SHOCK_THRESHOLD = 0.01;
+constexpr double DT_INF = 1.e15;
+
+// ---------------------------------------------------------------------------
+// Module selections (the reference's Makefile GEOMETRY/HYDRO/RADIATION slots and
+// environment.h switches) as compile-time policies.
+
+// cartesian + rel_cart, ideal gas, no shock detection / synchrotron: NUM_Q = 6.
+struct CfgCart {
+  static constexpr int NQ = 6;
+  static constexpr bool SPH = false;    // rel_sph hydro and spherical1D geometry
+  static constexpr bool SHOCK = false;  // SHOCK_DETECTION_
+  static constexpr bool SYNCH = false;  // LOCAL_SYNCHROTRON_
+  static constexpr bool BM = false;     // Blandford-McKee problem hooks + regrid
+};
+
+// spherical1D + rel_sph + radiation_sph: NUM_Q = 10.
+struct CfgSph {
+  static constexpr int NQ = 10;
+  static constexpr bool SPH = true;
+  static constexpr bool SHOCK = true;
+  static constexpr bool SYNCH = true;
+  static constexpr bool BM = true;
+};
+
+// Run-time constants shared by every run of a context.
+struct Phys {
+  double gamma_ad;  // GAMMA_
+  double cfl;       // CFL_
+  double vi;        // VI
+  int eos;          // 0 ideal, 1 Synge / Taub-Mathews (rel_sph.cpp:37-52)
+  int ngst;
+};
+
+template <class Cfg>
+struct Prim {
+  double v[Cfg::NQ];
+};
+
+// FluidState: primitive, conserved and physical flux of one state.
+template <class Cfg>
+struct FState {
+  double prim[Cfg::NQ];
+  double cons[Cfg::NQ];
+  double flux[Cfg::NQ];
+};
+
+GB_HD double lfac_of(double uu) {
+  // fluid.cpp:10-22 (u = sqrt(sum uu^2) then sqrt(1+u^2))
+  double u = 0.;
+  u += uu * uu;
+  u = sqrt(u);
+  return sqrt(1 + u * u);
+}
+
+// FluidState::gamma (rel_sph.cpp:37-52)
+GB_HD double eos_gamma(const Phys &ph, double rho, double p) {
+  const double G = ph.gamma_ad;
+  if (ph.eos == 0) return G;
+  double a = p / rho / (G - 1.);
+  double e_ratio = a + sqrt(a * a + 1.);
+  return G - (G - 1.) / 2. * (1. - 1. / (e_ratio * e_ratio));
+}
+
+template <class Cfg>
+GB_HD double state_gamma(const Phys &ph, const double *prim) {
+  return Cfg::SPH ? eos_gamma(ph, prim[RHO], prim[PPP]) : ph.gamma_ad;
+}
+
+// prim2cons (rel_sph.cpp:55-82, rel_cart.cpp:37-64)
+template <class Cfg>
+GB_HD void prim2cons(const Phys &ph, const double *prim, double *cons) {
+  double rho = prim[RHO];
+  double p = prim[PPP];
+  double uu = prim[UU1];
+  double lfac = lfac_of(uu);
+  double gma = state_gamma<Cfg>(ph, prim);
+  double h = 1. + p * gma / (gma - 1.) / rho;
+  double D = lfac * rho;
+  double tau = D * h * lfac - p - D;
+  double ss = D * h * uu;
+  cons[DEN] = D;
+  cons[TAU] = tau;
+  cons[SS1] = ss;
+  cons[SS2] = 0.;
+#pragma unroll
+  for (int t = TR1; t < Cfg::NQ; ++t) cons[t] = prim[t] * D;
+}
+
+// state2flux (rel_sph.cpp:85-113, rel_cart.cpp:67-95)
+template <class Cfg>
+GB_HD void state2flux(const double *prim, const double *cons, double *flux) {
+  double p = prim[PPP];
+  double uu = prim[UU1];
+  double lfac = lfac_of(uu);
+  double D = cons[DEN];
+  double ss = cons[SS1];
+  flux[DEN] = D * uu / lfac;
+  flux[SS1] = ss * uu / lfac + p;
+  flux[SS2] = 0.;
+  flux[TAU] = ss - D * uu / lfac;
+#pragma unroll
+  for (int t = TR1; t < Cfg::NQ; ++t) flux[t] = cons[t] * uu / lfac;
+}
+
+// ---------------------------------------------------------------------------
+// cons2prim: pressure root of f(p) (rel_sph.cpp:191-210 / rel_cart.cpp:108-123)
+// by safeguarded Newton-Raphson on the same bracket and with the same
+// no-solution semantics as the reference's Brent driver (rel_sph.cpp:243-286).
+
+struct C2PStats {
+  int iters;     // f evaluations after the bracket set-up
+  int fallback;  // 1 if the iteration cap was hit (bisection-limited)
+};
+
+template <class Cfg>
+GB_HD double c2p_f(const Phys &ph, double p, double D, double S, double E) {
+  if (Cfg::SPH) {
+    double lfac = 1. / sqrt(fabs(1. - (S * S) / ((E + p) * (E + p))));
+    double gma = eos_gamma(ph, D / lfac, p);
+    return (E + p - D * lfac - (gma * p * lfac * lfac) / (gma - 1.));
+  } else {
+    double g = ph.gamma_ad;
+    double lfac = 1. / sqrt(1. - (S * S) / ((E + p) * (E + p)));
+    return (E + p - D * lfac - (g * p * lfac * lfac) / (g - 1.));
+  }
+}
+
+// f and df/dp.  For the Synge EOS the derivative of Gamma_eff is included
+// through rho = D/lfac(p) and a = p/rho/(G-1).
+template <class Cfg>
+GB_HD double c2p_f_df(const Phys &ph, double p, double D, double S, double E, double *df) {
+  const double W = E + p;
+  const double x = (S * S) / (W * W);
+  const double arg = Cfg::SPH ? fabs(1. - x) : (1. - x);
+  const double lfac = 1. / sqrt(arg);
+  // d(lfac)/dp = -lfac^3 S^2 / W^3 (sign flips with fabs when x > 1)
+  const double sgn = (1. - x) >= 0. ? 1. : -1.;
+  const double dl = -sgn * lfac * lfac * lfac * x / W;
+  double gma, dgma;
+  if (Cfg::SPH && ph.eos != 0) {
+    const double G = ph.gamma_ad;
+    const double rho = D / lfac;
+    const double a = p / rho / (G - 1.);
+    const double sq = sqrt(a * a + 1.);
+    const double e = a + sq;
+    gma = G - (G - 1.) / 2. * (1. - 1. / (e * e));
+    // a = p lfac / (D (G-1)); da/dp = (lfac + p dl) / (D (G-1))
+    const double da = (lfac + p * dl) / (D * (G - 1.));
+    const double de = da * (1. + a / sq);
+    dgma = -(G - 1.) / (e * e * e) * de;
+  } else {
+    gma = ph.gamma_ad;
+    dgma = 0.;
+  }
+  const double k = gma / (gma - 1.);
+  const double dk = -dgma / ((gma - 1.) * (gma - 1.));
+  const double f = (E + p - D * lfac - (gma * p * lfac * lfac) / (gma - 1.));
+  *df = 1. - D * dl - dk * p * lfac * lfac - k * (lfac * lfac + 2. * p * lfac * dl);
+  return f;
+}
+
+// FluidState::cons2prim (rel_sph.cpp:213-320; rel_cart.cpp:125-229).
+// On entry prim holds the previous primitives (pressure warm start); on exit
+// prim holds the recovered primitives and cons is rewritten by prim2cons.
+template <class Cfg>
+GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
+  const double D = cons[DEN];
+  const double tau = cons[TAU];
+  const double E = D + tau;
+  const double ss = cons[SS1];
+  double S2 = 0.;
+  S2 += ss * ss;
+  const double S = sqrt(S2);
+
+  double pCand = Cfg::SPH ? fmax(1.e-13, prim[PPP]) : prim[PPP];
+  int iters = 0, fallback = 0;
+  const double f_init = c2p_f<Cfg>(ph, pCand, D, S, E);
+  if (fabs(f_init) > 0.) {
+    double p_lo = fmax(0., (1. + 1e-13) * S - E);
+    bool find_p = true;
+    if (c2p_f<Cfg>(ph, p_lo, D, S, E) < 0) find_p = false;
+    double p_hi;
+    if (f_init < 0) {
+      p_hi = 1. * pCand;
+    } else {
+      p_hi = pCand;
+      // the reference grows p_hi without bound (a zero guess would never end);
+      // 400 decades reach infinity, where f is NaN and the loop stops anyway
+      for (int g = 0; g < 400 && c2p_f<Cfg>(ph, p_hi, D, S, E) > 0; ++g) p_hi *= 10;
+    }
+    if (p_hi < p_lo) find_p = false;
+    if (find_p) {
+      // f(lo) >= 0 >= f(hi).  The warm start tightens one side.
+      double lo = p_lo, hi = p_hi;
+      if (f_init > 0.) lo = fmax(lo, pCand);
+      double p = fmin(fmax(pCand, lo), hi);
+      double df;
+      double f = c2p_f_df<Cfg>(ph, p, D, S, E, &df);
+      const int MAXIT = 100;
+      const double eps = 2.220446049250313e-16;
+      for (iters = 1; iters <= MAXIT; ++iters) {
+        // Rounding noise of f: E, p, D lfac and k p lfac^2 cancel, and lfac
+        // itself carries eps*lfac^2 relative error from 1 - S^2/W^2.  Below
+        // this level the sign of f is noise and p is as good as it gets.
+        const double W = E + p;
+        const double l2 = W * W / fmax(W * W - S * S, W * W * eps);
+        const double noise = eps * (E + p + D * sqrt(l2) * (1. + l2) + 4. * p * l2 * (1. + 2. * l2));
+        if (f == 0. || fabs(f) <= 4. * noise) break;
+        double pn = p - f / df;
+        if (!(pn > lo && pn < hi)) {
+          // Newton left the bracket: bisect, geometrically once lo > 0
+          pn = lo > 0. ? sqrt(lo) * sqrt(hi) : 0.5 * (lo + hi);
+          if (!(pn > lo && pn < hi)) pn = 0.5 * (lo + hi);
+        }
+        double dfn;
+        const double fn = c2p_f_df<Cfg>(ph, pn, D, S, E, &dfn);
+        if (fn > 0.) lo = pn;
+        else if (fn < 0.) hi = pn;
+        const double step = fabs(pn - p);
+        p = pn;
+        f = fn;
+        df = dfn;
+        if (fn == 0. || step <= 1.e-14 * pn || (hi - lo) <= 1.e-14 * hi) break;
+      }
+      if (iters > MAXIT) fallback = 1;
+      pCand = p;
+    }
+  }
+  if (st) {
+    st->iters = iters;
+    st->fallback = fallback;
+  }
+
+  double p = pCand;
+  double Ep2 = (E + p) * (E + p);
+  double v2 = S2 / Ep2;
+  double lfac = 1. / sqrt(fabs(1. - v2));
+  double rho = D / lfac;
+  double uu;
+  if (fabs(S) == 0.) {
+    uu = 0;
+  } else {
+    double v = sqrt(1. - 1. / (lfac * lfac));
+    uu = lfac * v * (ss / S);
+  }
+  if (Cfg::SPH) p = fmax(p, P_FLOOR);
+  prim[PPP] = p;
+  prim[RHO] = rho;
+  prim[UU1] = uu;
+  prim[UU2] = 0.;
+#pragma unroll
+  for (int t = TR1; t < Cfg::NQ; ++t) prim[t] = cons[t] / D;
+  prim2cons<Cfg>(ph, prim, cons);
+}
+
+// ---------------------------------------------------------------------------
+// Riemann problem at a moving interface
+
+struct Waves {
+  double lL, lS, lR;
+};
+
+// Interface::wavespeedEstimates + computeLambda (rel_sph.cpp:322-394;
+// rel_cart.cpp:260-302 switches to the linear root when |FhllE| < 1e-15).
+template <class Cfg>
+GB_HD Waves compute_lambda(const Phys &ph, const FState<Cfg> &L, const FState<Cfg> &R) {
+  const double G = ph.gamma_ad;
+  Waves w;
+  double lfacL = lfac_of(L.prim[UU1]);
+  double lfacR = lfac_of(R.prim[UU1]);
+  double vL = L.prim[UU1] / lfacL;
+  double vR = R.prim[UU1] / lfacR;
+  double cSL = sqrt(G * L.prim[PPP] / (L.prim[RHO] + L.prim[PPP] * G / (G - 1.)));
+  double cSR = sqrt(G * R.prim[PPP] / (R.prim[RHO] + R.prim[PPP] * G / (G - 1.)));
+  double sgSL = cSL * cSL / (lfacL * lfacL * (1. - cSL * cSL));
+  double sgSR = cSR * cSR / (lfacR * lfacR * (1. - cSR * cSR));
+  double l1, l2;
+  l1 = (vR - sqrt(sgSR * (1. - vR * vR + sgSR))) / (1. + sgSR);
+  l2 = (vL - sqrt(sgSL * (1. - vL * vL + sgSL))) / (1. + sgSL);
+  w.lL = fmin(l1, l2);
+  l1 = (vR + sqrt(sgSR * (1. - vR * vR + sgSR))) / (1. + sgSR);
+  l2 = (vL + sqrt(sgSL * (1. - vL * vL + sgSL))) / (1. + sgSL);
+  w.lR = fmax(l1, l2);
+
+  const double lL = w.lL, lR = w.lR;
+  double mmL = L.cons[SS1];
+  double mmR = R.cons[SS1];
+  double pL = L.prim[PPP];
+  double pR = R.prim[PPP];
+  double EL = L.cons[TAU] + L.cons[DEN];
+  double ER = R.cons[TAU] + R.cons[DEN];
+  double AL = lL * EL - mmL;
+  double AR = lR * ER - mmR;
+  double BL = mmL * (lL - vL) - pL;
+  double BR = mmR * (lR - vR) - pR;
+  double FhllE = (lL * AR - lR * AL) / (lR - lL);
+  double Ehll = (AR - AL) / (lR - lL);
+  double Fhllm = (lL * BR - lR * BL) / (lR - lL);
+  double mhll = (BR - BL) / (lR - lL);
+  bool linear = Cfg::SPH ? (fabs(FhllE) == 0) : (fabs(FhllE) < 1.e-15);
+  if (linear) {
+    w.lS = mhll / (Ehll + Fhllm);
+  } else {
+    double eh = Ehll + Fhllm;
+    double delta = eh * eh - 4. * FhllE * mhll;
+    w.lS = ((Ehll + Fhllm) - sqrt(delta)) / (2. * FhllE);
+  }
+  return w;
+}
+
+// HLLC flux F - vU in the frame of an interface moving at v, times dA
+// (hllc.cpp:12-39 with starState rel_sph.cpp:397-450).  The four branch tests
+// are independent ifs in the reference and stay so.
+template <class Cfg>
+GB_HD void hllc_flux(const FState<Cfg> &L, const FState<Cfg> &R, const Waves &w, double v, double dA,
+                     double *flux) {
+  const double lS = w.lS;
+  auto star = [&](const FState<Cfg> &Sin, double lbda, double *out_cons) {
+    double m = Sin.cons[SS1];
+    double lfac = lfac_of(Sin.prim[UU1]);
+    double vv = Sin.prim[UU1] / lfac;
+    double p = Sin.prim[PPP];
+    double D = Sin.cons[DEN];
+    double E = Sin.cons[TAU] + Sin.cons[DEN];
+    double A = lbda * E - m;
+    double B = m * (lbda - vv) - p;
+    double pS = (A * lS - B) / (1. - lbda * lS);
+    double k = (lbda - vv) / (lbda - lS);
+    out_cons[DEN] = D * k;
+    out_cons[SS1] = (m * (lbda - vv) + pS - p) / (lbda - lS);
+    out_cons[SS2] = 0.;
+    out_cons[TAU] = (E * (lbda - vv) + pS * lS - p * vv) / (lbda - lS) - D * k;
+#pragma unroll
+    for (int t = TR1; t < Cfg::NQ; ++t) out_cons[t] = Sin.cons[t] * k;
+  };
+  if (v < w.lL) {
+#pragma unroll
+    for (int q = 0; q < Cfg::NQ; ++q) flux[q] = L.flux[q] - v * L.cons[q];
+  }
+  if (w.lL <= v && v < lS) {
+    double sc[Cfg::NQ];
+    star(L, w.lL, sc);
+#pragma unroll
+    for (int q = 0; q < Cfg::NQ; ++q) flux[q] = L.flux[q] + w.lL * (sc[q] - L.cons[q]) - v * sc[q];
+  }
+  if (lS <= v && v < w.lR) {
+    double sc[Cfg::NQ];
+    star(R, w.lR, sc);
+#pragma unroll
+    for (int q = 0; q < Cfg::NQ; ++q) flux[q] = R.flux[q] + w.lR * (sc[q] - R.cons[q]) - v * sc[q];
+  }
+  if (w.lR <= v) {
+#pragma unroll
+    for (int q = 0; q < Cfg::NQ; ++q) flux[q] = R.flux[q] - v * R.cons[q];
+  }
+#pragma unroll
+  for (int q = 0; q < Cfg::NQ; ++q) flux[q] *= dA;
+}
+
+// ---------------------------------------------------------------------------
+// Shock detector (radiation_sph.cpp:41-158), forward direction.  Returns false
+// (and leaves *pspec alone) where the reference returns -1 early.
+template <class Cfg>
+GB_HD bool compute_Sd(const Phys &ph, const FState<Cfg> &S1, const FState<Cfg> &S2, double *Sd,
+                      double *pspec) {
+  const double G = ph.gamma_ad;
+  const int n_evals = 10;
+  const double chi = 0.5;
+  double p1 = S1.prim[PPP];
+  double p2 = S2.prim[PPP];
+  if (fabs((p1 - p2) / p1) < 1.e-10 || p1 < p2) {
+    *Sd = -1;
+    return false;
+  }
+  double delta_p = p2 - p1;
+  double dp = delta_p / (double)n_evals;
+  double rho1 = S1.prim[RHO];
+  double rho2 = S2.prim[RHO];
+  double h1 = 1 + p1 * G / (G - 1.) / rho1;
+  double h2 = 1 + p2 * G / (G - 1.) / rho2;
+  double lfac1 = lfac_of(S1.prim[UU1]);
+  double lfac2 = lfac_of(S2.prim[UU1]);
+  double vx1 = S1.prim[UU1] / lfac1;
+  double vx2 = S2.prim[UU1] / lfac2;
+  double v12 = (vx1 - vx2) / (1 - vx1 * vx2);
+  double A1 = h1 * 0.;
+  double I = 0;
+  const double ginv = 1. / G;
+#pragma unroll 2
+  for (int ip = 0; ip < n_evals; ++ip) {
+    double p = p1 + (ip + .5) * dp;
+    double rho = rho1 * pow(p / p1, ginv);
+    double h = 1 + p * G / (G - 1.) / rho;
+    double cs = sqrt(G * p / (rho + p * G / (G - 1.)));
+    double dI = sqrt(h * h + A1 * A1 * (1. - cs * cs)) / ((h * h + A1 * A1) * rho * cs) * dp;
+    I += dI;
+  }
+  double vSR = tanh(I);
+  double rho22 = rho2 * rho2;
+  double lfac22 = lfac2 * lfac2;
+  double vx22 = vx2 * vx2;
+  double g = G;
+  double gm1 = (g - 1.);
+  double gm12 = gm1 * gm1;
+  double Da = 4. * g * p1 * ((g - 1) * p2 + p1) / (gm12 * (p1 - p2) * (p1 - p2));
+  double Db = h2 * (p2 - p1) / rho2 - h2 * h2;
+  double Dd = 1. - Da * Db;
+  double h3 = (sqrt(Dd) - 1) * gm1 * (p1 - p2) / (2 * (gm1 * p2 + p1));
+  double J232a = -g / gm1 * (p1 - p2);
+  double J232b = h3 * (h3 - 1) / p1 - h2 * (h2 - 1) / p2;
+  double J232 = J232a / J232b;
+  double J23 = sqrt(J232);
+  double Vsa = rho22 * lfac22 * vx2 + fabs(J23) * sqrt(J232 + rho22 * lfac22 * (1. - vx22));
+  double Vsb = rho22 * lfac22 + J232;
+  double Vs = Vsa / Vsb;
+  double v2Sa = (p1 - p2) * (1. - vx2 * Vs);
+  double v2Sb = (Vs - vx2) * (h2 * rho2 * lfac22 * (1. - vx22) + p1 - p2);
+  double v2S = v2Sa / v2Sb;
+  double vlim = vSR + chi * (v2S - vSR);
+  *Sd = v12 - vlim;
+  *pspec = P_SPEC;  // spectral_p with VARIABLE_PSPEC_ disabled
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Local synchrotron tracers (radiation_sph.cpp:196-300)
+
+struct SynchConst {
+  double Nalpha, Nmp, Nme;
+};
+
+template <class Cfg>
+GB_HD double gammae2trac(double gme, const double *prim) {
+  double lfac = lfac_of(prim[UU1]);
+  double rho = prim[RHO];
+  if (gme != 0.) return (lfac * pow(rho, 4. / 3.) / gme);
+  return 0;
+}
+
+template <class Cfg>
+GB_HD double gamma_min_init(const Phys &ph, const SynchConst &sc, const double *prim) {
+  double rho = prim[RHO];
+  double p = prim[PPP];
+  double psyn = prim[PSN];
+  double gma = state_gamma<Cfg>(ph, prim);
+  double h = 1. + p * gma / (gma - 1.) / rho;
+  double eps = rho * (h - 1.) / gma;
+  double ee = EPS_E * eps;
+  double ne = ZETA * rho / sc.Nmp;
+  double lfac_av = ee / (ne * sc.Nme);
+  return (psyn - 2.) / (psyn - 1.) * lfac_av;
+}
+
+// Cell::radiation_injectParticles
+template <class Cfg>
+GB_HD void inject_particles(const Phys &ph, const SynchConst &sc, double *prim, bool shocked, double pspec) {
+  double lfac = lfac_of(prim[UU1]);
+  double rho = prim[RHO];
+  double lim = lfac * pow(rho, 4. / 3.) / (lfac * rho);
+  if (shocked) {
+    if (pspec > prim[PSN] || isnan(prim[PSN])) prim[PSN] = pspec;
+    prim[GMX] = gammae2trac<Cfg>(GAMMA_MAX_INIT, prim) / (lfac * rho);
+    prim[GMN] = gammae2trac<Cfg>(gamma_min_init<Cfg>(ph, sc, prim), prim) / (lfac * rho);
+  }
+  if (isnan(prim[GMX])) prim[GMX] = lim;
+  if (isnan(prim[GMN])) prim[GMN] = lim;
+}
+
+// Cell::radiativeSourceTerms: returns the increment of cons[GMX] and cons[GMN]
+template <class Cfg>
+GB_HD double radiative_source(const Phys &ph, const SynchConst &sc, const double *prim, double dV, double dt) {
+  double rho = prim[RHO];
+  double p = prim[PPP];
+  double gma = state_gamma<Cfg>(ph, prim);
+  double h = 1 + p * gma / (gma - 1.) / rho;
+  double eps = rho * (h - 1.) / gma;
+  double eB = EPS_B * eps;
+  double B = sqrt(8. * PI_ * eB);
+  return sc.Nalpha * pow(rho, 4. / 3.) * B * B * dV * dt;
+}
+
+// ---------------------------------------------------------------------------
+// Geometry (spherical1D.cpp:12-76, cartesian.cpp:11-43)
+
+struct Geom {
+  double x, dx, dV, dl, cen;
+};
+
+template <class Cfg>
+GB_HD Geom make_geom(double x, double dx) {
+  Geom g;
+  g.x = x;
+  g.dx = dx;
+  g.dl = dx;
+  if (Cfg::SPH) {
+    double r = x, dr = dx;
+    g.dV = 4. * PI_ * r * r * dr;
+    double r2 = r * r;
+    double dr2 = dr * dr;
+    g.cen = 3. * r * (r2 + dr2) / (3 * r2 + dr2);
+  } else {
+    g.dV = 1. * dx;
+    g.cen = x;
+  }
+  return g;
+}
+
+// Cell::move: geometry between two interfaces
+template <class Cfg>
+GB_HD Geom geom_between(double xL, double xR) {
+  return make_geom<Cfg>((xR + xL) / 2., (xR - xL));
+}
+
+template <class Cfg>
+GB_HD double iface_area(double x) {
+  if (Cfg::SPH) {
+    double r = x;
+    return 4. * PI_ * r * r;
+  }
+  return 1.;
+}
+
+GB_HD double minmod(double a, double b) {
+  if (fabs(a) < fabs(b) && a * b > 0) return a;
+  if (fabs(b) < fabs(a) && a * b > 0) return b;
+  return 0;
+}
+
+}  // namespace gb

@@ -1,0 +1,582 @@
+// One CTA advances one run (one 1D track of cells) through whole RK3 steps.
+//
+// Per step (src/simu.cpp:79-105): [regrid] -> reset shocks -> ghosts ->
+// stage-1 CFL candidates -> per-run dt (block min) -> stage-1 update ->
+// ghosts -> stage-2 fluxes+update+RK combine -> ghosts -> stage-3 -> inject.
+//
+// Each stage is one left-to-right sweep over the track in chunks of BS cells
+// (one interface and one cell per thread).  A chunk stages the stencil
+// (cells a-1 .. a+BS+1) in shared memory, computes the BS interfaces
+// a .. a+BS-1 (PLM + HLLC at the contact-speed interface), then updates cells
+// a .. a+BS-1 in place.  The old state of cell a+BS-1 and the results of
+// interface a+BS-1 are carried to the next chunk, so the in-place update never
+// feeds a neighbour's stencil.  Runs are independent (own dt, own regrid), so
+// a CTA takes runs from a work queue and can advance each by many steps
+// without any grid-wide synchronisation.
+#pragma once
+
+#include "physics.cuh"
+#include "regrid.cuh"
+
+namespace gb {
+
+// Device view of the pooled structure-of-arrays state.  Run r owns cells
+// [off[r], off[r]+cap[r]) of every per-cell array.  Primitive slot q is stored
+// at row (q < 3 ? q : q-1): slot 3 is identically zero in 1D.
+struct Tracks {
+  double *prim;     // [NQS][N]
+  double *x, *dx;   // cell centre and width at step start
+  double *dtl;      // Cell::dt_loc, carried between steps
+  double *xI;       // interface i sits between cells i and i+1
+  double *u0;       // [NQS][N] step-start cons * dV (stage combine)
+  double *xI0;      // step-start interface positions
+  double *sd, *pspec;
+  uint8_t *shocked;
+  long long N;      // row stride
+  const long long *off;
+  const int *cap;
+  RunState *run;    // per-run scalars (ntrack, t, dt, it, status)
+  const RunParams *par;
+  RegridScratch rg;
+};
+
+template <class Cfg>
+struct Slots {
+  static constexpr int NQS = Cfg::NQ - 1;
+  __device__ __forceinline__ static constexpr int q_of(int s) { return s < 3 ? s : s + 1; }
+};
+
+struct StepStats {
+  unsigned long long c2p_calls;
+  unsigned long long c2p_iters;
+  unsigned long long c2p_fallbacks;
+  unsigned long long zone_updates;
+  unsigned long long splits, merges;
+  int c2p_max_iters;
+  int status;
+};
+
+// calcBM (BM1D.cpp:62-86) with per-run parameters; r in code units (ls).
+__device__ __forceinline__ void calc_bm(const Phys &ph, const RunParams &P, double r_code, double t,
+                                        double *rho, double *u, double *p) {
+  const double G = ph.gamma_ad;
+  const double r = r_code * P.lNorm;
+  const double c5 = C_LIGHT * C_LIGHT * C_LIGHT * C_LIGHT * C_LIGHT;
+  double lfacShock2 = P.Etot * (17. - 4. * P.k) / (8. * PI_ * P.n_ext * MP * (t * t * t) * c5);
+  double RShock = C_LIGHT * t * (1. - 1. / (1. + 2. * (4. - P.k) * lfacShock2));
+  double rhoa = P.n_ext * MP * pow(RShock / P.Rscale, -P.k);
+  double pa = rhoa * P.eta * C_LIGHT * C_LIGHT;
+  double ha = C_LIGHT * C_LIGHT + pa * G / (G - 1.) / rhoa;
+  double pf = 2. / 3. * lfacShock2 * ha * rhoa;
+  double lfacf = sqrt(fmax(1., .5 * lfacShock2));
+  double Df = 2. * lfacShock2 * rhoa;
+  double chi = (1. + 2. * (4. - P.k) * lfacShock2) * (1. - r / (C_LIGHT * t));
+  *p = pf * pow(chi, -(17. - 4. * P.k) / (12. - 3. * P.k)) / P.pNorm;
+  double lfac = sqrt(lfacf * lfacf / chi + 1);
+  double D = Df * pow(chi, -(7. - 2. * P.k) / (4. - P.k));
+  *rho = D / lfac / P.rhoNorm;
+  *u = C_LIGHT * sqrt(1. - 1. / (lfac * lfac)) * lfac / P.vNorm;
+}
+
+template <class Cfg, int BS>
+struct TrackStep {
+  static constexpr int NQ = Cfg::NQ;
+  static constexpr int NQS = Cfg::NQ - 1;
+  static constexpr int NC = BS + 3;  // staged cells per chunk: a-1 .. a+BS+1
+
+  struct Smem {
+    double cp[NQS][NC];  // staged primitives
+    double cx[NC], cdx[NC];
+    double fl[NQS][BS + 1];  // interface fluxes; slot 0 = carry (interface a-1)
+    double lL[BS + 1], lR[BS + 1], v[BS + 1];
+    double xold[BS + 1], xnew[BS + 1], xcmb[BS + 1];
+    double red[BS / 32];
+    double edge[4];  // x, dx of the left and right edge cells this stage
+    int ints[4];
+  };
+
+  // --- helpers ------------------------------------------------------------
+
+  __device__ static double block_min(Smem &sm, double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sm.red[w] = v;
+    __syncthreads();
+    double r = sm.red[0];
+#pragma unroll
+    for (int k = 1; k < BS / 32; ++k) r = fmin(r, sm.red[k]);
+    __syncthreads();
+    return r;
+  }
+
+  __device__ static void load_prim(const Tracks &T, long long g, double *p) {
+#pragma unroll
+    for (int s = 0; s < NQS; ++s) p[Slots<Cfg>::q_of(s)] = T.prim[s * T.N + g];
+    p[UU2] = 0.;
+  }
+  __device__ static void store_prim(const Tracks &T, long long g, const double *p) {
+#pragma unroll
+    for (int s = 0; s < NQS; ++s) T.prim[s * T.N + g] = p[Slots<Cfg>::q_of(s)];
+  }
+
+  // Ghost cells and ghost interfaces (Grid::updateGhosts, 1d.cpp:217-246) and
+  // the problem's boundary hook.  ex/edx: geometry of the two edge cells.
+  __device__ static void ghosts(const Tracks &T, const Phys &ph, const RunParams &P, long long off, int n,
+                                const double *edge, double t) {
+    const int ng = ph.ngst, iL = ng - 1, iR = n - ng;
+    const int tid = threadIdx.x;
+    if (tid < 2 * ng) {
+      const bool left = tid < ng;
+      const int e = left ? iL + 1 : iR - 1;
+      const int i = left ? tid : iR + (tid - ng);
+      const long long ge = off + e, gi = off + i;
+      double p[NQ];
+      load_prim(T, ge, p);
+      const double ex = left ? edge[0] : edge[2];
+      const double edx = left ? edge[1] : edge[3];
+      if (Cfg::BM && left && t < P.t_bm_until) {
+        const double gx = ex - (iL - i + 1) * edx;
+        double rho, u, pp;
+        calc_bm(ph, P, gx, t, &rho, &u, &pp);
+        p[RHO] = rho;
+        p[UU1] = u;
+        p[PPP] = pp;
+        p[TR1] = 2.;
+      }
+      store_prim(T, gi, p);
+      T.dtl[gi] = T.dtl[ge];
+      if (Cfg::SHOCK) {
+        T.sd[gi] = T.sd[ge];
+        T.pspec[gi] = T.pspec[ge];
+        T.shocked[gi] = T.shocked[ge];
+      }
+    }
+    // ghost interfaces: left 0..iL-1 from iL+1; right iR..n-2 from iR-1
+    if (tid >= 32 && tid < 32 + ng) {
+      const int i = tid - 32;
+      if (i <= iL - 1) T.xI[off + i] = T.xI[off + iL + 1] - (iL - i + 1) * edge[1];
+      const int j = iR + i;
+      if (j <= n - 2) T.xI[off + j] = T.xI[off + iR - 1] + (j - iR) * edge[3];
+    }
+  }
+
+  // Geometry of cell i during the current stage.  Active cells: the step-start
+  // arrays (stage 1) or the span of their interfaces (stages 2, 3: set by
+  // Cell::move and CellGeomFromInterfacePos).  Ghosts: shifted copies of the
+  // edge cells (updateGhosts).
+  __device__ static void cell_geom(const Tracks &T, const Smem &sm, long long off, int n, int ng, int stage,
+                                   int i, const double *xIold_prev, double *gx, double *gdx) {
+    const int iL = ng - 1, iR = n - ng;
+    if (i <= iL) {
+      *gx = sm.edge[0] - (iL - i + 1) * sm.edge[1];
+      *gdx = sm.edge[1];
+    } else if (i >= iR) {
+      *gx = sm.edge[2] + (i - iR + 1) * sm.edge[3];
+      *gdx = sm.edge[3];
+    } else if (stage == 1) {
+      *gx = T.x[off + i];
+      *gdx = T.dx[off + i];
+    } else {
+      const double xL = xIold_prev ? *xIold_prev : T.xI[off + i - 1];
+      const double xR = T.xI[off + i];
+      *gx = (xR + xL) / 2.;
+      *gdx = (xR - xL);
+    }
+  }
+
+  // Reconstructed left/right states at interface i from staged cells
+  // (Grid::reconstructStates, 1d.cpp:370-461).  c = slot of cell i.
+  __device__ static void reconstruct(const Smem &sm, const Phys &ph, int i, int n, int c, double xI,
+                                     FState<Cfg> &L, FState<Cfg> &R) {
+    if (i == 0 || i == n - 2) {
+#pragma unroll
+      for (int s = 0; s < NQS; ++s) {
+        L.prim[Slots<Cfg>::q_of(s)] = sm.cp[s][c];
+        R.prim[Slots<Cfg>::q_of(s)] = sm.cp[s][c + 1];
+      }
+    } else {
+      const double cenLL = make_geom<Cfg>(sm.cx[c - 1], sm.cdx[c - 1]).cen;
+      const double cenL = make_geom<Cfg>(sm.cx[c], sm.cdx[c]).cen;
+      const double cenR = make_geom<Cfg>(sm.cx[c + 1], sm.cdx[c + 1]).cen;
+      const int cRR = (i + 2 < n - 1) ? c + 2 : c + 1 + ((n - 1) - (i + 1));
+      const double cenRR = make_geom<Cfg>(sm.cx[cRR], sm.cdx[cRR]).cen;
+#pragma unroll
+      for (int s = 0; s < NQS; ++s) {
+        const double qLL = sm.cp[s][c - 1], qL = sm.cp[s][c], qR = sm.cp[s][c + 1], qRR = sm.cp[s][cRR];
+        double gL = (qL - qLL) / (cenL - cenLL);
+        double gN = (qR - qL) / (cenR - cenL);
+        double gR = (qRR - qR) / (cenRR - cenR);
+        gL = minmod(gL, gN);
+        gR = minmod(gR, gN);
+        L.prim[Slots<Cfg>::q_of(s)] = qL + gL * (xI - cenL);
+        R.prim[Slots<Cfg>::q_of(s)] = qR + gR * (xI - cenR);
+      }
+    }
+    L.prim[UU2] = 0.;
+    R.prim[UU2] = 0.;
+    prim2cons<Cfg>(ph, L.prim, L.cons);
+    state2flux<Cfg>(L.prim, L.cons, L.flux);
+    prim2cons<Cfg>(ph, R.prim, R.cons);
+    state2flux<Cfg>(R.prim, R.cons, R.flux);
+  }
+
+  // Cell::update_dt, moving direction (cell.cpp:47-74).  Returns false on a
+  // negative candidate (the reference's exit(30)).
+  __device__ static bool dt_candidate(double a, double lR_left, double v_right, double lL_right, double v_left,
+                                      double *cand) {
+    double dL = (lR_left > v_right) ? a / (lR_left - v_right) : DT_INF;
+    double dR = (lL_right < v_left) ? a / (v_left - lL_right) : DT_INF;
+    *cand = fmin(dL, dR);
+    return !(*cand < 0);
+  }
+
+  // --- one stage sweep ------------------------------------------------------
+  // mode 0: stage-1 CFL candidates only (returns the run's min dt_loc and
+  //         resets dt_loc); mode 1: fluxes + update (+ RK combine for stage>1).
+  __device__ static double sweep(const Tracks &T, const Phys &ph, const RunParams &P, const SynchConst &sc,
+                                 Smem &sm, long long off, int n, int stage, int mode, double dt, double t,
+                                 StepStats &st) {
+    const int tid = threadIdx.x;
+    const int ng = ph.ngst, iL = ng - 1, iR = n - ng;
+    const double w0 = stage == 2 ? 3. / 4. : 1. / 3.;
+    const double w1 = stage == 2 ? 1. / 4. : 2. / 3.;
+    double run_min = DT_INF;
+
+    for (int a = 0; a < n; a += BS) {
+      // ---- stage cells a-1 .. a+BS+1 (slot k <-> cell a-1+k); slot 0 is carried
+      for (int k = tid + 1; k < NC; k += BS) {
+        const int i = a - 1 + k;
+        if (i < n) {
+          const long long g = off + i;
+#pragma unroll
+          for (int s = 0; s < NQS; ++s) sm.cp[s][k] = T.prim[s * T.N + g];
+          double gx, gdx;
+          // cell a's left interface was rewritten by the previous chunk: use its carried old position
+          cell_geom(T, sm, off, n, ng, stage, i, (k == 1 && a > 0) ? &sm.xold[0] : nullptr, &gx, &gdx);
+          sm.cx[k] = gx;
+          sm.cdx[k] = gdx;
+        }
+      }
+      __syncthreads();
+
+      // ---- interface i = a + tid
+      const int i = a + tid;
+      const bool has_if = i <= n - 2;
+      const int c = tid + 1;  // slot of cell i
+      double myflux[NQ];
+      double my_lL = 0, my_lR = 0, my_v = 0, my_xold = 0, my_xnew = 0, my_xcmb = 0;
+      if (has_if) {
+        FState<Cfg> L, R;
+        const double xI = T.xI[off + i];
+        my_xold = xI;
+        reconstruct(sm, ph, i, n, c, xI, L, R);
+        const Waves w = compute_lambda<Cfg>(ph, L, R);
+        double v = ph.vi * w.lS;
+        if (Cfg::BM) {  // userKinematics (BM1D.cpp:188-246)
+          if (i < ng) v = P.v_in;
+          if (i >= n - 1 - ng) v = P.v_out;
+        }
+        my_lL = w.lL;
+        my_lR = w.lR;
+        my_v = v;
+        if (mode == 1) {
+          hllc_flux<Cfg>(L, R, w, v, iface_area<Cfg>(xI), myflux);
+          if (Cfg::SHOCK) {  // measureShock into cell i (radiation_sph.cpp:160-175)
+            double Sd, ps;
+            const bool have = compute_Sd<Cfg>(ph, L, R, &Sd, &ps);
+            const long long g = off + i;
+            const double sd0 = fmax(T.sd[g], Sd);
+            T.sd[g] = sd0;
+            if (have && ps > T.pspec[g]) T.pspec[g] = ps;
+            if (stage == 1) T.shocked[g] = sd0 > DETECT_SHOCK_THRESHOLD ? 1 : 0;  // detectShock
+          }
+          // Interface::move, then the RK combine of interface positions
+          my_xnew = xI + dt * v;
+          if (stage == 1) {
+            T.xI0[off + i] = xI;
+            my_xcmb = my_xnew;
+          } else if (i >= iL && i <= iR - 1) {
+            my_xcmb = w0 * T.xI0[off + i] + w1 * my_xnew;
+          } else {
+            my_xcmb = my_xnew;
+          }
+          T.xI[off + i] = my_xcmb;
+        }
+      }
+      // cell n-1 has no interface of its own; as for every cell, the shock
+      // detector result of the last real interface is already in place.
+      sm.lL[tid + 1] = my_lL;
+      sm.lR[tid + 1] = my_lR;
+      sm.v[tid + 1] = my_v;
+      if (mode == 1) {
+        sm.xold[tid + 1] = my_xold;
+        sm.xnew[tid + 1] = my_xnew;
+        sm.xcmb[tid + 1] = my_xcmb;
+#pragma unroll
+        for (int s = 0; s < NQS; ++s) sm.fl[s][tid + 1] = myflux[Slots<Cfg>::q_of(s)];
+      }
+      __syncthreads();
+
+      // ---- cell i = a + tid
+      if (i < n) {
+        const long long g = off + i;
+        if (i >= 1 && i <= n - 2 && (mode == 0 || stage > 1)) {
+          double cand;
+          if (!dt_candidate(sm.cdx[c], sm.lR[tid], sm.v[tid + 1], sm.lL[tid + 1], sm.v[tid], &cand)) {
+            st.status = 30;
+            cand = DT_INF;
+          }
+          const double d = fmin(T.dtl[g], cand);
+          if (mode == 0) {
+            run_min = fmin(run_min, d);
+            T.dtl[g] = DT_INF;  // collect_dt resets (1d.cpp:785)
+          } else {
+            T.dtl[g] = d;
+          }
+        } else if (mode == 0) {
+          run_min = fmin(run_min, T.dtl[g]);
+          T.dtl[g] = DT_INF;
+        }
+
+        if (mode == 1 && i >= iL + 1 && i <= iR - 1) {
+          // Cell::update (cell.cpp:102-127)
+          double prim[NQ], cons[NQ];
+#pragma unroll
+          for (int s = 0; s < NQS; ++s) prim[Slots<Cfg>::q_of(s)] = sm.cp[s][c];
+          prim[UU2] = 0.;
+          const Geom G0 = make_geom<Cfg>(sm.cx[c], sm.cdx[c]);
+          prim2cons<Cfg>(ph, prim, cons);
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) cons[q] *= G0.dV;
+          if (stage == 1) {
+#pragma unroll
+            for (int s = 0; s < NQS; ++s) T.u0[s * T.N + g] = cons[Slots<Cfg>::q_of(s)];
+          }
+#pragma unroll
+          for (int s = 0; s < NQS; ++s) {
+            const int q = Slots<Cfg>::q_of(s);
+            cons[q] += (sm.fl[s][tid] - sm.fl[s][tid + 1]) * dt;
+          }
+          if (Cfg::SPH) {  // Cell::sourceTerms, 1D (rel_sph.cpp:452-466)
+            double p = prim[PPP];
+            double r = G0.x, dr = G0.dx, dV = G0.dV;
+            double r1 = r - dr / 2., r2 = r + dr / 2.;
+            double rsq = (r2 * r2 + r1 * r1 + r2 * r1) / 3.;
+            cons[SS1] += (2. * p) * (r / rsq) * dV * dt;
+          }
+          if (Cfg::SYNCH) {
+            const double dg = radiative_source<Cfg>(ph, sc, prim, G0.dV, dt);
+            cons[GMX] += dg;
+            cons[GMN] += dg;
+          }
+          const Geom G1 = geom_between<Cfg>(sm.xnew[tid], sm.xnew[tid + 1]);
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) cons[q] /= G1.dV;
+          C2PStats cs;
+          cons2prim<Cfg>(ph, cons, prim, &cs);
+          st.c2p_calls++;
+          st.c2p_iters += cs.iters;
+          st.c2p_fallbacks += cs.fallback;
+          st.c2p_max_iters = max(st.c2p_max_iters, cs.iters);
+          if (stage > 1) {  // RK3 combine (rk3.cpp:27-55, 63-92)
+#pragma unroll
+            for (int s = 0; s < NQS; ++s) {
+              const int q = Slots<Cfg>::q_of(s);
+              cons[q] = w0 * T.u0[s * T.N + g] + w1 * cons[q] * G1.dV;
+            }
+            const Geom G2 = geom_between<Cfg>(sm.xcmb[tid], sm.xcmb[tid + 1]);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) cons[q] /= G2.dV;
+            cons2prim<Cfg>(ph, cons, prim, &cs);
+            st.c2p_calls++;
+            st.c2p_iters += cs.iters;
+            st.c2p_fallbacks += cs.fallback;
+            st.c2p_max_iters = max(st.c2p_max_iters, cs.iters);
+          }
+          if (Cfg::SYNCH && stage == 3) {  // radiation_injectParticles, active cells
+            inject_particles<Cfg>(ph, sc, prim, T.shocked[g] != 0, T.pspec[g]);
+          }
+          store_prim(T, g, prim);
+        }
+      }
+      __syncthreads();
+      // ---- carry cell a+BS-1 and interface a+BS-1 to the next chunk
+      if (tid == 0) {
+        sm.lL[0] = sm.lL[BS];
+        sm.lR[0] = sm.lR[BS];
+        sm.v[0] = sm.v[BS];
+        sm.xold[0] = sm.xold[BS];
+        sm.xnew[0] = sm.xnew[BS];
+        sm.xcmb[0] = sm.xcmb[BS];
+        sm.cx[0] = sm.cx[BS];
+        sm.cdx[0] = sm.cdx[BS];
+      }
+      if (tid < NQS) {
+        sm.fl[tid][0] = sm.fl[tid][BS];
+        sm.cp[tid][0] = sm.cp[tid][BS];
+      }
+      __syncthreads();
+    }
+    return run_min;
+  }
+
+  // Edge-cell geometry for the current stage (written to sm.edge)
+  __device__ static void edge_geom(const Tracks &T, Smem &sm, long long off, int n, int ng, int stage) {
+    if (threadIdx.x == 0) {
+      const int e[2] = {ng, n - ng - 1};
+      for (int k = 0; k < 2; ++k) {
+        const long long g = off + e[k];
+        double gx, gdx;
+        if (stage == 1) {
+          gx = T.x[g];
+          gdx = T.dx[g];
+        } else {
+          const double xL = T.xI[g - 1], xR = T.xI[g];
+          gx = (xR + xL) / 2.;
+          gdx = (xR - xL);
+        }
+        sm.edge[2 * k] = gx;
+        sm.edge[2 * k + 1] = gdx;
+      }
+    }
+    __syncthreads();
+  }
+
+  // --- one full step of run r ---------------------------------------------
+  __device__ static void step(const Tracks &T, const Phys &ph, Smem &sm, uint32_t *words, int r, StepStats &st,
+                              bool regrid_only) {
+    const long long off = T.off[r];
+    const RunParams P = T.par[r];
+    const SynchConst sc{P.Nalpha, P.Nmp, P.Nme};
+    RunState &R = T.run[r];
+    int n = R.ntrack;
+    const double t = R.t;
+    const int ng = ph.ngst;
+
+    if (Cfg::BM) {
+      n = regrid_track<Cfg, BS>(T.prim, T.N, T.x, T.dx, T.dtl, T.xI, off, n, T.cap[r], ph, P, T.rg, words,
+                                st.splits, st.merges);
+      __syncthreads();
+    }
+    if (regrid_only) {
+      if (threadIdx.x == 0) R.ntrack = n;
+      __syncthreads();
+      return;
+    }
+    if (Cfg::SHOCK) {  // Cell::resetShock
+      for (int i = threadIdx.x; i < n; i += BS) {
+        T.sd[off + i] = -1.;
+        T.pspec[off + i] = 0.;
+        T.shocked[off + i] = 0;
+      }
+    }
+    __syncthreads();
+
+    // stage 1: ghosts, CFL candidates, dt
+    edge_geom(T, sm, off, n, ng, 1);
+    ghosts(T, ph, P, off, n, sm.edge, t);
+    __syncthreads();
+    double m = sweep(T, ph, P, sc, sm, off, n, 1, 0, 0., t, st);
+    m = block_min(sm, m);
+    const double dt = ph.cfl * m;
+    // stage 1 update
+    sweep(T, ph, P, sc, sm, off, n, 1, 1, dt, t, st);
+    __syncthreads();
+    // stage 2
+    edge_geom(T, sm, off, n, ng, 2);
+    ghosts(T, ph, P, off, n, sm.edge, t);
+    __syncthreads();
+    sweep(T, ph, P, sc, sm, off, n, 2, 1, dt, t, st);
+    __syncthreads();
+    // stage 3
+    edge_geom(T, sm, off, n, ng, 3);
+    ghosts(T, ph, P, off, n, sm.edge, t);
+    __syncthreads();
+    sweep(T, ph, P, sc, sm, off, n, 3, 1, dt, t, st);
+    __syncthreads();
+
+    // step-end cell geometry: ghosts 0 and n-1 keep the stage-3 ghost copies,
+    // cells 1..n-2 span their interfaces (CellGeomFromInterfacePos)
+    const int iL = ng - 1, iR = n - ng;
+    for (int i = threadIdx.x; i < n; i += BS) {
+      double gx, gdx;
+      if (i == 0 || i == n - 1) {
+        if (i == 0) {
+          gx = sm.edge[0] - (iL - i + 1) * sm.edge[1];
+          gdx = sm.edge[1];
+        } else {
+          gx = sm.edge[2] + (i - iR + 1) * sm.edge[3];
+          gdx = sm.edge[3];
+        }
+      } else {
+        const double xL = T.xI[off + i - 1], xR = T.xI[off + i];
+        gx = (xR + xL) / 2.;
+        gdx = (xR - xL);
+      }
+      T.x[off + i] = gx;
+      T.dx[off + i] = gdx;
+      // radiation_injectParticles on ghost cells (active cells did it in the sweep)
+      if (Cfg::SYNCH && (i <= iL || i >= iR)) {
+        double prim[NQ];
+        load_prim(T, off + i, prim);
+        inject_particles<Cfg>(ph, sc, prim, T.shocked[off + i] != 0, T.pspec[off + i]);
+        store_prim(T, off + i, prim);
+      }
+    }
+    if (st.status) R.status = st.status;  // any thread; every writer stores the same code
+    if (threadIdx.x == 0) {
+      R.ntrack = n;
+      R.dt = dt;
+      R.t = t + dt;
+      R.it = R.it + 1;
+    }
+    st.zone_updates += (unsigned long long)(n - 2 * ng);
+    __syncthreads();
+  }
+};
+
+template <class Cfg, int BS>
+__global__ void __launch_bounds__(BS) track_step_kernel(Tracks T, Phys ph, int nsteps, const int *order, int nruns,
+                                                         int *queue, StepStats *stats, int regrid_only) {
+  using TS = TrackStep<Cfg, BS>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  typename TS::Smem &sm = *reinterpret_cast<typename TS::Smem *>(smem_raw);
+  uint32_t *words = reinterpret_cast<uint32_t *>(smem_raw + sizeof(typename TS::Smem));
+  StepStats st{};
+  __shared__ int s_item, s_status;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= nruns) break;
+    const int r = order[item];
+    for (int k = 0; k < nsteps; ++k) {
+      // a run whose step failed stops (block-uniform test)
+      if (threadIdx.x == 0) s_status = T.run[r].status;
+      __syncthreads();
+      const int bad = s_status;
+      __syncthreads();
+      if (bad != 0) break;
+      TS::step(T, ph, sm, words, r, st, regrid_only != 0);
+    }
+  }
+  // fold the per-thread statistics into the launch totals
+  __syncthreads();
+  if (st.c2p_calls) {
+    atomicAdd(&stats->c2p_calls, st.c2p_calls);
+    atomicAdd(&stats->c2p_iters, st.c2p_iters);
+    atomicAdd(&stats->c2p_fallbacks, st.c2p_fallbacks);
+    atomicMax(&stats->c2p_max_iters, st.c2p_max_iters);
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(&stats->zone_updates, st.zone_updates);
+    if (st.splits) atomicAdd(&stats->splits, st.splits);
+    if (st.merges) atomicAdd(&stats->merges, st.merges);
+  }
+  if (st.status) atomicMax(&stats->status, st.status);
+}
+
+}  // namespace gb

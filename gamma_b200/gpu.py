@@ -1,0 +1,219 @@
+"""ctypes binding of the C ABI in include/gamma_gpu.h (gamma_b200/lib/libgamma_b200.so).
+
+There is no CPU fallback: importing works everywhere, but creating a context
+raises if the library is missing or no sm_100 device is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgamma_b200.so")
+
+GAMMA_OK = 0
+GAMMA_ERR_INVALID = -1
+GAMMA_ERR_CUDA = -2
+GAMMA_ERR_CAPACITY = -3
+GAMMA_ERR_NO_DEVICE = -4
+GAMMA_ERR_NEG_DT = -30
+
+GEOM_SPHERICAL1D, GEOM_CARTESIAN = 0, 1
+HYDRO_REL_SPH, HYDRO_REL_CART = 0, 1
+EOS_IDEAL, EOS_SYNGE = 0, 1
+PROBLEM_BM1D, PROBLEM_TUBE = 0, 1
+
+# every symbol include/gamma_gpu.h declares
+EXPORTS = (
+    "gamma_gpu_create", "gamma_gpu_layout", "gamma_gpu_set_params", "gamma_gpu_upload", "gamma_gpu_step",
+    "gamma_gpu_regrid",
+    "gamma_gpu_download", "gamma_gpu_cons2prim", "gamma_gpu_stream", "gamma_gpu_strerror",
+    "gamma_gpu_last_error", "gamma_gpu_destroy",
+)
+
+
+class GammaError(RuntimeError):
+    def __init__(self, code: int, detail: str = ""):
+        self.code = code
+        super().__init__(f"{strerror(code)} ({code}){': ' + detail if detail else ''}")
+
+
+class Config(ctypes.Structure):
+    """gamma_config_t"""
+
+    _fields_ = [(n, ctypes.c_int) for n in ("geometry", "hydro", "eos", "nq", "shock_detection",
+                                             "local_synchrotron", "problem", "ngst")] + \
+               [(n, ctypes.c_double) for n in ("gamma_ad", "cfl", "vi")]
+
+
+class RunParams(ctypes.Structure):
+    """gamma_run_params_t"""
+
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "Etot", "n_ext", "eta", "k", "Rscale", "rhoNorm", "pNorm", "lNorm", "vNorm", "dth", "target_ar",
+        "split_AR", "merge_AR", "t_bm_until", "v_in", "v_out", "Nalpha", "Nmp", "Nme")]
+
+
+class StepStats(ctypes.Structure):
+    """gamma_step_stats_t"""
+
+    _fields_ = [(n, ctypes.c_ulonglong) for n in ("c2p_calls", "c2p_iters", "c2p_fallbacks", "zone_updates",
+                                                  "splits", "merges")] + \
+               [("c2p_max_iters", ctypes.c_int), ("status", ctypes.c_int), ("device_ms", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
+def config_sph(gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=EOS_IDEAL) -> Config:
+    """spherical1D + rel_sph + radiation_sph, shock detection and local synchrotron (NUM_Q = 10)."""
+    return Config(GEOM_SPHERICAL1D, HYDRO_REL_SPH, eos, 10, 1, 1, PROBLEM_BM1D, 2, gamma_ad, cfl, vi)
+
+
+def config_cart(gamma_ad=5. / 3., cfl=0.2, vi=1.0) -> Config:
+    """cartesian + rel_cart, no shock detection or synchrotron (NUM_Q = 6)."""
+    return Config(GEOM_CARTESIAN, HYDRO_REL_CART, EOS_IDEAL, 6, 0, 0, PROBLEM_TUBE, 2, gamma_ad, cfl, vi)
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_lp = ctypes.POINTER(ctypes.c_longlong)
+_LIB = None
+
+
+def lib() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+                                    f"(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.gamma_gpu_create.argtypes = [ctypes.POINTER(Config), ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_void_p)]
+        L.gamma_gpu_layout.argtypes = [ctypes.c_void_p, _lp, _lp]
+        L.gamma_gpu_set_params.argtypes = [ctypes.c_void_p, ctypes.POINTER(RunParams)]
+        L.gamma_gpu_upload.argtypes = [ctypes.c_void_p, _ip, _dp, _lp, _dp, _dp, _dp, _dp, _dp]
+        L.gamma_gpu_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StepStats)]
+        L.gamma_gpu_regrid.argtypes = [ctypes.c_void_p, ctypes.POINTER(StepStats)]
+        L.gamma_gpu_download.argtypes = [ctypes.c_void_p, _ip, _dp, _dp, _lp, _ip, _dp, _dp, _dp, _dp, _dp]
+        L.gamma_gpu_cons2prim.argtypes = [ctypes.POINTER(Config), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.c_void_p]
+        L.gamma_gpu_stream.restype = ctypes.c_void_p
+        L.gamma_gpu_stream.argtypes = [ctypes.c_void_p]
+        L.gamma_gpu_strerror.restype = ctypes.c_char_p
+        L.gamma_gpu_strerror.argtypes = [ctypes.c_int]
+        L.gamma_gpu_last_error.restype = ctypes.c_char_p
+        L.gamma_gpu_last_error.argtypes = [ctypes.c_void_p]
+        L.gamma_gpu_destroy.argtypes = [ctypes.c_void_p]
+        for name in ("gamma_gpu_create", "gamma_gpu_layout", "gamma_gpu_set_params", "gamma_gpu_upload",
+                     "gamma_gpu_step", "gamma_gpu_regrid", "gamma_gpu_download", "gamma_gpu_cons2prim"):
+            getattr(L, name).restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def strerror(code: int) -> str:
+    return lib().gamma_gpu_strerror(int(code)).decode()
+
+
+def _p(a, typ=_dp):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(typ)
+
+
+class GammaGPU:
+    """One context: nruns independent tracks on the current CUDA device."""
+
+    def __init__(self, cfg: Config, capacities):
+        self.cfg = cfg
+        self.nq = cfg.nq
+        caps = np.ascontiguousarray(capacities, dtype=np.int32)
+        self.nruns = caps.size
+        self.cap = caps
+        h = ctypes.c_void_p()
+        rc = lib().gamma_gpu_create(ctypes.byref(cfg), self.nruns, _p(caps, _ip), ctypes.byref(h))
+        if rc != GAMMA_OK:
+            raise GammaError(rc)
+        self.h = h
+        offs = np.zeros(self.nruns, dtype=np.int64)
+        tot = ctypes.c_longlong()
+        lib().gamma_gpu_layout(self.h, _p(offs, _lp), ctypes.byref(tot))
+        self.offsets = offs
+        self.total = int(tot.value)
+
+    def _check(self, rc):
+        if rc != GAMMA_OK:
+            raise GammaError(rc, lib().gamma_gpu_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gamma_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def stream(self) -> int:
+        return lib().gamma_gpu_stream(self.h)
+
+    def set_params(self, params):
+        arr = (RunParams * self.nruns)(*params)
+        self._check(lib().gamma_gpu_set_params(self.h, arr))
+
+    def upload(self, ntrack, prim, x, dx, xI, dt_loc=None, t=None, it=None):
+        nt = np.ascontiguousarray(ntrack, dtype=np.int32)
+        tt = None if t is None else np.ascontiguousarray(t, dtype=np.float64)
+        ii = None if it is None else np.ascontiguousarray(it, dtype=np.int64)
+        self._check(lib().gamma_gpu_upload(self.h, _p(nt, _ip), _p(tt), _p(ii, _lp), _p(prim), _p(x), _p(dx),
+                                           _p(dt_loc), _p(xI)))
+
+    def upload_ptrs(self, ntrack, t, it, prim_ptr, x_ptr, dx_ptr, dtl_ptr, xI_ptr):
+        """Upload from raw host addresses (e.g. pinned torch tensors)."""
+        nt = np.ascontiguousarray(ntrack, dtype=np.int32)
+        tt = np.ascontiguousarray(t, dtype=np.float64)
+        ii = np.ascontiguousarray(it, dtype=np.int64)
+        c = lambda v: ctypes.cast(ctypes.c_void_p(v), _dp) if v else None
+        self._check(lib().gamma_gpu_upload(self.h, _p(nt, _ip), _p(tt), _p(ii, _lp), c(prim_ptr), c(x_ptr),
+                                           c(dx_ptr), c(dtl_ptr), c(xI_ptr)))
+
+    def step(self, nsteps: int = 1, stats: bool = True):
+        st = StepStats()
+        self._check(lib().gamma_gpu_step(self.h, int(nsteps), ctypes.byref(st) if stats else None))
+        return st.as_dict() if stats else None
+
+    def regrid(self):
+        st = StepStats()
+        self._check(lib().gamma_gpu_regrid(self.h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def download(self) -> dict:
+        R, N = self.nruns, self.total
+        out = dict(ntrack=np.zeros(R, np.int32), t=np.zeros(R), dt=np.zeros(R), it=np.zeros(R, np.int64),
+                   status=np.zeros(R, np.int32), prim=np.zeros((self.nq, N)), x=np.zeros(N), dx=np.zeros(N),
+                   dt_loc=np.zeros(N), xI=np.zeros(N))
+        self._check(lib().gamma_gpu_download(
+            self.h, _p(out["ntrack"], _ip), _p(out["t"]), _p(out["dt"]), _p(out["it"], _lp), _p(out["status"], _ip),
+            _p(out["prim"]), _p(out["x"]), _p(out["dx"]), _p(out["dt_loc"]), _p(out["xI"])))
+        return out
+
+    def download_ptrs(self, prim_ptr, x_ptr=None, dx_ptr=None, dtl_ptr=None, xI_ptr=None):
+        R = self.nruns
+        nt = np.zeros(R, np.int32)
+        c = lambda v: ctypes.cast(ctypes.c_void_p(v), _dp) if v else None
+        self._check(lib().gamma_gpu_download(self.h, _p(nt, _ip), None, None, None, None, c(prim_ptr), c(x_ptr),
+                                             c(dx_ptr), c(dtl_ptr), c(xI_ptr)))
+        return nt
+
+
+def cons2prim_device(cfg: Config, cons_ptr: int, prim_ptr: int, n: int, iters_ptr: int = 0, stream: int = 0):
+    """FluidState::cons2prim on device arrays [nq][n] (raw CUDA pointers)."""
+    rc = lib().gamma_gpu_cons2prim(ctypes.byref(cfg), ctypes.c_void_p(cons_ptr), ctypes.c_void_p(prim_ptr), int(n),
+                                   ctypes.c_void_p(iters_ptr) if iters_ptr else None,
+                                   ctypes.c_void_p(stream) if stream else None)
+    if rc != GAMMA_OK:
+        raise GammaError(rc)

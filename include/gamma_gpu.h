@@ -1,0 +1,146 @@
+/*
+ * gamma_gpu.h -- C ABI of the B200 moving-mesh relativistic hydro step.
+ *
+ * The GAMMA reference has no FFI: its "operator API" is the C++ class surface
+ * (Grid / Cell / FluidState / Interface) with module bodies picked at link
+ * time (Makefile:1-8, 82-92).  This header is the boundary a replacement of that
+ * path binds: plain pointers and sizes, status codes, no C++ or torch types.
+ * Each entry point names the reference member(s) it stands in for.
+ *
+ * Data model.  A context holds the physics configuration (the reference's
+ * compile-time switches, src/environment.h:46-66) and nruns independent runs.
+ * Each run is one 1D track of cells (Grid::Ctot / Grid::Itot of
+ * src/Dimensions/1d.cpp) with its own time, time step and cell count.  Run r
+ * owns cells [offset[r], offset[r] + capacity[r]) of every per-cell array;
+ * the host arrays passed to upload/download use exactly that layout, so each
+ * field moves in one copy:
+ *   prim    [nq][total]   primitive variables (FluidState::prim slots,
+ *                         src/environment.h:33-82; slot 3 is zero in 1D)
+ *   x, dx   [total]       cell centre and width (s_cell_geometry x, dx)
+ *   dt_loc  [total]       Cell::dt_loc (carried between steps, cell.cpp:97)
+ *   xI      [total]       interface i between cells i and i+1 (Interface::x)
+ * Cells [0, ngst) and [ntrack-ngst, ntrack) of a run are its ghost cells.
+ *
+ * Errors: every call returns GAMMA_OK (0) or a negative code;
+ * gamma_gpu_strerror gives its text and gamma_gpu_last_error the detail of the
+ * last failure on a context.  A context is used by one host thread at a time
+ * and runs its work on its own CUDA stream.
+ */
+#ifndef GAMMA_GPU_H
+#define GAMMA_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GAMMA_OK 0
+#define GAMMA_ERR_INVALID (-1)     /* bad argument or unsupported module combination */
+#define GAMMA_ERR_CUDA (-2)        /* a CUDA call failed; see gamma_gpu_last_error */
+#define GAMMA_ERR_CAPACITY (-3)    /* a track does not fit its capacity */
+#define GAMMA_ERR_NO_DEVICE (-4)   /* no usable sm_100 device */
+#define GAMMA_ERR_NEG_DT (-30)     /* a CFL candidate was negative: the reference exit(30)s (cell.cpp:70-73) */
+
+enum { GAMMA_GEOM_SPHERICAL1D = 0, GAMMA_GEOM_CARTESIAN = 1 };
+enum { GAMMA_HYDRO_REL_SPH = 0, GAMMA_HYDRO_REL_CART = 1 };
+enum { GAMMA_EOS_IDEAL = 0, GAMMA_EOS_SYNGE = 1 };
+enum { GAMMA_PROBLEM_BM1D = 0, GAMMA_PROBLEM_TUBE = 1 };
+
+/* Module selection and switches (Makefile GEOMETRY/HYDRO/RADIATION/INITIAL,
+ * environment.h GAMMA_, EOS_, CFL_, VI, SHOCK_DETECTION_, LOCAL_SYNCHROTRON_).
+ * Supported combinations:
+ *   spherical1D + rel_sph + shock detection + local synchrotron (nq = 10), BM1D hooks
+ *   cartesian   + rel_cart, no shock detection, no synchrotron   (nq = 6),  no hooks */
+typedef struct {
+  int geometry;
+  int hydro;
+  int eos;
+  int nq;
+  int shock_detection;
+  int local_synchrotron;
+  int problem;
+  int ngst;
+  double gamma_ad;
+  double cfl;
+  double vi;
+} gamma_config_t;
+
+/* Per-run parameters of the Blandford-McKee problem hooks
+ * (src/Initial/Tests/BM1D.cpp: calcBM 62-86, userKinematics 188-246,
+ * userBoundaries 254-274, checkCellForRegrid 277-319) and the normalised
+ * synchrotron constants (src/constants.cpp:12-20).  Ignored by tubes. */
+typedef struct {
+  double Etot, n_ext, eta, k, Rscale;
+  double rhoNorm, pNorm, lNorm, vNorm;
+  double dth, target_ar, split_AR, merge_AR;
+  double t_bm_until, v_in, v_out;
+  double Nalpha, Nmp, Nme;
+} gamma_run_params_t;
+
+typedef struct {
+  unsigned long long c2p_calls;      /* FluidState::cons2prim calls */
+  unsigned long long c2p_iters;      /* Newton iterations over those calls */
+  unsigned long long c2p_fallbacks;  /* calls that hit the iteration cap */
+  unsigned long long zone_updates;   /* sum over steps of active cells */
+  unsigned long long splits, merges; /* regrid actions */
+  int c2p_max_iters;
+  int status;                        /* 0 or the first failing run's GAMMA_ERR_* */
+  float device_ms;                   /* device time of the step launch(es) */
+} gamma_step_stats_t;
+
+typedef struct gamma_ctx gamma_ctx_t;
+
+/* Allocate device state for nruns tracks of the given capacities (cells,
+ * ghosts included: Grid::nde_nax = nmax + 2 ngst, 1d.cpp:60).
+ * Replaces Grid::initialise (1d.cpp:53-81). */
+int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *capacity, gamma_ctx_t **out);
+
+/* offsets[r] of each run in the pooled arrays and the total length. */
+int gamma_gpu_layout(const gamma_ctx_t *ctx, long long *offsets, long long *total);
+
+/* Problem parameters, one record per run. */
+int gamma_gpu_set_params(gamma_ctx_t *ctx, const gamma_run_params_t *params);
+
+/* Host -> device state of every run (mpi_distribute + prepForRun leave this
+ * state in the reference, 1d.cpp:956-969, grid.cpp:20-26).  t[r], it[r]:
+ * Simu::t and Simu::it.  Pinned host memory makes the copies asynchronous. */
+int gamma_gpu_upload(gamma_ctx_t *ctx, const int *ntrack, const double *t, const long long *it,
+                     const double *prim, const double *x, const double *dx, const double *dt_loc,
+                     const double *xI);
+
+/* Advance every run by nsteps iterations of the Simu::run loop body
+ * (src/simu.cpp:79-105: regrid, resetShock, updateGhosts, prepForUpdate,
+ * detectShock, collect_dt, Grid::evolve (rk3.cpp:13-95), injectParticles),
+ * each run with its own dt.  With stats == NULL the call only enqueues the
+ * work; otherwise it waits and fills stats. */
+int gamma_gpu_step(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats);
+
+/* Grid::regrid alone (1d.cpp:484-557 with the problem's checkCellForRegrid):
+ * split / merge every run once, as the first phase of gamma_gpu_step does.
+ * A no-op for problems without a refinement criterion (tubes). */
+int gamma_gpu_regrid(gamma_ctx_t *ctx, gamma_step_stats_t *stats);
+
+/* Device -> host state (waits for the context's stream).  Any pointer may be
+ * NULL.  status[r]: 0 or GAMMA_ERR_NEG_DT for a run stopped by a negative CFL
+ * candidate. */
+int gamma_gpu_download(gamma_ctx_t *ctx, int *ntrack, double *t, double *dt, long long *it, int *status,
+                       double *prim, double *x, double *dx, double *dt_loc, double *xI);
+
+/* FluidState::cons2prim (rel_sph.cpp:213-320 / rel_cart.cpp:125-229) on n
+ * independent states, DEVICE pointers, layout [nq][n]; prim holds the previous
+ * primitives (pressure warm start) on entry, cons is rewritten by the closing
+ * prim2cons as in the reference.  iters (may be NULL): Newton iterations per
+ * state.  stream: a cudaStream_t, or NULL for the default stream. */
+int gamma_gpu_cons2prim(const gamma_config_t *cfg, double *cons, double *prim, int n, int *iters, void *stream);
+
+/* The context's CUDA stream (a cudaStream_t). */
+void *gamma_gpu_stream(gamma_ctx_t *ctx);
+
+const char *gamma_gpu_strerror(int code);
+const char *gamma_gpu_last_error(const gamma_ctx_t *ctx);
+void gamma_gpu_destroy(gamma_ctx_t *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

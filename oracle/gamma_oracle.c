@@ -233,7 +233,7 @@ static int cons2prim(const oc_sim *s, fstate *St, double r, double pin) {
         res = b.b;
         p_lo = b.lower;
         p_hi = b.upper;
-        cont = oracle_brent_continue(p_lo, p_hi, 0., 1.e-13);
+        cont = oracle_brent_continue(p_lo, p_hi, 0., s->c.c2p_epsrel);
       } while (cont && iter < max_iter);
       pCand = res;
     }
@@ -1086,6 +1086,7 @@ void oc_config_bm1d_defaults(oc_config *c) {
   c->t_bm_until = 1.e7;
   c->v_in = 0.;
   c->v_out = 1.5;
+  c->c2p_epsrel = 1.e-13;
 }
 
 void oc_config_tube_defaults(oc_config *c) {
@@ -1114,6 +1115,7 @@ void oc_config_tube_defaults(oc_config *c) {
   c->pR = 1.e-7;
   c->vR = 0.;
   c->trR = 2.;
+  c->c2p_epsrel = 1.e-13;
 }
 
 oc_sim *oc_create(const oc_config *cfg) {

@@ -47,6 +47,9 @@ typedef struct {
   double grid_log, r_lo, r_hi, dth, target_ar, split_AR, merge_AR, t_bm_until, v_in, v_out;
   /* planar tube */
   double xmin, xmax, xmid, rhoL, pL, vL, trL, rhoR, pR, vR, trR;
+  /* relative bracket width at which the pressure root search stops: 1e-13 in
+   * the reference (rel_sph.cpp:281); smaller values give a tighter oracle */
+  double c2p_epsrel;
 } oc_config;
 
 typedef struct oc_sim oc_sim;

@@ -35,7 +35,7 @@ class OcConfig(ctypes.Structure):
                                           "grid_log", "r_lo", "r_hi", "dth", "target_ar", "split_AR",
                                           "merge_AR", "t_bm_until", "v_in", "v_out",
                                           "xmin", "xmax", "xmid", "rhoL", "pL", "vL", "trL",
-                                          "rhoR", "pR", "vR", "trR")]
+                                          "rhoR", "pR", "vR", "trR", "c2p_epsrel")]
     )
 
 
