@@ -75,6 +75,7 @@ int check_cfg(const gamma_config_t *cfg, int *kind) {
 gb::Phys phys_of(const gamma_config_t &c) {
   gb::Phys p;
   p.gamma_ad = c.gamma_ad;
+  p.kgam = c.gamma_ad / (c.gamma_ad - 1.);
   p.cfl = c.cfl;
   p.vi = c.vi;
   p.eos = c.eos;
@@ -121,7 +122,7 @@ __global__ void cons2prim_kernel(gb::Phys ph, double *cons, double *prim, int n,
       p[q] = prim[(long long)q * n + k];
     }
     gb::C2PStats st;
-    gb::cons2prim<Cfg>(ph, c, p, &st);
+    gb::cons2prim<Cfg>(ph, c, p, &st);  // warm start from prim[PPP]
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
       cons[(long long)q * n + k] = c[q];
@@ -218,6 +219,8 @@ GAMMA_API int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *
   GB_ALLOC(T.xI, N * d);
   GB_ALLOC(T.u0, nqs * N * d);
   GB_ALLOC(T.xI0, N * d);
+  GB_ALLOC(T.fl1, nqs * N * d);
+  GB_ALLOC(T.v1, N * d);
   if (kind == KIND_SPH) {
     GB_ALLOC(T.sd, N * d);
     GB_ALLOC(T.pspec, N * d);

@@ -44,8 +44,20 @@ constexpr double DT_INF = 1.e15;
 // Module selections (the reference's Makefile GEOMETRY/HYDRO/RADIATION slots and
 // environment.h switches) as compile-time policies.
 
+// Arithmetic form.  0 (default): every formula in the reference's operation
+// order, so a state, flux or wave speed computed from the same inputs is bit
+// for bit the reference's.  1: divisions by a shared denominator become one
+// reciprocal and multiplications (about half the FP64 instructions of the
+// step); results then move at the ulp level, which the reference's own
+// cold-gas conditioning (lambda* from a near-cancelling quadratic) amplifies.
+#ifndef GB_FAST_ARITH
+#define GB_FAST_ARITH 0
+#endif
+
 // cartesian + rel_cart, ideal gas, no shock detection / synchrotron: NUM_Q = 6.
 struct CfgCart {
+  static constexpr bool FAST = GB_FAST_ARITH;
+  static constexpr int MIN_BLOCKS = 4;  // 128-thread CTAs per SM: caps registers at 128
   static constexpr int NQ = 6;
   static constexpr bool SPH = false;    // rel_sph hydro and spherical1D geometry
   static constexpr bool SHOCK = false;  // SHOCK_DETECTION_
@@ -55,6 +67,8 @@ struct CfgCart {
 
 // spherical1D + rel_sph + radiation_sph: NUM_Q = 10.
 struct CfgSph {
+  static constexpr bool FAST = GB_FAST_ARITH;
+  static constexpr int MIN_BLOCKS = 1;
   static constexpr int NQ = 10;
   static constexpr bool SPH = true;
   static constexpr bool SHOCK = true;
@@ -65,6 +79,7 @@ struct CfgSph {
 // Run-time constants shared by every run of a context.
 struct Phys {
   double gamma_ad;  // GAMMA_
+  double kgam;      // GAMMA_ / (GAMMA_ - 1), the enthalpy factor of the ideal EOS
   double cfl;       // CFL_
   double vi;        // VI
   int eos;          // 0 ideal, 1 Synge / Taub-Mathews (rel_sph.cpp:37-52)
@@ -76,12 +91,15 @@ struct Prim {
   double v[Cfg::NQ];
 };
 
-// FluidState: primitive, conserved and physical flux of one state.
+// FluidState: primitive, conserved and physical flux of one state, with its
+// Lorentz factor and 3-velocity cached (FluidState::lfac is called many times
+// per interface in the reference).
 template <class Cfg>
 struct FState {
   double prim[Cfg::NQ];
   double cons[Cfg::NQ];
   double flux[Cfg::NQ];
+  double lfac, v;
 };
 
 GB_HD double lfac_of(double uu) {
@@ -106,6 +124,16 @@ GB_HD double state_gamma(const Phys &ph, const double *prim) {
   return Cfg::SPH ? eos_gamma(ph, prim[RHO], prim[PPP]) : ph.gamma_ad;
 }
 
+// gamma/(gamma-1) of a state: cached for the ideal EOS
+template <class Cfg>
+GB_HD double enth_k(const Phys &ph, const double *prim) {
+  if (Cfg::SPH && ph.eos != 0) {
+    const double g = eos_gamma(ph, prim[RHO], prim[PPP]);
+    return g / (g - 1.);
+  }
+  return ph.kgam;
+}
+
 // prim2cons (rel_sph.cpp:55-82, rel_cart.cpp:37-64)
 template <class Cfg>
 GB_HD void prim2cons(const Phys &ph, const double *prim, double *cons) {
@@ -113,8 +141,13 @@ GB_HD void prim2cons(const Phys &ph, const double *prim, double *cons) {
   double p = prim[PPP];
   double uu = prim[UU1];
   double lfac = lfac_of(uu);
-  double gma = state_gamma<Cfg>(ph, prim);
-  double h = 1. + p * gma / (gma - 1.) / rho;
+  double h;
+  if (Cfg::FAST) {
+    h = 1. + enth_k<Cfg>(ph, prim) * p / rho;
+  } else {
+    const double gma = state_gamma<Cfg>(ph, prim);
+    h = 1. + p * gma / (gma - 1.) / rho;
+  }
   double D = lfac * rho;
   double tau = D * h * lfac - p - D;
   double ss = D * h * uu;
@@ -124,6 +157,43 @@ GB_HD void prim2cons(const Phys &ph, const double *prim, double *cons) {
   cons[SS2] = 0.;
 #pragma unroll
   for (int t = TR1; t < Cfg::NQ; ++t) cons[t] = prim[t] * D;
+}
+
+// prim2cons + state2flux of a reconstructed or cell state in one pass
+// (rel_sph.cpp:55-113): lfac and v = u/lfac are formed once.
+template <class Cfg>
+GB_HD void state2flux(const double *prim, const double *cons, double *flux);
+
+template <class Cfg>
+GB_HD void fill_state(const Phys &ph, FState<Cfg> &S) {
+  if (!Cfg::FAST) {
+    prim2cons<Cfg>(ph, S.prim, S.cons);
+    state2flux<Cfg>(S.prim, S.cons, S.flux);
+    S.lfac = lfac_of(S.prim[UU1]);
+    S.v = S.prim[UU1] / S.lfac;
+    return;
+  }
+  const double rho = S.prim[RHO], p = S.prim[PPP], uu = S.prim[UU1];
+  const double lfac = sqrt(1. + uu * uu);
+  const double v = uu / lfac;
+  const double h = 1. + enth_k<Cfg>(ph, S.prim) * p / rho;
+  const double D = lfac * rho;
+  const double Dh = D * h;
+  S.lfac = lfac;
+  S.v = v;
+  S.cons[DEN] = D;
+  S.cons[TAU] = Dh * lfac - p - D;
+  S.cons[SS1] = Dh * uu;
+  S.cons[SS2] = 0.;
+  S.flux[DEN] = D * v;
+  S.flux[SS1] = S.cons[SS1] * v + p;
+  S.flux[SS2] = 0.;
+  S.flux[TAU] = S.cons[SS1] - D * v;
+#pragma unroll
+  for (int t = TR1; t < Cfg::NQ; ++t) {
+    S.cons[t] = S.prim[t] * D;
+    S.flux[t] = S.cons[t] * v;
+  }
 }
 
 // state2flux (rel_sph.cpp:85-113, rel_cart.cpp:67-95)
@@ -152,50 +222,67 @@ struct C2PStats {
   int fallback;  // 1 if the iteration cap was hit (bisection-limited)
 };
 
+// f(p) = E + p - D lfac - k p lfac^2 with lfac = (1 - S^2/(E+p)^2)^(-1/2)
+// (rel_sph.cpp:191-210 takes |1 - S^2/W^2|, rel_cart.cpp:108-123 does not).
+// Returns f; with df != nullptr also df/dp and lfac^2.  For the Synge EOS the
+// derivative of Gamma_eff is included through rho = D/lfac and a = p/rho/(G-1).
 template <class Cfg>
-GB_HD double c2p_f(const Phys &ph, double p, double D, double S, double E) {
-  if (Cfg::SPH) {
-    double lfac = 1. / sqrt(fabs(1. - (S * S) / ((E + p) * (E + p))));
-    double gma = eos_gamma(ph, D / lfac, p);
-    return (E + p - D * lfac - (gma * p * lfac * lfac) / (gma - 1.));
-  } else {
-    double g = ph.gamma_ad;
-    double lfac = 1. / sqrt(1. - (S * S) / ((E + p) * (E + p)));
-    return (E + p - D * lfac - (g * p * lfac * lfac) / (g - 1.));
-  }
-}
-
-// f and df/dp.  For the Synge EOS the derivative of Gamma_eff is included
-// through rho = D/lfac(p) and a = p/rho/(G-1).
-template <class Cfg>
-GB_HD double c2p_f_df(const Phys &ph, double p, double D, double S, double E, double *df) {
+GB_HD double c2p_f(const Phys &ph, double p, double D, double S2, double E, double *df = nullptr,
+                   double *l2out = nullptr) {
   const double W = E + p;
-  const double x = (S * S) / (W * W);
+  const double rW = 1. / W;
+  const double x = S2 * rW * rW;
   const double arg = Cfg::SPH ? fabs(1. - x) : (1. - x);
-  const double lfac = 1. / sqrt(arg);
-  // d(lfac)/dp = -lfac^3 S^2 / W^3 (sign flips with fabs when x > 1)
-  const double sgn = (1. - x) >= 0. ? 1. : -1.;
-  const double dl = -sgn * lfac * lfac * lfac * x / W;
-  double gma, dgma;
+  const double lfac = rsqrt(arg);
+  const double l2 = lfac * lfac;
+  double k, dk = 0.;
   if (Cfg::SPH && ph.eos != 0) {
     const double G = ph.gamma_ad;
     const double rho = D / lfac;
     const double a = p / rho / (G - 1.);
     const double sq = sqrt(a * a + 1.);
     const double e = a + sq;
-    gma = G - (G - 1.) / 2. * (1. - 1. / (e * e));
-    // a = p lfac / (D (G-1)); da/dp = (lfac + p dl) / (D (G-1))
-    const double da = (lfac + p * dl) / (D * (G - 1.));
-    const double de = da * (1. + a / sq);
-    dgma = -(G - 1.) / (e * e * e) * de;
+    const double gma = G - (G - 1.) / 2. * (1. - 1. / (e * e));
+    k = gma / (gma - 1.);
+    if (df) {
+      const double sgn = (1. - x) >= 0. ? 1. : -1.;
+      const double dl = -sgn * lfac * l2 * x * rW;
+      const double da = (lfac + p * dl) / (D * (G - 1.));
+      const double dgma = -(G - 1.) / (e * e * e) * (da * (1. + a / sq));
+      dk = -dgma / ((gma - 1.) * (gma - 1.));
+    }
   } else {
-    gma = ph.gamma_ad;
-    dgma = 0.;
+    k = ph.kgam;
   }
-  const double k = gma / (gma - 1.);
-  const double dk = -dgma / ((gma - 1.) * (gma - 1.));
+  const double f = W - D * lfac - k * p * l2;
+  if (df) {
+    const double sgn = (1. - x) >= 0. ? 1. : -1.;
+    const double dl = -sgn * lfac * l2 * x * rW;
+    *df = 1. - D * dl - dk * p * l2 - k * (l2 + 2. * p * lfac * dl);
+  }
+  if (l2out) *l2out = l2;
+  return f;
+}
+
+// f in the reference's operation order (rel_sph.cpp:198-207, rel_cart.cpp:118-120),
+// with df/dp and lfac^2 on request.
+template <class Cfg>
+GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, double *df = nullptr,
+                       double *l2out = nullptr) {
+  const double W = E + p;
+  const double x = (S * S) / (W * W);
+  const double arg = Cfg::SPH ? fabs(1. - x) : (1. - x);
+  const double lfac = 1. / sqrt(arg);
+  double gma;
+  if (Cfg::SPH) gma = eos_gamma(ph, D / lfac, p);
+  else gma = ph.gamma_ad;
   const double f = (E + p - D * lfac - (gma * p * lfac * lfac) / (gma - 1.));
-  *df = 1. - D * dl - dk * p * lfac * lfac - k * (lfac * lfac + 2. * p * lfac * dl);
+  if (df) {
+    double dfast;
+    c2p_f<Cfg>(ph, p, D, S * S, E, &dfast);
+    *df = dfast;
+  }
+  if (l2out) *l2out = lfac * lfac;
   return f;
 }
 
@@ -210,15 +297,18 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
   const double ss = cons[SS1];
   double S2 = 0.;
   S2 += ss * ss;
-  const double S = sqrt(S2);
+  const double S = Cfg::FAST ? fabs(ss) : sqrt(S2);
+  auto fval = [&](double p, double *df, double *l2) -> double {
+    return Cfg::FAST ? c2p_f<Cfg>(ph, p, D, S2, E, df, l2) : c2p_f_ref<Cfg>(ph, p, D, S, E, df, l2);
+  };
 
   double pCand = Cfg::SPH ? fmax(1.e-13, prim[PPP]) : prim[PPP];
   int iters = 0, fallback = 0;
-  const double f_init = c2p_f<Cfg>(ph, pCand, D, S, E);
+  const double f_init = fval(pCand, nullptr, nullptr);
   if (fabs(f_init) > 0.) {
     double p_lo = fmax(0., (1. + 1e-13) * S - E);
     bool find_p = true;
-    if (c2p_f<Cfg>(ph, p_lo, D, S, E) < 0) find_p = false;
+    if (fval(p_lo, nullptr, nullptr) < 0) find_p = false;
     double p_hi;
     if (f_init < 0) {
       p_hi = 1. * pCand;
@@ -226,7 +316,7 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
       p_hi = pCand;
       // the reference grows p_hi without bound (a zero guess would never end);
       // 400 decades reach infinity, where f is NaN and the loop stops anyway
-      for (int g = 0; g < 400 && c2p_f<Cfg>(ph, p_hi, D, S, E) > 0; ++g) p_hi *= 10;
+      for (int g = 0; g < 400 && fval(p_hi, nullptr, nullptr) > 0; ++g) p_hi *= 10;
     }
     if (p_hi < p_lo) find_p = false;
     if (find_p) {
@@ -234,32 +324,31 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
       double lo = p_lo, hi = p_hi;
       if (f_init > 0.) lo = fmax(lo, pCand);
       double p = fmin(fmax(pCand, lo), hi);
-      double df;
-      double f = c2p_f_df<Cfg>(ph, p, D, S, E, &df);
+      double df, l2;
+      double f = fval(p, &df, &l2);
       const int MAXIT = 100;
       const double eps = 2.220446049250313e-16;
       for (iters = 1; iters <= MAXIT; ++iters) {
         // Rounding noise of f: E, p, D lfac and k p lfac^2 cancel, and lfac
         // itself carries eps*lfac^2 relative error from 1 - S^2/W^2.  Below
         // this level the sign of f is noise and p is as good as it gets.
-        const double W = E + p;
-        const double l2 = W * W / fmax(W * W - S * S, W * W * eps);
         const double noise = eps * (E + p + D * sqrt(l2) * (1. + l2) + 4. * p * l2 * (1. + 2. * l2));
-        if (f == 0. || fabs(f) <= 4. * noise) break;
+        if (f == 0. || fabs(f) <= noise) break;
         double pn = p - f / df;
         if (!(pn > lo && pn < hi)) {
           // Newton left the bracket: bisect, geometrically once lo > 0
           pn = lo > 0. ? sqrt(lo) * sqrt(hi) : 0.5 * (lo + hi);
           if (!(pn > lo && pn < hi)) pn = 0.5 * (lo + hi);
         }
-        double dfn;
-        const double fn = c2p_f_df<Cfg>(ph, pn, D, S, E, &dfn);
+        double dfn, l2n;
+        const double fn = fval(pn, &dfn, &l2n);
         if (fn > 0.) lo = pn;
         else if (fn < 0.) hi = pn;
         const double step = fabs(pn - p);
         p = pn;
         f = fn;
         df = dfn;
+        l2 = l2n;
         if (fn == 0. || step <= 1.e-14 * pn || (hi - lo) <= 1.e-14 * hi) break;
       }
       if (iters > MAXIT) fallback = 1;
@@ -272,24 +361,38 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
   }
 
   double p = pCand;
-  double Ep2 = (E + p) * (E + p);
-  double v2 = S2 / Ep2;
-  double lfac = 1. / sqrt(fabs(1. - v2));
-  double rho = D / lfac;
-  double uu;
-  if (fabs(S) == 0.) {
-    uu = 0;
-  } else {
-    double v = sqrt(1. - 1. / (lfac * lfac));
-    uu = lfac * v * (ss / S);
+  double rho, uu;
+  if (Cfg::FAST) {  // lfac = W/sqrt(W^2-S^2), rho = D/lfac, u = lfac v S_i/S with v = S/W
+    const double rW = 1. / (E + p);
+    const double v2 = S2 * rW * rW;
+    const double s1 = sqrt(fabs(1. - v2));  // 1/lfac
+    rho = D * s1;
+    uu = (fabs(S) == 0.) ? 0. : (ss * rW) / s1;
+  } else {  // rel_sph.cpp:288-302
+    double Ep2 = (E + p) * (E + p);
+    double v2 = S2 / Ep2;
+    double lfac = 1. / sqrt(fabs(1. - v2));
+    rho = D / lfac;
+    if (fabs(S) == 0.) {
+      uu = 0;
+    } else {
+      double v = sqrt(1. - 1. / (lfac * lfac));
+      uu = lfac * v * (ss / S);
+    }
   }
   if (Cfg::SPH) p = fmax(p, P_FLOOR);
   prim[PPP] = p;
   prim[RHO] = rho;
   prim[UU1] = uu;
   prim[UU2] = 0.;
+  if (Cfg::FAST) {
+    const double rD = 1. / D;
 #pragma unroll
-  for (int t = TR1; t < Cfg::NQ; ++t) prim[t] = cons[t] / D;
+    for (int t = TR1; t < Cfg::NQ; ++t) prim[t] = cons[t] * rD;
+  } else {
+#pragma unroll
+    for (int t = TR1; t < Cfg::NQ; ++t) prim[t] = cons[t] / D;
+  }
   prim2cons<Cfg>(ph, prim, cons);
 }
 
@@ -303,13 +406,13 @@ struct Waves {
 // Interface::wavespeedEstimates + computeLambda (rel_sph.cpp:322-394;
 // rel_cart.cpp:260-302 switches to the linear root when |FhllE| < 1e-15).
 template <class Cfg>
-GB_HD Waves compute_lambda(const Phys &ph, const FState<Cfg> &L, const FState<Cfg> &R) {
+GB_HD Waves compute_lambda_ref(const Phys &ph, const FState<Cfg> &L, const FState<Cfg> &R) {
   const double G = ph.gamma_ad;
   Waves w;
-  double lfacL = lfac_of(L.prim[UU1]);
-  double lfacR = lfac_of(R.prim[UU1]);
-  double vL = L.prim[UU1] / lfacL;
-  double vR = R.prim[UU1] / lfacR;
+  double lfacL = L.lfac;
+  double lfacR = R.lfac;
+  double vL = L.v;
+  double vR = R.v;
   double cSL = sqrt(G * L.prim[PPP] / (L.prim[RHO] + L.prim[PPP] * G / (G - 1.)));
   double cSR = sqrt(G * R.prim[PPP] / (R.prim[RHO] + R.prim[PPP] * G / (G - 1.)));
   double sgSL = cSL * cSL / (lfacL * lfacL * (1. - cSL * cSL));
@@ -341,9 +444,51 @@ GB_HD Waves compute_lambda(const Phys &ph, const FState<Cfg> &L, const FState<Cf
   if (linear) {
     w.lS = mhll / (Ehll + Fhllm);
   } else {
-    double eh = Ehll + Fhllm;
-    double delta = eh * eh - 4. * FhllE * mhll;
+    double delta = pow(Ehll + Fhllm, 2.) - 4. * FhllE * mhll;
     w.lS = ((Ehll + Fhllm) - sqrt(delta)) / (2. * FhllE);
+  }
+  return w;
+}
+
+template <class Cfg>
+GB_HD Waves compute_lambda(const Phys &ph, const FState<Cfg> &L, const FState<Cfg> &R) {
+  if (!Cfg::FAST) return compute_lambda_ref<Cfg>(ph, L, R);
+  const double G = ph.gamma_ad;
+  const double kg = ph.kgam;
+  Waves w;
+  const double vL = L.v, vR = R.v;
+  // relativistic sound speed (uses GAMMA_ in the reference for either EOS)
+  const double cs2L = G * L.prim[PPP] / (L.prim[RHO] + L.prim[PPP] * kg);
+  const double cs2R = G * R.prim[PPP] / (R.prim[RHO] + R.prim[PPP] * kg);
+  const double sgSL = cs2L / (L.lfac * L.lfac * (1. - cs2L));
+  const double sgSR = cs2R / (R.lfac * R.lfac * (1. - cs2R));
+  const double qL = sqrt(sgSL * (1. - vL * vL + sgSL));
+  const double qR = sqrt(sgSR * (1. - vR * vR + sgSR));
+  const double rL = 1. / (1. + sgSL), rR = 1. / (1. + sgSR);
+  w.lL = fmin((vR - qR) * rR, (vL - qL) * rL);
+  w.lR = fmax((vR + qR) * rR, (vL + qL) * rL);
+
+  const double lL = w.lL, lR = w.lR;
+  const double mmL = L.cons[SS1], mmR = R.cons[SS1];
+  const double pL = L.prim[PPP], pR = R.prim[PPP];
+  const double EL = L.cons[TAU] + L.cons[DEN];
+  const double ER = R.cons[TAU] + R.cons[DEN];
+  const double AL = lL * EL - mmL;
+  const double AR = lR * ER - mmR;
+  const double BL = mmL * (lL - vL) - pL;
+  const double BR = mmR * (lR - vR) - pR;
+  const double rd = 1. / (lR - lL);
+  const double FhllE = (lL * AR - lR * AL) * rd;
+  const double Ehll = (AR - AL) * rd;
+  const double Fhllm = (lL * BR - lR * BL) * rd;
+  const double mhll = (BR - BL) * rd;
+  const bool linear = Cfg::SPH ? (fabs(FhllE) == 0) : (fabs(FhllE) < 1.e-15);
+  const double eh = Ehll + Fhllm;
+  if (linear) {
+    w.lS = mhll / eh;
+  } else {
+    const double delta = eh * eh - 4. * FhllE * mhll;
+    w.lS = (eh - sqrt(delta)) / (2. * FhllE);
   }
   return w;
 }
@@ -356,20 +501,27 @@ GB_HD void hllc_flux(const FState<Cfg> &L, const FState<Cfg> &R, const Waves &w,
                      double *flux) {
   const double lS = w.lS;
   auto star = [&](const FState<Cfg> &Sin, double lbda, double *out_cons) {
-    double m = Sin.cons[SS1];
-    double lfac = lfac_of(Sin.prim[UU1]);
-    double vv = Sin.prim[UU1] / lfac;
-    double p = Sin.prim[PPP];
-    double D = Sin.cons[DEN];
-    double E = Sin.cons[TAU] + Sin.cons[DEN];
-    double A = lbda * E - m;
-    double B = m * (lbda - vv) - p;
-    double pS = (A * lS - B) / (1. - lbda * lS);
-    double k = (lbda - vv) / (lbda - lS);
+    const double m = Sin.cons[SS1];
+    const double vv = Sin.v;
+    const double p = Sin.prim[PPP];
+    const double D = Sin.cons[DEN];
+    const double E = Sin.cons[TAU] + Sin.cons[DEN];
+    const double A = lbda * E - m;
+    const double B = m * (lbda - vv) - p;
+    const double pS = (A * lS - B) / (1. - lbda * lS);
+    double k;
+    if (Cfg::FAST) {
+      const double rk = 1. / (lbda - lS);
+      k = (lbda - vv) * rk;
+      out_cons[SS1] = (m * (lbda - vv) + pS - p) * rk;
+      out_cons[TAU] = (E * (lbda - vv) + pS * lS - p * vv) * rk - D * k;
+    } else {  // rel_sph.cpp:433-442
+      k = (lbda - vv) / (lbda - lS);
+      out_cons[SS1] = (m * (lbda - vv) + pS - p) / (lbda - lS);
+      out_cons[TAU] = (E * (lbda - vv) + pS * lS - p * vv) / (lbda - lS) - D * k;
+    }
     out_cons[DEN] = D * k;
-    out_cons[SS1] = (m * (lbda - vv) + pS - p) / (lbda - lS);
     out_cons[SS2] = 0.;
-    out_cons[TAU] = (E * (lbda - vv) + pS * lS - p * vv) / (lbda - lS) - D * k;
 #pragma unroll
     for (int t = TR1; t < Cfg::NQ; ++t) out_cons[t] = Sin.cons[t] * k;
   };
@@ -418,10 +570,9 @@ GB_HD bool compute_Sd(const Phys &ph, const FState<Cfg> &S1, const FState<Cfg> &
   double rho2 = S2.prim[RHO];
   double h1 = 1 + p1 * G / (G - 1.) / rho1;
   double h2 = 1 + p2 * G / (G - 1.) / rho2;
-  double lfac1 = lfac_of(S1.prim[UU1]);
-  double lfac2 = lfac_of(S2.prim[UU1]);
-  double vx1 = S1.prim[UU1] / lfac1;
-  double vx2 = S2.prim[UU1] / lfac2;
+  double lfac2 = S2.lfac;
+  double vx1 = S1.v;
+  double vx2 = S2.v;
   double v12 = (vx1 - vx2) / (1 - vx1 * vx2);
   double A1 = h1 * 0.;
   double I = 0;

@@ -18,6 +18,12 @@
 #include "physics.cuh"
 #include "regrid.cuh"
 
+#ifdef GB_SWEEP_NOINLINE
+#define GB_SWEEP_ATTR __noinline__
+#else
+#define GB_SWEEP_ATTR __forceinline__
+#endif
+
 namespace gb {
 
 // Device view of the pooled structure-of-arrays state.  Run r owns cells
@@ -30,6 +36,8 @@ struct Tracks {
   double *xI;       // interface i sits between cells i and i+1
   double *u0;       // [NQS][N] step-start cons * dV (stage combine)
   double *xI0;      // step-start interface positions
+  double *fl1;      // [NQS][N] stage-1 interface fluxes (kept from the CFL pass)
+  double *v1;       // stage-1 interface velocities
   double *sd, *pspec;
   uint8_t *shocked;
   long long N;      // row stride
@@ -86,7 +94,7 @@ struct TrackStep {
 
   struct Smem {
     double cp[NQS][NC];  // staged primitives
-    double cx[NC], cdx[NC];
+    double cx[NC], cdx[NC], cen[NC];
     double fl[NQS][BS + 1];  // interface fluxes; slot 0 = carry (interface a-1)
     double lL[BS + 1], lR[BS + 1], v[BS + 1];
     double xold[BS + 1], xnew[BS + 1], xcmb[BS + 1];
@@ -197,29 +205,34 @@ struct TrackStep {
         R.prim[Slots<Cfg>::q_of(s)] = sm.cp[s][c + 1];
       }
     } else {
-      const double cenLL = make_geom<Cfg>(sm.cx[c - 1], sm.cdx[c - 1]).cen;
-      const double cenL = make_geom<Cfg>(sm.cx[c], sm.cdx[c]).cen;
-      const double cenR = make_geom<Cfg>(sm.cx[c + 1], sm.cdx[c + 1]).cen;
-      const int cRR = (i + 2 < n - 1) ? c + 2 : c + 1 + ((n - 1) - (i + 1));
-      const double cenRR = make_geom<Cfg>(sm.cx[cRR], sm.cdx[cRR]).cen;
+      // cells i-1 .. i+2 (i+2 <= n-1 for every interior interface)
+      const double cenLL = sm.cen[c - 1], cenL = sm.cen[c], cenR = sm.cen[c + 1], cenRR = sm.cen[c + 2];
+      const double d1 = cenL - cenLL, d2 = cenR - cenL, d3 = cenRR - cenR;
+      const double r1 = 1. / d1, r2 = 1. / d2, r3 = 1. / d3;
+      const double dL = xI - cenL, dR = xI - cenR;
 #pragma unroll
       for (int s = 0; s < NQS; ++s) {
-        const double qLL = sm.cp[s][c - 1], qL = sm.cp[s][c], qR = sm.cp[s][c + 1], qRR = sm.cp[s][cRR];
-        double gL = (qL - qLL) / (cenL - cenLL);
-        double gN = (qR - qL) / (cenR - cenL);
-        double gR = (qRR - qR) / (cenRR - cenR);
+        const double qLL = sm.cp[s][c - 1], qL = sm.cp[s][c], qR = sm.cp[s][c + 1], qRR = sm.cp[s][c + 2];
+        double gN, gL, gR;
+        if (Cfg::FAST) {
+          gN = (qR - qL) * r2;
+          gL = (qL - qLL) * r1;
+          gR = (qRR - qR) * r3;
+        } else {  // grad() of 1d.cpp:262-274
+          gN = (qR - qL) / d2;
+          gL = (qL - qLL) / d1;
+          gR = (qRR - qR) / d3;
+        }
         gL = minmod(gL, gN);
         gR = minmod(gR, gN);
-        L.prim[Slots<Cfg>::q_of(s)] = qL + gL * (xI - cenL);
-        R.prim[Slots<Cfg>::q_of(s)] = qR + gR * (xI - cenR);
+        L.prim[Slots<Cfg>::q_of(s)] = qL + gL * dL;
+        R.prim[Slots<Cfg>::q_of(s)] = qR + gR * dR;
       }
     }
     L.prim[UU2] = 0.;
     R.prim[UU2] = 0.;
-    prim2cons<Cfg>(ph, L.prim, L.cons);
-    state2flux<Cfg>(L.prim, L.cons, L.flux);
-    prim2cons<Cfg>(ph, R.prim, R.cons);
-    state2flux<Cfg>(R.prim, R.cons, R.flux);
+    fill_state<Cfg>(ph, L);
+    fill_state<Cfg>(ph, R);
   }
 
   // Cell::update_dt, moving direction (cell.cpp:47-74).  Returns false on a
@@ -235,7 +248,10 @@ struct TrackStep {
   // --- one stage sweep ------------------------------------------------------
   // mode 0: stage-1 CFL candidates only (returns the run's min dt_loc and
   //         resets dt_loc); mode 1: fluxes + update (+ RK combine for stage>1).
-  __device__ static double sweep(const Tracks &T, const Phys &ph, const RunParams &P, const SynchConst &sc,
+  // Inlined into the step (measured faster than one shared out-of-line copy,
+  // whose call frame costs local-memory traffic).
+  __device__ GB_SWEEP_ATTR static double sweep(const Tracks &T, const Phys &ph, const RunParams &P,
+                                              const SynchConst &sc,
                                  Smem &sm, long long off, int n, int stage, int mode, double dt, double t,
                                  StepStats &st) {
     const int tid = threadIdx.x;
@@ -257,6 +273,7 @@ struct TrackStep {
           cell_geom(T, sm, off, n, ng, stage, i, (k == 1 && a > 0) ? &sm.xold[0] : nullptr, &gx, &gdx);
           sm.cx[k] = gx;
           sm.cdx[k] = gdx;
+          sm.cen[k] = make_geom<Cfg>(gx, gdx).cen;
         }
       }
       __syncthreads();
@@ -266,43 +283,57 @@ struct TrackStep {
       const bool has_if = i <= n - 2;
       const int c = tid + 1;  // slot of cell i
       double myflux[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) myflux[q] = 0.;
       double my_lL = 0, my_lR = 0, my_v = 0, my_xold = 0, my_xnew = 0, my_xcmb = 0;
       if (has_if) {
-        FState<Cfg> L, R;
-        const double xI = T.xI[off + i];
+        const long long gi = off + i;
+        const double xI = T.xI[gi];
         my_xold = xI;
-        reconstruct(sm, ph, i, n, c, xI, L, R);
-        const Waves w = compute_lambda<Cfg>(ph, L, R);
-        double v = ph.vi * w.lS;
-        if (Cfg::BM) {  // userKinematics (BM1D.cpp:188-246)
-          if (i < ng) v = P.v_in;
-          if (i >= n - 1 - ng) v = P.v_out;
-        }
-        my_lL = w.lL;
-        my_lR = w.lR;
-        my_v = v;
-        if (mode == 1) {
+        if (mode == 1 && stage == 1) {
+          // stage-1 fluxes and velocities were solved by the CFL pass
+          my_v = T.v1[gi];
+#pragma unroll
+          for (int s = 0; s < NQS; ++s) myflux[Slots<Cfg>::q_of(s)] = T.fl1[s * T.N + gi];
+        } else {
+          FState<Cfg> L, R;
+          reconstruct(sm, ph, i, n, c, xI, L, R);
+          const Waves w = compute_lambda<Cfg>(ph, L, R);
+          double v = ph.vi * w.lS;
+          if (Cfg::BM) {  // userKinematics (BM1D.cpp:188-246)
+            if (i < ng) v = P.v_in;
+            if (i >= n - 1 - ng) v = P.v_out;
+          }
+          my_lL = w.lL;
+          my_lR = w.lR;
+          my_v = v;
           hllc_flux<Cfg>(L, R, w, v, iface_area<Cfg>(xI), myflux);
           if (Cfg::SHOCK) {  // measureShock into cell i (radiation_sph.cpp:160-175)
             double Sd, ps;
             const bool have = compute_Sd<Cfg>(ph, L, R, &Sd, &ps);
-            const long long g = off + i;
-            const double sd0 = fmax(T.sd[g], Sd);
-            T.sd[g] = sd0;
-            if (have && ps > T.pspec[g]) T.pspec[g] = ps;
-            if (stage == 1) T.shocked[g] = sd0 > DETECT_SHOCK_THRESHOLD ? 1 : 0;  // detectShock
+            const double sd0 = fmax(T.sd[gi], Sd);
+            T.sd[gi] = sd0;
+            if (have && ps > T.pspec[gi]) T.pspec[gi] = ps;
+            if (stage == 1) T.shocked[gi] = sd0 > DETECT_SHOCK_THRESHOLD ? 1 : 0;  // detectShock
           }
+          if (mode == 0) {  // keep the stage-1 solution for the update pass
+            T.v1[gi] = v;
+#pragma unroll
+            for (int s = 0; s < NQS; ++s) T.fl1[s * T.N + gi] = myflux[Slots<Cfg>::q_of(s)];
+          }
+        }
+        if (mode == 1) {
           // Interface::move, then the RK combine of interface positions
-          my_xnew = xI + dt * v;
+          my_xnew = xI + dt * my_v;
           if (stage == 1) {
-            T.xI0[off + i] = xI;
+            T.xI0[gi] = xI;
             my_xcmb = my_xnew;
           } else if (i >= iL && i <= iR - 1) {
-            my_xcmb = w0 * T.xI0[off + i] + w1 * my_xnew;
+            my_xcmb = w0 * T.xI0[gi] + w1 * my_xnew;
           } else {
             my_xcmb = my_xnew;
           }
-          T.xI[off + i] = my_xcmb;
+          T.xI[gi] = my_xcmb;
         }
       }
       // cell n-1 has no interface of its own; as for every cell, the shock
@@ -372,8 +403,14 @@ struct TrackStep {
             cons[GMN] += dg;
           }
           const Geom G1 = geom_between<Cfg>(sm.xnew[tid], sm.xnew[tid + 1]);
+          if (Cfg::FAST) {
+            const double rdV1 = 1. / G1.dV;
 #pragma unroll
-          for (int q = 0; q < NQ; ++q) cons[q] /= G1.dV;
+            for (int q = 0; q < NQ; ++q) cons[q] *= rdV1;
+          } else {
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) cons[q] /= G1.dV;
+          }
           C2PStats cs;
           cons2prim<Cfg>(ph, cons, prim, &cs);
           st.c2p_calls++;
@@ -387,8 +424,14 @@ struct TrackStep {
               cons[q] = w0 * T.u0[s * T.N + g] + w1 * cons[q] * G1.dV;
             }
             const Geom G2 = geom_between<Cfg>(sm.xcmb[tid], sm.xcmb[tid + 1]);
+            if (Cfg::FAST) {
+              const double rdV2 = 1. / G2.dV;
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) cons[q] /= G2.dV;
+              for (int q = 0; q < NQ; ++q) cons[q] *= rdV2;
+            } else {
+#pragma unroll
+              for (int q = 0; q < NQ; ++q) cons[q] /= G2.dV;
+            }
             cons2prim<Cfg>(ph, cons, prim, &cs);
             st.c2p_calls++;
             st.c2p_iters += cs.iters;
@@ -412,6 +455,7 @@ struct TrackStep {
         sm.xcmb[0] = sm.xcmb[BS];
         sm.cx[0] = sm.cx[BS];
         sm.cdx[0] = sm.cdx[BS];
+        sm.cen[0] = sm.cen[BS];
       }
       if (tid < NQS) {
         sm.fl[tid][0] = sm.fl[tid][BS];
@@ -538,7 +582,7 @@ struct TrackStep {
 };
 
 template <class Cfg, int BS>
-__global__ void __launch_bounds__(BS) track_step_kernel(Tracks T, Phys ph, int nsteps, const int *order, int nruns,
+__global__ void __launch_bounds__(BS, Cfg::MIN_BLOCKS) track_step_kernel(Tracks T, Phys ph, int nsteps, const int *order, int nruns,
                                                          int *queue, StepStats *stats, int regrid_only) {
   using TS = TrackStep<Cfg, BS>;
   extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -12,7 +12,7 @@ from dataclasses import dataclass, fields
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libgamma_b200.so")
+LIB_PATH = os.environ.get("GAMMA_B200_LIB") or os.path.join(HERE, "lib", "libgamma_b200.so")
 
 GAMMA_OK = 0
 GAMMA_ERR_INVALID = -1

@@ -53,3 +53,44 @@ def l1_rel(a, b):
     """sum |a-b| / sum |b| over active cells"""
     den = np.sum(np.abs(b))
     return float(np.sum(np.abs(a - b)) / den) if den > 0 else float(np.sum(np.abs(a - b)))
+
+
+def solver_sensitivity(run, eps_list=(1e-13, 1e-14, 1e-15), converged=1e-16):
+    """How much the oracle's own solution moves when only its pressure root
+    finder stops elsewhere.
+
+    run(eps) returns an oracle snapshot after the same steps with Brent
+    stopping at relative bracket eps.  Returns (converged snapshot, per-field
+    per-cell max |snap(eps) - snap(converged)| over eps_list)."""
+    ref = run(converged)
+    sens = {}
+    for eps in eps_list:
+        s = run(eps)
+        assert s.ntrack == ref.ntrack
+        for q in range(ref.prim.shape[0]):
+            d = np.abs(s.prim[q] - ref.prim[q])
+            sens[q] = np.maximum(sens.get(q, 0.0), d)
+    return ref, sens
+
+
+def within_sensitivity(got, ref, sens, gamma_ad, rtol=1e-12, k=4.0, qs=(0, 1, 2)):
+    """Per-cell check |got - ref| <= rtol * scale + k * sensitivity.
+
+    scale is |ref| (pressure: max(|p|, 1e-2 E)).  Returns the worst ratio
+    |got - ref| / bound per field (<= 1 passes) and the fraction of cells that
+    are within rtol alone."""
+    E = energy_scale(ref.prim, gamma_ad)
+    worst, frac = {}, {}
+    for q in qs:
+        b = ref.prim[q]
+        scale = np.maximum(np.abs(b), 1e-2 * np.abs(E)) if q == 1 else np.abs(b)
+        if q >= 2:
+            # velocities and tracers vanish in parts of a track: below 1e-4 of
+            # the field's largest magnitude (or of one for a track at rest)
+            # differences are rounding of the fluxes that carry them
+            scale = np.maximum(scale, 1e-4 * max(np.max(np.abs(b)), 1.0 if q == 2 else 1e-300))
+        d = np.abs(got.prim[q] - b)
+        bound = rtol * scale + k * sens[q]
+        worst[q] = float(np.max(d / np.maximum(bound, 1e-300)))
+        frac[q] = float(np.mean(d <= rtol * scale))
+    return worst, frac
