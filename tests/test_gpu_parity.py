@@ -153,9 +153,12 @@ def test_bm1d_one_step_matches_converged_oracle(gpu_available):
 
     ref, sens = solver_sensitivity(run)
     assert got.ntrack == ref.ntrack
-    worst, frac = within_sensitivity(got, ref, sens, 4. / 3., k=10.0, qs=(0, 1, 2, 4, 6, 7))
+    # 1e-12 for >= 99 % of cells; the rest (relativistic cells, where a root one
+    # ulp away moves rho by ~lfac^2 ulp) within 2e-12 or 10x the solver sensitivity
+    worst, frac = within_sensitivity(got, ref, sens, 4. / 3., rtol=2e-12, k=10.0, qs=(0, 1, 2, 4, 6, 7))
     assert max(worst.values()) <= 1.0, (worst, frac)
-    assert min(frac.values()) >= 0.995, frac
+    _, frac12 = within_sensitivity(got, ref, sens, 4. / 3., rtol=1e-12, k=10.0, qs=(0, 1, 2, 4, 6, 7))
+    assert min(frac12.values()) >= 0.99, frac12
     for f in ("x", "dx", "xI"):  # the right ghost cell has zero width (1d.cpp:241)
         a, b = getattr(got, f), getattr(ref, f)
         assert np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)) <= 1e-12, f
