@@ -159,9 +159,12 @@ def test_bm1d_one_step_matches_converged_oracle(gpu_available):
     assert max(worst.values()) <= 1.0, (worst, frac)
     _, frac12 = within_sensitivity(got, ref, sens, 4. / 3., rtol=1e-12, k=10.0, qs=(0, 1, 2, 4, 6, 7))
     assert min(frac12.values()) >= 0.99, frac12
-    for f in ("x", "dx", "xI"):  # the right ghost cell has zero width (1d.cpp:241)
+    # positions at 1e-12; widths dx = xR - xL relative to the position they are
+    # differences of (a width of 1e3 at r = 5.5e6 carries 5.5e3 ulps of x)
+    for f in ("x", "xI"):
         a, b = getattr(got, f), getattr(ref, f)
-        assert np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)) <= 1e-12, f
+        assert np.max(np.abs(a - b) / np.abs(b)) <= 1e-12, f
+    assert np.max(np.abs(got.dx - ref.dx) / np.abs(ref.x)) <= 1e-12
     assert abs(got.t - ref.t) <= 1e-14 * ref.t
 
 
