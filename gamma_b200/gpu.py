@@ -29,7 +29,7 @@ PROBLEM_BM1D, PROBLEM_TUBE = 0, 1
 # every symbol include/gamma_gpu.h declares
 EXPORTS = (
     "gamma_gpu_create", "gamma_gpu_layout", "gamma_gpu_set_params", "gamma_gpu_upload", "gamma_gpu_step",
-    "gamma_gpu_regrid",
+    "gamma_gpu_regrid", "gamma_gpu_step_tubes_noalloc",
     "gamma_gpu_download", "gamma_gpu_cons2prim", "gamma_gpu_stream", "gamma_gpu_strerror",
     "gamma_gpu_last_error", "gamma_gpu_destroy",
 )
@@ -100,6 +100,9 @@ def lib() -> ctypes.CDLL:
         L.gamma_gpu_download.argtypes = [ctypes.c_void_p, _ip, _dp, _dp, _lp, _ip, _dp, _dp, _dp, _dp, _dp]
         L.gamma_gpu_cons2prim.argtypes = [ctypes.POINTER(Config), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                           ctypes.c_void_p, ctypes.c_void_p]
+        L.gamma_gpu_step_tubes_noalloc.argtypes = [ctypes.POINTER(Config), ctypes.c_int, ctypes.c_longlong] + \
+            [ctypes.c_void_p] * 8 + [ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(StepStats)]
+        L.gamma_gpu_step_tubes_noalloc.restype = ctypes.c_int
         L.gamma_gpu_stream.restype = ctypes.c_void_p
         L.gamma_gpu_stream.argtypes = [ctypes.c_void_p]
         L.gamma_gpu_strerror.restype = ctypes.c_char_p
@@ -217,3 +220,25 @@ def cons2prim_device(cfg: Config, cons_ptr: int, prim_ptr: int, n: int, iters_pt
                                    ctypes.c_void_p(stream) if stream else None)
     if rc != GAMMA_OK:
         raise GammaError(rc)
+
+
+class RunState(ctypes.Structure):
+    """gamma_run_state_t"""
+
+    _fields_ = [("ntrack", ctypes.c_int), ("status", ctypes.c_int), ("t", ctypes.c_double),
+                ("dt", ctypes.c_double), ("it", ctypes.c_longlong)]
+
+
+def step_tubes_noalloc(cfg: Config, nruns: int, total: int, offsets_ptr: int, capacity_ptr: int, runs_ptr: int,
+                       prim_ptr: int, x_ptr: int, dx_ptr: int, dtl_ptr: int, xI_ptr: int, nsteps: int,
+                       stream: int = 0, stats: bool = True):
+    """gamma_gpu_step_tubes_noalloc on caller-owned device arrays (raw CUDA pointers)."""
+    st = StepStats()
+    v = ctypes.c_void_p
+    rc = lib().gamma_gpu_step_tubes_noalloc(ctypes.byref(cfg), int(nruns), int(total), v(offsets_ptr),
+                                            v(capacity_ptr), v(runs_ptr), v(prim_ptr), v(x_ptr), v(dx_ptr),
+                                            v(dtl_ptr), v(xI_ptr), int(nsteps), v(stream) if stream else None,
+                                            ctypes.byref(st) if stats else None)
+    if rc != GAMMA_OK:
+        raise GammaError(rc)
+    return st.as_dict() if stats else None

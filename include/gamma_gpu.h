@@ -132,6 +132,39 @@ int gamma_gpu_download(gamma_ctx_t *ctx, int *ntrack, double *t, double *dt, lon
  * state.  stream: a cudaStream_t, or NULL for the default stream. */
 int gamma_gpu_cons2prim(const gamma_config_t *cfg, double *cons, double *prim, int n, int *iters, void *stream);
 
+/* Per-run scalars in device memory for gamma_gpu_step_tubes_noalloc (the
+ * fields a context keeps internally: Grid::ntrack, the run status, Simu::t,
+ * Simu::dt and Simu::it). */
+typedef struct {
+  int ntrack;
+  int status;    /* 0 on input; 30 after a negative CFL candidate (the reference's exit code) */
+  double t;
+  double dt;
+  long long it;
+} gamma_run_state_t;
+
+/* No counterpart in the reference.  The batched shock-tube step
+ * (cartesian + rel_cart configuration only) for callers that cannot allocate
+ * device memory -- a solver embedded in a framework that owns every device
+ * allocation, a memory-budgeted service, or code that must not synchronise
+ * the device the way cudaMalloc/cudaFree can.  The caller passes its own
+ * DEVICE arrays in the layout of this header (prim holds the nq-1 stored rows
+ * -- slots 0,1,2,4,5 -- of `total` doubles each; offsets/capacity/runs have
+ * nruns entries) and the call allocates nothing: the step's workspace lives
+ * in one fixed 64 MiB device array inside the library (about 690,000 cells per
+ * call), held by every GPU that loads the library until the process exits.
+ * A call needing more returns GAMMA_ERR_CAPACITY before anything runs.  The
+ * first call on a device looks up that array's address (cudaGetSymbolAddress)
+ * and should come before any CUDA graph capture.  All calls on a device share
+ * the workspace and it keeps the last call's contents (what must start at
+ * zero is cleared on every call), so calls that overlap on the GPU race: issue
+ * them one after another.  stream: a cudaStream_t or NULL; stats (host, may be
+ * NULL) makes the call wait and report. */
+int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg, int nruns, long long total,
+                                 const long long *offsets, const int *capacity, gamma_run_state_t *runs,
+                                 double *prim, double *x, double *dx, double *dt_loc, double *xI,
+                                 int nsteps, void *stream, gamma_step_stats_t *stats);
+
 /* The context's CUDA stream (a cudaStream_t). */
 void *gamma_gpu_stream(gamma_ctx_t *ctx);
 
