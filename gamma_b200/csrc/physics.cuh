@@ -278,9 +278,17 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
   else gma = ph.gamma_ad;
   const double f = (E + p - D * lfac - (gma * p * lfac * lfac) / (gma - 1.));
   if (df) {
-    double dfast;
-    c2p_f<Cfg>(ph, p, D, S * S, E, &dfast);
-    *df = dfast;
+    if (Cfg::SPH && ph.eos != 0) {  // Gamma_eff(p) terms: take them from the derivative form
+      double dfast;
+      c2p_f<Cfg>(ph, p, D, S * S, E, &dfast);
+      *df = dfast;
+    } else {  // d lfac/dp = -lfac^3 x / W with the same lfac and x as f
+      const double sgn = (1. - x) >= 0. ? 1. : -1.;
+      const double l2 = lfac * lfac;
+      const double dl = -sgn * lfac * l2 * x / W;
+      const double k = gma / (gma - 1.);
+      *df = 1. - D * dl - k * (l2 + 2. * p * lfac * dl);
+    }
   }
   if (l2out) *l2out = lfac * lfac;
   return f;
@@ -315,8 +323,9 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
     } else {
       p_hi = pCand;
       // the reference grows p_hi without bound (a zero guess would never end);
-      // 400 decades reach infinity, where f is NaN and the loop stops anyway
-      for (int g = 0; g < 400 && fval(p_hi, nullptr, nullptr) > 0; ++g) p_hi *= 10;
+      // 400 decades reach infinity, where f is NaN and the loop stops anyway.
+      // Its first test re-evaluates f(pCand), which is f_init.
+      for (int g = 0; g < 400 && (g == 0 ? f_init : fval(p_hi, nullptr, nullptr)) > 0; ++g) p_hi *= 10;
     }
     if (p_hi < p_lo) find_p = false;
     if (find_p) {
