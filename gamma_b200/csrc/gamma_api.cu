@@ -38,6 +38,8 @@ struct gamma_ctx {
   gb::StepStats *d_stats = nullptr;
   int grid = 0;
   size_t smem = 0;
+  int grid_guess = 0;  // launch shape of the kernel with the learned guess
+  size_t smem_guess = 0;
   std::string err;
 };
 
@@ -83,30 +85,37 @@ gb::Phys phys_of(const gamma_config_t &c) {
   return p;
 }
 
-template <class Cfg>
+unsigned words_bytes(int max_cap) { return 4u * 4u * (unsigned)gb::regrid_words(max_cap); }
+
+template <class Cfg, bool GUESS>
 size_t smem_bytes(int max_cap) {
-  using TS = gb::TrackStep<Cfg, kBlock>;
-  return sizeof(typename TS::Smem) + 4u * 4u * (size_t)gb::regrid_words(max_cap);
+  using TS = gb::TrackStep<Cfg, kBlock, GUESS>;
+  size_t b = sizeof(typename TS::Smem) + words_bytes(max_cap);
+  if (GUESS) b = ((b + 15u) & ~size_t(15)) + sizeof(gb::mlp::InferSmem);
+  return b;
 }
 
-template <class Cfg>
-int configure_launch(gamma_ctx *c) {
-  auto kern = gb::track_step_kernel<Cfg, kBlock>;
-  c->smem = smem_bytes<Cfg>(c->max_cap);
-  GB_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem));
+template <class Cfg, bool GUESS>
+int configure_launch(gamma_ctx *c, int *grid, size_t *smem) {
+  auto kern = gb::track_step_kernel<Cfg, kBlock, GUESS>;
+  *smem = smem_bytes<Cfg, GUESS>(c->max_cap);
+  GB_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
   int dev = 0, nsm = 0, occ = 0;
   GB_CUDA(c, cudaGetDevice(&dev));
   GB_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  GB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlock, c->smem));
+  GB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlock, *smem));
   if (occ < 1) occ = 1;
-  c->grid = std::min(c->nruns, nsm * occ);
+  *grid = std::min(c->nruns, nsm * occ);
   return GAMMA_OK;
 }
 
-template <class Cfg>
+template <class Cfg, bool GUESS>
 int launch_step(gamma_ctx *c, int nsteps, int regrid_only) {
-  gb::track_step_kernel<Cfg, kBlock><<<c->grid, kBlock, c->smem, c->stream>>>(
-      c->T, phys_of(c->cfg), nsteps, c->d_order, c->nruns, c->d_queue, c->d_stats, regrid_only);
+  const int grid = GUESS ? c->grid_guess : c->grid;
+  const size_t smem = GUESS ? c->smem_guess : c->smem;
+  gb::track_step_kernel<Cfg, kBlock, GUESS><<<grid, kBlock, smem, c->stream>>>(
+      c->T, phys_of(c->cfg), nsteps, c->d_order, c->nruns, c->d_queue, c->d_stats, regrid_only,
+      words_bytes(c->max_cap));
   GB_CUDA(c, cudaGetLastError());
   return GAMMA_OK;
 }
@@ -264,7 +273,8 @@ GAMMA_API int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *
       cudaSuccess)
     return fail(e, "copy capacities");
   if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return fail(e, "sync");
-  int rc = kind == KIND_SPH ? configure_launch<gb::CfgSph>(c) : configure_launch<gb::CfgCart>(c);
+  int rc = kind == KIND_SPH ? configure_launch<gb::CfgSph, false>(c, &c->grid, &c->smem)
+                            : configure_launch<gb::CfgCart, false>(c, &c->grid, &c->smem);
   if (rc != GAMMA_OK) {
     gamma_gpu_destroy(c);
     return rc;
@@ -336,8 +346,14 @@ int run_steps(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats, int regri
   GB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(int), ctx->stream));
   GB_CUDA(ctx, cudaMemsetAsync(ctx->d_stats, 0, sizeof(gb::StepStats), ctx->stream));
   GB_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-  int rc = ctx->kind == KIND_SPH ? launch_step<gb::CfgSph>(ctx, nsteps, regrid_only)
-                                 : launch_step<gb::CfgCart>(ctx, nsteps, regrid_only);
+  const bool guess = ctx->T.mlp != nullptr && !regrid_only;
+  int rc;
+  if (ctx->kind == KIND_SPH)
+    rc = guess ? launch_step<gb::CfgSph, true>(ctx, nsteps, regrid_only)
+               : launch_step<gb::CfgSph, false>(ctx, nsteps, regrid_only);
+  else
+    rc = guess ? launch_step<gb::CfgCart, true>(ctx, nsteps, regrid_only)
+               : launch_step<gb::CfgCart, false>(ctx, nsteps, regrid_only);
   if (rc != GAMMA_OK) return rc;
   GB_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
   if (stats) {
@@ -362,6 +378,17 @@ int run_steps(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats, int regri
 
 GAMMA_API int gamma_gpu_step(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats) {
   return run_steps(ctx, nsteps, stats, 0);
+}
+
+GAMMA_API int gamma_gpu_set_guess(gamma_ctx_t *ctx, const float *params) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  if (params && !ctx->grid_guess) {
+    int rc = ctx->kind == KIND_SPH ? configure_launch<gb::CfgSph, true>(ctx, &ctx->grid_guess, &ctx->smem_guess)
+                                   : configure_launch<gb::CfgCart, true>(ctx, &ctx->grid_guess, &ctx->smem_guess);
+    if (rc != GAMMA_OK) return rc;
+  }
+  ctx->T.mlp = params;
+  return GAMMA_OK;
 }
 
 GAMMA_API int gamma_gpu_regrid(gamma_ctx_t *ctx, gamma_step_stats_t *stats) {

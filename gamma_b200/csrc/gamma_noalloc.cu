@@ -140,7 +140,8 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
   const int grid = nruns < nsm * (occ > 0 ? occ : 1) ? nruns : nsm * (occ > 0 ? occ : 1);
   auto *qs = reinterpret_cast<int *>(ws + off_queue);
   auto *st = reinterpret_cast<gb::StepStats *>(ws + off_stats);
-  kern<<<grid, kBlock, smem, s>>>(T, ph, nsteps, reinterpret_cast<const int *>(ws + off_order), nruns, qs, st, 0);
+  kern<<<grid, kBlock, smem, s>>>(T, ph, nsteps, reinterpret_cast<const int *>(ws + off_order), nruns, qs, st, 0,
+                                  4u * 4u * (unsigned)gb::regrid_words(32));
   if (cudaGetLastError() != cudaSuccess) return GAMMA_ERR_CUDA;
 
   if (stats) {

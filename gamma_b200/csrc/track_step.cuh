@@ -15,6 +15,7 @@
 // without any grid-wide synchronisation.
 #pragma once
 
+#include "mlp.cuh"
 #include "physics.cuh"
 #include "regrid.cuh"
 
@@ -46,6 +47,7 @@ struct Tracks {
   RunState *run;    // per-run scalars (ntrack, t, dt, it, status)
   const RunParams *par;
   RegridScratch rg;
+  const float *mlp;  // learned cons2prim guess parameters (kernels built with GUESS only)
 };
 
 template <class Cfg>
@@ -86,7 +88,7 @@ __device__ __forceinline__ void calc_bm(const Phys &ph, const RunParams &P, doub
   *u = C_LIGHT * sqrt(1. - 1. / (lfac * lfac)) * lfac / P.vNorm;
 }
 
-template <class Cfg, int BS>
+template <class Cfg, int BS, bool GUESS = false>
 struct TrackStep {
   static constexpr int NQ = Cfg::NQ;
   static constexpr int NQS = Cfg::NQ - 1;
@@ -245,6 +247,27 @@ struct TrackStep {
     return !(*cand < 0);
   }
 
+  __device__ static void count_c2p(StepStats &st, const C2PStats &cs) {
+    st.c2p_calls++;
+    st.c2p_iters += cs.iters;
+    st.c2p_fallbacks += cs.fallback;
+    st.c2p_max_iters = max(st.c2p_max_iters, cs.iters);
+  }
+
+  // Learned cons2prim starting pressure for the cells of this warp (all 32
+  // lanes call; lanes with on = false only take part in the tensor-core tiles).
+  // A non-finite or non-positive guess keeps the warm start.
+  __device__ static void learned_guess(const mlp::InferSmem &inf, const double *cons, double *prim, bool on) {
+    float f[3] = {0.f, 0.f, 0.f}, o[2] = {0.f, 0.f};
+    if (on) mlp::features(cons[DEN], cons[TAU], cons[SS1], f);
+    __syncwarp();
+    mlp::infer_warp(inf, f, o);
+    if (on) {
+      const double pg = mlp::guess_pressure(cons[DEN], o[0]);
+      if (isfinite(pg) && pg > 0.) prim[PPP] = pg;
+    }
+  }
+
   // --- one stage sweep ------------------------------------------------------
   // mode 0: stage-1 CFL candidates only (returns the run's min dt_loc and
   //         resets dt_loc); mode 1: fluxes + update (+ RK combine for stage>1).
@@ -253,7 +276,7 @@ struct TrackStep {
   __device__ GB_SWEEP_ATTR static double sweep(const Tracks &T, const Phys &ph, const RunParams &P,
                                               const SynchConst &sc,
                                  Smem &sm, long long off, int n, int stage, int mode, double dt, double t,
-                                 StepStats &st) {
+                                 StepStats &st, const mlp::InferSmem *inf) {
     const int tid = threadIdx.x;
     const int ng = ph.ngst, iL = ng - 1, iR = n - ng;
     const double w0 = stage == 2 ? 3. / 4. : 1. / 3.;
@@ -370,10 +393,18 @@ struct TrackStep {
           run_min = fmin(run_min, T.dtl[g]);
           T.dtl[g] = DT_INF;
         }
+      }
 
-        if (mode == 1 && i >= iL + 1 && i <= iR - 1) {
-          // Cell::update (cell.cpp:102-127)
-          double prim[NQ], cons[NQ];
+      if (mode == 1) {
+        // Cell::update (cell.cpp:102-127).  Written as straight-line blocks
+        // under `upd` so that, with the learned guess, the whole warp meets at
+        // each inference.
+        const bool upd = i >= iL + 1 && i <= iR - 1;
+        const long long g = off + i;
+        double prim[NQ], cons[NQ];
+        Geom G1;
+        C2PStats cs;
+        if (upd) {
 #pragma unroll
           for (int s = 0; s < NQS; ++s) prim[Slots<Cfg>::q_of(s)] = sm.cp[s][c];
           prim[UU2] = 0.;
@@ -402,7 +433,7 @@ struct TrackStep {
             cons[GMX] += dg;
             cons[GMN] += dg;
           }
-          const Geom G1 = geom_between<Cfg>(sm.xnew[tid], sm.xnew[tid + 1]);
+          G1 = geom_between<Cfg>(sm.xnew[tid], sm.xnew[tid + 1]);
           if (Cfg::FAST) {
             const double rdV1 = 1. / G1.dV;
 #pragma unroll
@@ -411,13 +442,14 @@ struct TrackStep {
 #pragma unroll
             for (int q = 0; q < NQ; ++q) cons[q] /= G1.dV;
           }
-          C2PStats cs;
+        }
+        if (GUESS) learned_guess(*inf, cons, prim, upd);
+        if (upd) {
           cons2prim<Cfg>(ph, cons, prim, &cs);
-          st.c2p_calls++;
-          st.c2p_iters += cs.iters;
-          st.c2p_fallbacks += cs.fallback;
-          st.c2p_max_iters = max(st.c2p_max_iters, cs.iters);
-          if (stage > 1) {  // RK3 combine (rk3.cpp:27-55, 63-92)
+          count_c2p(st, cs);
+        }
+        if (stage > 1) {
+          if (upd) {  // RK3 combine (rk3.cpp:27-55, 63-92)
 #pragma unroll
             for (int s = 0; s < NQS; ++s) {
               const int q = Slots<Cfg>::q_of(s);
@@ -432,12 +464,14 @@ struct TrackStep {
 #pragma unroll
               for (int q = 0; q < NQ; ++q) cons[q] /= G2.dV;
             }
-            cons2prim<Cfg>(ph, cons, prim, &cs);
-            st.c2p_calls++;
-            st.c2p_iters += cs.iters;
-            st.c2p_fallbacks += cs.fallback;
-            st.c2p_max_iters = max(st.c2p_max_iters, cs.iters);
           }
+          if (GUESS) learned_guess(*inf, cons, prim, upd);
+          if (upd) {
+            cons2prim<Cfg>(ph, cons, prim, &cs);
+            count_c2p(st, cs);
+          }
+        }
+        if (upd) {
           if (Cfg::SYNCH && stage == 3) {  // radiation_injectParticles, active cells
             inject_particles<Cfg>(ph, sc, prim, T.shocked[g] != 0, T.pspec[g]);
           }
@@ -490,7 +524,7 @@ struct TrackStep {
 
   // --- one full step of run r ---------------------------------------------
   __device__ static void step(const Tracks &T, const Phys &ph, Smem &sm, uint32_t *words, int r, StepStats &st,
-                              bool regrid_only) {
+                              bool regrid_only, const mlp::InferSmem *inf) {
     const long long off = T.off[r];
     const RunParams P = T.par[r];
     const SynchConst sc{P.Nalpha, P.Nmp, P.Nme};
@@ -522,23 +556,23 @@ struct TrackStep {
     edge_geom(T, sm, off, n, ng, 1);
     ghosts(T, ph, P, off, n, sm.edge, t);
     __syncthreads();
-    double m = sweep(T, ph, P, sc, sm, off, n, 1, 0, 0., t, st);
+    double m = sweep(T, ph, P, sc, sm, off, n, 1, 0, 0., t, st, inf);
     m = block_min(sm, m);
     const double dt = ph.cfl * m;
     // stage 1 update
-    sweep(T, ph, P, sc, sm, off, n, 1, 1, dt, t, st);
+    sweep(T, ph, P, sc, sm, off, n, 1, 1, dt, t, st, inf);
     __syncthreads();
     // stage 2
     edge_geom(T, sm, off, n, ng, 2);
     ghosts(T, ph, P, off, n, sm.edge, t);
     __syncthreads();
-    sweep(T, ph, P, sc, sm, off, n, 2, 1, dt, t, st);
+    sweep(T, ph, P, sc, sm, off, n, 2, 1, dt, t, st, inf);
     __syncthreads();
     // stage 3
     edge_geom(T, sm, off, n, ng, 3);
     ghosts(T, ph, P, off, n, sm.edge, t);
     __syncthreads();
-    sweep(T, ph, P, sc, sm, off, n, 3, 1, dt, t, st);
+    sweep(T, ph, P, sc, sm, off, n, 3, 1, dt, t, st, inf);
     __syncthreads();
 
     // step-end cell geometry: ghosts 0 and n-1 keep the stage-3 ghost copies,
@@ -581,13 +615,22 @@ struct TrackStep {
   }
 };
 
-template <class Cfg, int BS>
-__global__ void __launch_bounds__(BS, Cfg::MIN_BLOCKS) track_step_kernel(Tracks T, Phys ph, int nsteps, const int *order, int nruns,
-                                                         int *queue, StepStats *stats, int regrid_only) {
-  using TS = TrackStep<Cfg, BS>;
+// Dynamic shared memory: TrackStep::Smem, the regrid bit words (words_bytes),
+// then, with GUESS, the tensor-core weights of the learned guess.
+template <class Cfg, int BS, bool GUESS = false>
+__global__ void __launch_bounds__(BS, Cfg::MIN_BLOCKS)
+    track_step_kernel(Tracks T, Phys ph, int nsteps, const int *order, int nruns, int *queue, StepStats *stats,
+                      int regrid_only, unsigned words_bytes) {
+  using TS = TrackStep<Cfg, BS, GUESS>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typename TS::Smem &sm = *reinterpret_cast<typename TS::Smem *>(smem_raw);
   uint32_t *words = reinterpret_cast<uint32_t *>(smem_raw + sizeof(typename TS::Smem));
+  mlp::InferSmem *inf = nullptr;
+  if (GUESS) {
+    inf = reinterpret_cast<mlp::InferSmem *>(smem_raw + ((sizeof(typename TS::Smem) + words_bytes + 15u) & ~size_t(15)));
+    mlp::load_infer_weights(T.mlp, *inf);
+    __syncthreads();
+  }
   StepStats st{};
   __shared__ int s_item, s_status;
   for (;;) {
@@ -604,7 +647,7 @@ __global__ void __launch_bounds__(BS, Cfg::MIN_BLOCKS) track_step_kernel(Tracks 
       const int bad = s_status;
       __syncthreads();
       if (bad != 0) break;
-      TS::step(T, ph, sm, words, r, st, regrid_only != 0);
+      TS::step(T, ph, sm, words, r, st, regrid_only != 0, inf);
     }
   }
   // fold the per-thread statistics into the launch totals

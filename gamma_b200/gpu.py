@@ -32,6 +32,8 @@ EXPORTS = (
     "gamma_gpu_regrid", "gamma_gpu_step_tubes_noalloc",
     "gamma_gpu_download", "gamma_gpu_cons2prim", "gamma_gpu_stream", "gamma_gpu_strerror",
     "gamma_gpu_last_error", "gamma_gpu_destroy",
+    "gamma_mlp_param_count", "gamma_mlp_init", "gamma_mlp_pairs", "gamma_mlp_train", "gamma_mlp_forward",
+    "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess",
 )
 
 
@@ -66,6 +68,13 @@ class StepStats(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
+class MlpTrain(ctypes.Structure):
+    """gamma_mlp_train_t"""
+
+    _fields_ = [("epochs", ctypes.c_int), ("batch", ctypes.c_int), ("lr", ctypes.c_float),
+                ("lr_final", ctypes.c_float), ("seed", ctypes.c_ulonglong)]
 
 
 def config_sph(gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=EOS_IDEAL) -> Config:
@@ -110,8 +119,20 @@ def lib() -> ctypes.CDLL:
         L.gamma_gpu_last_error.restype = ctypes.c_char_p
         L.gamma_gpu_last_error.argtypes = [ctypes.c_void_p]
         L.gamma_gpu_destroy.argtypes = [ctypes.c_void_p]
+        v = ctypes.c_void_p
+        L.gamma_mlp_param_count.argtypes = []
+        L.gamma_mlp_init.argtypes = [v, ctypes.c_ulonglong, v]
+        L.gamma_mlp_pairs.argtypes = [ctypes.POINTER(Config), v, ctypes.c_longlong, ctypes.c_longlong,
+                                      ctypes.c_ulonglong, v, v, v]
+        L.gamma_mlp_train.argtypes = [v, v, v, ctypes.c_longlong, ctypes.POINTER(MlpTrain),
+                                      ctypes.POINTER(ctypes.c_float), v]
+        L.gamma_mlp_forward.argtypes = [v, v, ctypes.c_longlong, v, ctypes.c_int, v]
+        L.gamma_gpu_cons2prim_guess.argtypes = [ctypes.POINTER(Config), v, v, ctypes.c_int, v, v, v]
+        L.gamma_gpu_set_guess.argtypes = [v, v]
         for name in ("gamma_gpu_create", "gamma_gpu_layout", "gamma_gpu_set_params", "gamma_gpu_upload",
-                     "gamma_gpu_step", "gamma_gpu_regrid", "gamma_gpu_download", "gamma_gpu_cons2prim"):
+                     "gamma_gpu_step", "gamma_gpu_regrid", "gamma_gpu_download", "gamma_gpu_cons2prim",
+                     "gamma_mlp_param_count", "gamma_mlp_init", "gamma_mlp_pairs", "gamma_mlp_train",
+                     "gamma_mlp_forward", "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess"):
             getattr(L, name).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -189,6 +210,11 @@ class GammaGPU:
         self._check(lib().gamma_gpu_step(self.h, int(nsteps), ctypes.byref(st) if stats else None))
         return st.as_dict() if stats else None
 
+    def set_guess(self, params_ptr: int):
+        """Learned cons2prim starting pressure in every step (device parameter
+        pointer), or 0 for the warm start of the reference."""
+        self._check(lib().gamma_gpu_set_guess(self.h, ctypes.c_void_p(params_ptr) if params_ptr else None))
+
     def regrid(self):
         st = StepStats()
         self._check(lib().gamma_gpu_regrid(self.h, ctypes.byref(st)))
@@ -242,3 +268,50 @@ def step_tubes_noalloc(cfg: Config, nruns: int, total: int, offsets_ptr: int, ca
     if rc != GAMMA_OK:
         raise GammaError(rc)
     return st.as_dict() if stats else None
+
+
+def _ok(rc):
+    if rc != GAMMA_OK:
+        raise GammaError(rc)
+
+
+def mlp_param_count() -> int:
+    return int(lib().gamma_mlp_param_count())
+
+
+def mlp_init(params_ptr: int, seed: int, stream: int = 0):
+    _ok(lib().gamma_mlp_init(ctypes.c_void_p(params_ptr), ctypes.c_ulonglong(seed),
+                             ctypes.c_void_p(stream) if stream else None))
+
+
+def mlp_pairs(cfg: Config, prim_ptr: int, n_states: int, n_uniform: int, seed: int, x_ptr: int, y_ptr: int,
+              stream: int = 0):
+    """Training pairs (x [n][3], y [n][2] floats) from n_states device primitive
+    states [nq][n_states] followed by n_uniform drawn states."""
+    _ok(lib().gamma_mlp_pairs(ctypes.byref(cfg), ctypes.c_void_p(prim_ptr) if prim_ptr else None, int(n_states),
+                              int(n_uniform), ctypes.c_ulonglong(seed), ctypes.c_void_p(x_ptr),
+                              ctypes.c_void_p(y_ptr), ctypes.c_void_p(stream) if stream else None))
+
+
+def mlp_train(params_ptr: int, x_ptr: int, y_ptr: int, n: int, epochs: int = 8, batch: int = 8192,
+              lr: float = 3e-3, lr_final: float = 1e-4, seed: int = 7, stream: int = 0) -> np.ndarray:
+    """Mini-batch Adam; returns the mean training loss of each epoch."""
+    tc = MlpTrain(int(epochs), int(batch), float(lr), float(lr_final), int(seed))
+    loss = np.zeros(max(int(epochs), 1), dtype=np.float32)
+    _ok(lib().gamma_mlp_train(ctypes.c_void_p(params_ptr), ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), int(n),
+                              ctypes.byref(tc), loss.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                              ctypes.c_void_p(stream) if stream else None))
+    return loss[:int(epochs)]
+
+
+def mlp_forward(params_ptr: int, x_ptr: int, n: int, out_ptr: int, tensor_cores: bool, stream: int = 0):
+    _ok(lib().gamma_mlp_forward(ctypes.c_void_p(params_ptr), ctypes.c_void_p(x_ptr), int(n), ctypes.c_void_p(out_ptr),
+                                1 if tensor_cores else 0, ctypes.c_void_p(stream) if stream else None))
+
+
+def cons2prim_guess_device(cfg: Config, cons_ptr: int, prim_ptr: int, n: int, params_ptr: int, iters_ptr: int = 0,
+                           stream: int = 0):
+    """cons2prim on device arrays [nq][n] started from the network's pressure."""
+    _ok(lib().gamma_gpu_cons2prim_guess(ctypes.byref(cfg), ctypes.c_void_p(cons_ptr), ctypes.c_void_p(prim_ptr),
+                                        int(n), ctypes.c_void_p(iters_ptr) if iters_ptr else None,
+                                        ctypes.c_void_p(params_ptr), ctypes.c_void_p(stream) if stream else None))

@@ -165,6 +165,53 @@ int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg, int nruns, long long
                                  double *prim, double *x, double *dx, double *dt_loc, double *xI,
                                  int nsteps, void *stream, gamma_step_stats_t *stats);
 
+/* ---- Learned cons2prim guess ------------------------------------------------
+ * No counterpart in the reference, whose cons2prim always starts its Brent
+ * search from the cell's previous pressure (rel_sph.cpp:243-250).  A
+ * 3 -> 64 -> 64 -> 2 SiLU network maps a conserved state to a starting
+ * pressure; the Newton iteration still runs to the same tolerance, so only the
+ * iteration count changes.  Parameters: gamma_mlp_param_count() floats in
+ * DEVICE memory.  Inputs per state (x, [n][3] floats): log1p(|S|/D)/8,
+ * log10 of the thermal part of tau/D (tau/D - sqrt(1+(S/D)^2) + 1)/10,
+ * log10(D)/6.  Outputs (y, [n][2]): (ln(p/D)+14)/10 and ln(lfac)/3. */
+typedef struct {
+  int epochs;
+  int batch;                /* samples per Adam step */
+  float lr, lr_final;       /* cosine decay from lr to lr_final over all steps */
+  unsigned long long seed;  /* sample order of each epoch */
+} gamma_mlp_train_t;
+
+int gamma_mlp_param_count(void);
+
+/* Glorot-uniform weights, zero biases (device pointer). */
+int gamma_mlp_init(float *params, unsigned long long seed, void *stream);
+
+/* Training pairs: the first n_states from primitive states prim ([nq][n_states],
+ * device, reference slot order), then n_uniform states drawn with
+ * ln lfac ~ U(0, ln 1e3), log10 p/rho ~ U(-10, 3), log10 rho ~ U(-6, 6). */
+int gamma_mlp_pairs(const gamma_config_t *cfg, const double *prim, long long n_states, long long n_uniform,
+                    unsigned long long seed, float *x, float *y, void *stream);
+
+/* Mini-batch Adam on the mean squared error (device x, y, params).
+ * loss_per_epoch (host, may be NULL): mean training loss of each epoch.
+ * Allocates its optimiser state for the duration of the call and waits. */
+int gamma_mlp_train(float *params, const float *x, const float *y, long long n, const gamma_mlp_train_t *tc,
+                    float *loss_per_epoch, void *stream);
+
+/* Network outputs for n inputs: FP32 (tensor_cores = 0) or the BF16
+ * tensor-core path used inside the step (tensor_cores = 1). */
+int gamma_mlp_forward(const float *params, const float *x, long long n, float *out, int tensor_cores,
+                      void *stream);
+
+/* gamma_gpu_cons2prim started from the network's pressure instead of prim's. */
+int gamma_gpu_cons2prim_guess(const gamma_config_t *cfg, double *cons, double *prim, int n, int *iters,
+                              const float *params, void *stream);
+
+/* Use the network's starting pressure in every cons2prim of gamma_gpu_step
+ * (params: device pointer that stays valid while in use), or NULL for the
+ * reference's warm start.  Merges during regrid keep the warm start. */
+int gamma_gpu_set_guess(gamma_ctx_t *ctx, const float *params);
+
 /* The context's CUDA stream (a cudaStream_t). */
 void *gamma_gpu_stream(gamma_ctx_t *ctx);
 

@@ -12,7 +12,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     src = open(os.path.join(ROOT, "include", "gamma_gpu.h")).read()
-    return sorted(set(re.findall(r"\b(gamma_gpu_\w+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(gamma_(?:gpu|mlp)_\w+)\s*\(", src)))
 
 
 def test_header_matches_binding_list():

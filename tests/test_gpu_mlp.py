@@ -1,0 +1,263 @@
+"""The learned cons2prim guess: network kernels, training, and its use inside
+cons2prim and the step.
+
+The guess only moves where the Newton iteration starts; the root it converges
+to is the same.  So results with the guess are compared with results without
+it (and with the converged oracle) at the parity tolerances, while the
+iteration counts are what the network changes.
+"""
+import numpy as np
+import pytest
+
+from helpers import l1_rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _silu(z):
+    return z / (1.0 + np.exp(-z))
+
+
+def _unpack(P):
+    H = 64
+    W1 = P[:3 * H].reshape(H, 3)
+    b1 = P[3 * H:4 * H]
+    o = 4 * H
+    W2 = P[o:o + H * H].reshape(H, H)
+    b2 = P[o + H * H:o + H * H + H]
+    o2 = o + H * H + H
+    W3 = P[o2:o2 + 2 * H].reshape(2, H)
+    b3 = P[o2 + 2 * H:o2 + 2 * H + 2]
+    return W1, b1, W2, b2, W3, b3
+
+
+def _forward_np(P, x, cast=lambda a: a):
+    W1, b1, W2, b2, W3, b3 = _unpack(P.astype(np.float64))
+    h1 = cast(_silu(cast(x) @ cast(W1).T + b1))
+    h2 = cast(_silu(h1 @ cast(W2).T + b2))
+    return h2 @ cast(W3).T + b3
+
+
+def _bf16(a):
+    """round to bfloat16 (nearest even) and back"""
+    u = np.asarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def _params(seed=11):
+    import torch
+
+    from gamma_b200 import gpu
+    P = torch.zeros(gpu.mlp_param_count(), dtype=torch.float32, device="cuda")
+    gpu.mlp_init(P.data_ptr(), seed)
+    torch.cuda.synchronize()
+    return P
+
+
+def test_forward_fp32_and_tensor_core_paths(gpu_available):
+    import torch
+
+    from gamma_b200 import gpu
+    P = _params()
+    rng = np.random.default_rng(1)
+    n = 10_001  # not a multiple of the 32-cell warp tile
+    x = rng.uniform(-1.5, 1.5, (n, 3)).astype(np.float32)
+    dx = torch.tensor(x, device="cuda")
+    out = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+    Ph = P.cpu().numpy()
+    gpu.mlp_forward(P.data_ptr(), dx.data_ptr(), n, out.data_ptr(), tensor_cores=False)
+    torch.cuda.synchronize()
+    want = _forward_np(Ph, x.astype(np.float64))
+    got = out.cpu().numpy()
+    assert np.max(np.abs(got - want)) <= 1e-5 * max(1.0, np.max(np.abs(want)))
+    # BF16 operands, FP32 accumulation: compare with the same roundings on the host
+    gpu.mlp_forward(P.data_ptr(), dx.data_ptr(), n, out.data_ptr(), tensor_cores=True)
+    torch.cuda.synchronize()
+    want_b = _forward_np(Ph, x.astype(np.float64), cast=_bf16)
+    got_b = out.cpu().numpy()
+    assert np.max(np.abs(got_b - want_b)) <= 5e-3
+    # and the BF16 path stays near the FP32 network
+    assert np.max(np.abs(got_b - want)) <= 5e-2
+
+
+def test_training_pairs_from_states(gpu_available):
+    import torch
+
+    from gamma_b200 import gpu
+    rng = np.random.default_rng(2)
+    n = 4096
+    G = 5.0 / 3.0
+    lg = np.exp(rng.uniform(0, np.log(50.0), n))
+    u = np.sqrt(lg ** 2 - 1) * rng.choice([-1, 1], n)
+    rho = 10 ** rng.uniform(-3, 3, n)
+    p = rho * 10 ** rng.uniform(-6, 2, n)
+    prim = np.zeros((6, n))
+    prim[0], prim[1], prim[2], prim[4] = rho, p, u, 1.0
+    nu = 50_000
+    dprim = torch.tensor(prim, device="cuda")
+    x = torch.zeros((n + nu, 3), dtype=torch.float32, device="cuda")
+    y = torch.zeros((n + nu, 2), dtype=torch.float32, device="cuda")
+    gpu.mlp_pairs(gpu.config_cart(), dprim.data_ptr(), n, nu, 5, x.data_ptr(), y.data_ptr())
+    torch.cuda.synchronize()
+    xh, yh = x.cpu().numpy().astype(np.float64), y.cpu().numpy().astype(np.float64)
+    h = 1 + G / (G - 1) * p / rho
+    D = rho * lg
+    S = rho * h * lg * u
+    tau = rho * h * lg ** 2 - p - D
+    s = np.abs(S) / D
+    th = tau / D - (np.sqrt(1 + s * s) - 1)
+    want_x = np.stack([np.log1p(s) / 8, np.log10(th) / 10, np.log10(D) / 6], axis=1)
+    want_y = np.stack([(np.log(p / D) + 14) / 10, np.log(lg) / 3], axis=1)
+    assert np.allclose(xh[:n], want_x, rtol=1e-5, atol=1e-6)
+    assert np.allclose(yh[:n], want_y, rtol=1e-5, atol=1e-6)
+    # drawn states: p/rho = exp(10 y0 - 14 + 3 y1) in [1e-10, 1e3], lfac in [1, 1e3]
+    assert np.all(np.isfinite(xh)) and np.all(np.isfinite(yh))
+    pr = 10 * yh[n:, 0] - 14 + 3 * yh[n:, 1]
+    assert pr.min() >= np.log(1e-10) - 1e-3 and pr.max() <= np.log(1e3) + 1e-3
+    assert yh[n:, 1].min() >= -1e-6 and yh[n:, 1].max() <= np.log(1e3) / 3 + 1e-6
+
+
+@pytest.fixture(scope="module")
+def trained(gpu_available):
+    """A network trained on tube states (after 20 steps) and drawn states."""
+    import torch
+
+    from gamma_b200 import gpu, problems
+    setups = [problems.TubeSetup(ncell=n, vL=v, vR=v, rhoL=r) for n, v, r in
+              ((512, 0.0, 10.0), (700, 0.4, 9.0), (1000, -0.45, 11.0), (900, 0.2, 10.5))]
+    g = gpu.GammaGPU(gpu.config_cart(), [s.capacity for s in setups])
+    pk = problems.pack([s.initial_state() for s in setups], g.offsets, g.total, 6)
+    g.upload(pk["ntrack"], pk["prim"], pk["x"], pk["dx"], pk["xI"], pk["dt_loc"], pk["t"], pk["it"])
+    g.step(20)
+    out = g.download()
+    g.close()
+    states = np.ascontiguousarray(out["prim"][:, np.concatenate(
+        [np.arange(o, o + n) for o, n in zip(g.offsets, out["ntrack"])])])
+    ns, nu = states.shape[1], 600_000
+    dst = torch.tensor(states, device="cuda")
+    x = torch.zeros((ns + nu, 3), dtype=torch.float32, device="cuda")
+    y = torch.zeros((ns + nu, 2), dtype=torch.float32, device="cuda")
+    gpu.mlp_pairs(gpu.config_cart(), dst.data_ptr(), ns, nu, 9, x.data_ptr(), y.data_ptr())
+    P = _params(3)
+    loss = gpu.mlp_train(P.data_ptr(), x.data_ptr(), y.data_ptr(), ns + nu, epochs=8, batch=4096, lr=3e-3,
+                         lr_final=1e-4, seed=4)
+    torch.cuda.synchronize()
+    return P, loss
+
+
+def test_training_reduces_loss(trained):
+    import torch
+
+    from gamma_b200 import gpu
+    P, loss = trained
+    print("loss per epoch", loss)
+    assert np.all(np.isfinite(loss))
+    assert loss[-1] < 0.2 * loss[0]
+    # held-out drawn states: the guessed ln p is close to the truth
+    nu = 100_000
+    x = torch.zeros((nu, 3), dtype=torch.float32, device="cuda")
+    y = torch.zeros((nu, 2), dtype=torch.float32, device="cuda")
+    out = torch.zeros((nu, 2), dtype=torch.float32, device="cuda")
+    gpu.mlp_pairs(gpu.config_cart(), 0, 0, nu, 12345, x.data_ptr(), y.data_ptr())
+    gpu.mlp_forward(P.data_ptr(), x.data_ptr(), nu, out.data_ptr(), tensor_cores=True)
+    torch.cuda.synchronize()
+    err = np.abs(out.cpu().numpy()[:, 0] - y.cpu().numpy()[:, 0]) * 10  # |ln p_guess - ln p|
+    print("median |d ln p|", np.median(err), "p90", np.percentile(err, 90))
+    assert np.median(err) < 0.5
+
+
+def test_cons2prim_from_guess_matches_oracle(trained):
+    import torch
+
+    from gamma_b200 import gpu
+    from oracle import port
+    P, _ = trained
+    rng = np.random.default_rng(8)
+    n = 50_000
+    lg = np.exp(rng.uniform(0, np.log(100.), n))
+    u = np.sqrt(lg ** 2 - 1) * rng.choice([-1, 1], n)
+    rho = 10 ** rng.uniform(-4, 4, n)
+    p = rho * 10 ** rng.uniform(-6, 2, n)
+    prim = np.zeros((6, n))
+    prim[0], prim[1], prim[2], prim[4] = rho, p, u, 1.0
+    ps = port.PortSim(port.tube_config(c2p_epsrel=1e-15))
+    cons = ps.prim2cons(prim)
+    cold = prim.copy()
+    cold[1] = 1.0  # no warm start
+    rp, _, _ = ps.cons2prim(cons, prim.copy())
+    res = {}
+    for name in ("cold", "guess"):
+        dc = torch.tensor(cons, device="cuda")
+        dp = torch.tensor(cold, device="cuda")
+        it = torch.zeros(n, dtype=torch.int32, device="cuda")
+        if name == "cold":
+            gpu.cons2prim_device(gpu.config_cart(), dc.data_ptr(), dp.data_ptr(), n, it.data_ptr())
+        else:
+            gpu.cons2prim_guess_device(gpu.config_cart(), dc.data_ptr(), dp.data_ptr(), n, P.data_ptr(),
+                                       it.data_ptr())
+        torch.cuda.synchronize()
+        gp = dp.cpu().numpy()
+        E = cons[0] + cons[1]
+        cond = 1e-12 + 64 * 2.2e-16 * lg ** 2
+        assert np.all(np.abs(gp[0] - rp[0]) / rp[0] <= cond), name
+        assert np.all(np.abs(gp[2] - rp[2]) / np.maximum(np.abs(rp[2]), 1e-12) <= cond), name
+        assert np.max(np.abs(gp[1] - rp[1]) / np.maximum(rp[1], 1e-2 * E)) <= 1e-12, name
+        res[name] = it.cpu().numpy()
+    print("mean Newton iterations: cold", res["cold"].mean(), "guess", res["guess"].mean(),
+          "max", res["cold"].max(), res["guess"].max())
+    assert res["guess"].mean() < res["cold"].mean()
+    assert res["guess"].max() < 100
+
+
+def test_step_with_guess_matches_plain_step(trained):
+    from gamma_b200 import gpu, problems
+    P, _ = trained
+    setups = [problems.TubeSetup(ncell=n, vL=v, vR=v, rhoL=r) for n, v, r in
+              ((300, 0.1, 10.0), (777, -0.3, 9.5), (1500, 0.45, 10.5))]
+    outs, stats = [], []
+    for use in (False, True):
+        g = gpu.GammaGPU(gpu.config_cart(), [s.capacity for s in setups])
+        pk = problems.pack([s.initial_state() for s in setups], g.offsets, g.total, 6)
+        g.upload(pk["ntrack"], pk["prim"], pk["x"], pk["dx"], pk["xI"], pk["dt_loc"], pk["t"], pk["it"])
+        if use:
+            g.set_guess(P.data_ptr())
+        st = g.step(50)
+        assert st["status"] == 0 and st["c2p_fallbacks"] == 0
+        outs.append([problems.unpack(g.download(), r, g.offsets) for r in range(len(setups))])
+        stats.append(st)
+        g.close()
+    print("plain", stats[0]["c2p_iters"] / stats[0]["c2p_calls"], "guess",
+          stats[1]["c2p_iters"] / stats[1]["c2p_calls"])
+    assert stats[0]["zone_updates"] == stats[1]["zone_updates"]
+    for a, b in zip(outs[0], outs[1]):
+        assert a.ntrack == b.ntrack
+        s = slice(2, a.ntrack - 2)
+        for q in (0, 1, 2, 4):
+            assert l1_rel(b.prim[q, s], a.prim[q, s]) <= 1e-10, q
+        assert l1_rel(b.xI, a.xI) <= 1e-10
+
+
+def test_bm1d_step_with_guess_matches_plain_step(trained):
+    """Spherical blast wave (NUM_Q = 10, synchrotron tracers) with the network
+    trained on tube states: the guess is poorer there, the results the same."""
+    from gamma_b200 import gpu, problems
+    P, _ = trained
+    s = problems.Bm1dSetup(eta=1e-10, lorentz_mode=1, lfac_shock2=1e4, ncell=800, nmax=1600, grid_log=1)
+    outs = []
+    for use in (False, True):
+        g = gpu.GammaGPU(gpu.config_sph(), [s.capacity])
+        g.set_params([s.run_params()])
+        pk = problems.pack([s.initial_state()], g.offsets, g.total, 10)
+        g.upload(pk["ntrack"], pk["prim"], pk["x"], pk["dx"], pk["xI"], pk["dt_loc"], pk["t"], pk["it"])
+        if use:
+            g.set_guess(P.data_ptr())
+        st = g.step(30)
+        assert st["status"] == 0
+        outs.append(problems.unpack(g.download(), 0, g.offsets))
+        g.close()
+    a, b = outs
+    assert a.ntrack == b.ntrack
+    s_ = slice(2, a.ntrack - 2)
+    for q in (0, 1, 2):
+        assert l1_rel(b.prim[q, s_], a.prim[q, s_]) <= 1e-9, q
