@@ -201,6 +201,72 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+def learned_arm(args, g, pk, upload, stream, plain_prim, zones_per_step, plain_per_launch, plain_stats,
+                max_over_ranks, barrier, ws):
+    """The same workload with the learned cons2prim starting pressure.
+
+    The network is trained here (training pairs: 1M states of the tubes after
+    the timed steps plus 1M drawn states); the result after K steps is compared
+    with the plain run's (L1 over all cells and stored slots)."""
+    import torch
+
+    from gamma_b200 import gpu
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t0 = time.perf_counter()
+    out = g.download()
+    rng = np.random.default_rng(SEED)
+    live = np.concatenate([np.arange(o, o + n) for o, n in zip(g.offsets, out["ntrack"])])
+    pick = np.sort(rng.choice(live, size=min(1_000_000, live.size), replace=False))
+    states = torch.tensor(np.ascontiguousarray(out["prim"][:, pick]), device=dev)
+    ns, nu = states.shape[1], 1_000_000
+    x = torch.zeros((ns + nu, 3), dtype=torch.float32, device=dev)
+    y = torch.zeros((ns + nu, 2), dtype=torch.float32, device=dev)
+    gpu.mlp_pairs(gpu.config_cart(), states.data_ptr(), ns, nu, SEED, x.data_ptr(), y.data_ptr())
+    P = torch.zeros(gpu.mlp_param_count(), dtype=torch.float32, device=dev)
+    gpu.mlp_init(P.data_ptr(), SEED)
+    loss = gpu.mlp_train(P.data_ptr(), x.data_ptr(), y.data_ptr(), ns + nu, epochs=6, batch=8192)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+
+    g.set_guess(P.data_ptr())
+    # results: K steps from the initial state, against the plain run's K steps
+    upload()
+    g.step(args.steps, stats=False)
+    got = g.download()["prim"]
+    rows = [0, 1, 2, 4, 5]
+    want = plain_prim.numpy()
+    l1 = max(float(np.sum(np.abs(got[q] - want[q])) / max(np.sum(np.abs(want[q])), 1e-300)) for q in rows)
+    # timing: same protocol as the plain arm
+    upload()
+    for _ in range(args.warmup):
+        g.step(1, stats=False)
+    st = g.step(1)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for k in range(args.steps):
+            g.step(1, stats=False)
+            ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(sum(ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)))
+    g.set_guess(0)
+    return {
+        "value": ws * zones_per_step * args.steps / (ms / 1e3), "unit": "zone-updates/s",
+        "ms_per_step": ms / args.steps,
+        "mean_newton_iters": st["c2p_iters"] / max(st["c2p_calls"], 1), "max_newton_iters": st["c2p_max_iters"],
+        "fallbacks": st["c2p_fallbacks"],
+        "plain_mean_newton_iters": plain_stats["c2p_iters"] / max(plain_stats["c2p_calls"], 1),
+        "l1_vs_plain": l1, "steps_compared": args.steps,
+        "training": {"pairs": ns + nu, "from_states": ns, "drawn": nu, "epochs": len(loss),
+                     "final_loss": float(loss[-1]), "seconds": train_s},
+        "note": "network start replaces the previous-step pressure in every cons2prim of the step; "
+                "Newton still converges to the reference tolerance",
+    }
+
+
 def run_gpu_arm(args):
     import torch
 
@@ -305,6 +371,9 @@ def run_gpu_arm(args):
         "c2p": {"mean_newton_iters": stats0["c2p_iters"] / max(stats0["c2p_calls"], 1),
                 "max_newton_iters": stats0["c2p_max_iters"], "fallbacks": stats0["c2p_fallbacks"]},
     }
+    if not args.no_learned:
+        line["learned_guess"] = learned_arm(args, g, pk, upload, stream, out_prim, zones_per_step, per_launch,
+                                            stats0, max_over_ranks, barrier, ws)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         setups_cpu = setups
         cores = os.cpu_count() or 1
@@ -325,6 +394,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gamma", choices=["gamma", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned cons2prim guess arm")
     ap.add_argument("--ntubes", type=int, default=NTUBES, help="smaller batches for profiling captures")
     args = ap.parse_args()
     if args.impl == "reference":
