@@ -1,0 +1,608 @@
+// C-ABI of the 2D (r, theta) moving-mesh step (include/gamma_gpu.h, gamma_2d_*).
+//
+// One context holds one run: NJ = ntheta + 2 ngst theta tracks of `cap` cells.
+// A step is a fixed sequence of kernels over all tracks (regrid, then per RK3
+// stage: ghosts, moving-direction interfaces, per-cell dt and neighbour lists,
+// transverse gradients, theta fluxes, dt reduction, interface move, cell
+// update), captured once into a CUDA graph and replayed.  The time step lives
+// in device memory, so nothing returns to the host between steps.
+#include "gamma_gpu.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "step2d.cuh"
+
+using namespace gb;
+using namespace gb::d2;
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct Stats2 {
+  unsigned long long c2p_calls, c2p_iters, c2p_fallbacks, c2p_max_iters, splits, merges, zone_updates;
+};
+
+__device__ void add_stats(Stats2 *S, unsigned long long calls, unsigned long long iters, unsigned long long fb,
+                          unsigned long long mx) {
+  for (int o = 16; o > 0; o >>= 1) {
+    calls += __shfl_xor_sync(0xffffffffu, calls, o);
+    iters += __shfl_xor_sync(0xffffffffu, iters, o);
+    fb += __shfl_xor_sync(0xffffffffu, fb, o);
+    const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, mx, o);
+    mx = m2 > mx ? m2 : mx;
+  }
+  if ((threadIdx.x & 31) == 0 && calls) {
+    atomicAdd(&S->c2p_calls, calls);
+    atomicAdd(&S->c2p_iters, iters);
+    if (fb) atomicAdd(&S->c2p_fallbacks, fb);
+    atomicMax(&S->c2p_max_iters, mx);
+  }
+}
+
+// Per active track (one block each): does any cell act against the first
+// active track's current target?  flags[j] = 1 if so.
+__global__ void k_regrid_check(Params2 P, Grid2 G, int *flags) {
+  __shared__ int s_any;
+  const int j = jL_of(G) + 1 + blockIdx.x;
+  if (threadIdx.x == 0) s_any = 0;
+  __syncthreads();
+  const Target T = track_target(G, jL_of(G) + 1);
+  if (regrid_needed(P, G, j, T, threadIdx.x, blockDim.x)) s_any = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    flags[j] = s_any;
+    if (j == jL_of(G) + 1) {  // the reference target of the other tracks if this one does not change
+      double *t0 = reinterpret_cast<double *>(flags + ((G.NJ + 1) & ~1));
+      t0[0] = T.rmin;
+      t0[1] = T.rmax;
+      t0[2] = (double)T.nact;
+    }
+  }
+}
+
+__global__ void k_regrid_live(Phys ph, Params2 P, Grid2 G, Stats2 *S, const int *flags) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (!flags[jL_of(G) + 1]) return;
+  unsigned long long c2p[4] = {0, 0, 0, 0}, ns = 0, nm = 0;
+  Target none{0., 0., 1};
+  regrid_track(ph, P, G, jL_of(G) + 1, true, none, &ns, &nm, c2p);
+  S->splits += ns;
+  S->merges += nm;
+  S->c2p_calls += c2p[0];
+  S->c2p_iters += c2p[1];
+  S->c2p_fallbacks += c2p[2];
+  if (c2p[3] > S->c2p_max_iters) S->c2p_max_iters = c2p[3];
+}
+
+// the other active tracks, one thread each, against the first active track
+__global__ void k_regrid_rest(Phys ph, Params2 P, Grid2 G, Stats2 *S, const int *flags) {
+  const int j = jL_of(G) + 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long c2p[4] = {0, 0, 0, 0}, ns = 0, nm = 0;
+  if (j <= jR_of(G) - 1) {
+    const Target T = track_target(G, jL_of(G) + 1);
+    const double *t0 = reinterpret_cast<const double *>(flags + ((G.NJ + 1) & ~1));
+    const bool same = T.rmin == t0[0] && T.rmax == t0[1] && (double)T.nact == t0[2];
+    if (flags[j] || !same) regrid_track(ph, P, G, j, false, T, &ns, &nm, c2p);
+  }
+  if (ns) atomicAdd(&S->splits, ns);
+  if (nm) atomicAdd(&S->merges, nm);
+  add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3]);
+}
+
+__global__ void k_ghosts(Grid2 G, int reset) {
+  const int j = blockIdx.x;
+  if (reset) ghosts_reset(G, j, threadIdx.x, blockDim.x);
+  __syncthreads();
+  ghosts_tracks(G, j, threadIdx.x, blockDim.x, reset != 0);
+  __syncthreads();
+  ghosts_cells(G, j, threadIdx.x, blockDim.x);
+}
+
+// flat (track, cell) index of a thread; false past the last cell
+__device__ __forceinline__ bool cell_of(const Grid2 &G, int *j, int *i) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.NC) return false;
+  *j = (int)(g / G.cap);
+  *i = (int)(g % G.cap);
+  return true;
+}
+
+__global__ void k_mv(Phys ph, Params2 P, Grid2 G) {
+  int j, i;
+  if (cell_of(G, &j, &i)) mv_interface(ph, P, G, j, i, *G.it);
+}
+
+__global__ void k_cellmv(Grid2 G) {
+  int j, i;
+  if (cell_of(G, &j, &i)) cell_mv(G, j, i);
+}
+
+__global__ void k_stale(Grid2 G) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) stale_table(G);
+}
+
+__global__ void k_tgrad(Grid2 G) {
+  int j, i;
+  if (cell_of(G, &j, &i)) trans_grad(G, j, i);
+}
+
+__global__ void k_f1own(Phys ph, Grid2 G) {
+  int j, i;
+  if (cell_of(G, &j, &i)) f1_own(ph, G, j, i);
+}
+
+__global__ void k_f1gather(Phys ph, Grid2 G) {
+  int j, i;
+  if (cell_of(G, &j, &i)) f1_gather(ph, G, j, i);
+}
+
+// detectShock and collect_dt: per-block minima, then one block
+__global__ void k_dtpart(Grid2 G) {
+  __shared__ double red[kThreads / 32];
+  int j, i;
+  double m = DT_INF;
+  if (cell_of(G, &j, &i)) m = collect_cell(G, j, i);
+  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < kThreads / 32; ++k) m = fmin(m, red[k]);
+    G.red[blockIdx.x] = fmin(red[0], m);
+  }
+}
+
+__global__ void k_dtfinal(Grid2 G, int nblocks, double cfl) {
+  __shared__ double red[kThreads / 32];
+  double m = DT_INF;
+  for (int k = threadIdx.x; k < nblocks; k += blockDim.x) m = fmin(m, G.red[k]);
+  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kThreads / 32; ++k) m = fmin(m, red[k]);
+    *G.dt = cfl * m;
+  }
+}
+
+__global__ void k_iface(Grid2 G, int stage) {
+  int j, i;
+  if (cell_of(G, &j, &i)) iface_move(G, j, i, stage);
+}
+
+__global__ void k_update(Phys ph, Params2 P, Grid2 G, int stage, Stats2 *S) {
+  int j, i;
+  unsigned long long c2p[4] = {0, 0, 0, 0};
+  if (cell_of(G, &j, &i)) update_cell(ph, P, G, j, i, stage, c2p);
+  add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3]);
+}
+
+__global__ void k_advance(Grid2 G, Stats2 *S) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  *G.t += *G.dt;
+  *G.it += 1;
+  unsigned long long z = 0;
+  for (int j = jL_of(G) + 1; j <= jR_of(G) - 1; ++j) z += (unsigned long long)(G.ntrack[j] - 2 * G.ngst);
+  S->zone_updates += z;
+}
+
+}  // namespace
+
+struct gamma_2d {
+  gamma_2d_config_t cfg{};
+  gamma_2d_params_t par{};
+  int NJ = 0, cap = 0;
+  long long NC = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<void *> allocs;
+  Grid2 G{};
+  Stats2 *d_stats = nullptr;
+  int *d_flags = nullptr;  // [NJ] regrid flags, then 3 doubles: the first active track's target
+  std::vector<double> tg;  // host copy of the per-track factors
+  std::string err;
+};
+
+namespace {
+
+int fail(gamma_2d *c, cudaError_t e, const char *what) {
+  if (c) c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return GAMMA_ERR_CUDA;
+}
+#define G2_CUDA(ctx, call)                              \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return fail(ctx, e_, #call); \
+  } while (0)
+
+Phys phys_of(const gamma_2d_config_t &c) {
+  Phys p;
+  p.gamma_ad = c.gamma_ad;
+  p.kgam = c.gamma_ad / (c.gamma_ad - 1.);
+  p.cfl = c.cfl;
+  p.vi = c.vi;
+  p.eos = c.eos;
+  p.ngst = c.ngst;
+  return p;
+}
+
+Params2 params_of(const gamma_2d_params_t &q) {
+  Params2 P;
+  P.split_DR = q.split_DR;
+  P.merge_DR = q.merge_DR;
+  P.split_DR_slow = q.split_DR_slow;
+  P.merge_DR_slow = q.merge_DR_slow;
+  P.v_out = q.v_out;
+  P.it_hold = q.it_hold;
+  P.Nalpha = q.Nalpha;
+  P.Nmp = q.Nmp;
+  P.Nme = q.Nme;
+  return P;
+}
+
+int blocks_of(long long n) { return (int)((n + kThreads - 1) / kThreads); }
+
+// The first part of a step: regrid, reset shocks, ghosts and the stage-1
+// fluxes (everything before collect_dt).
+int enqueue_prepare(gamma_2d *c) {
+  const Phys ph = phys_of(c->cfg);
+  const Params2 P = params_of(c->par);
+  const Grid2 &G = c->G;
+  cudaStream_t s = c->stream;
+  const int nb = blocks_of(c->NC);
+  const int nrest = std::max(1, c->cfg.ntheta - 1);
+  k_regrid_check<<<c->cfg.ntheta, kThreads, 0, s>>>(P, G, c->d_flags);
+  k_regrid_live<<<1, 32, 0, s>>>(ph, P, G, c->d_stats, c->d_flags);
+  k_regrid_rest<<<(nrest + 31) / 32, 32, 0, s>>>(ph, P, G, c->d_stats, c->d_flags);
+  k_ghosts<<<c->NJ, kThreads, 0, s>>>(G, 1);
+  k_mv<<<nb, kThreads, 0, s>>>(ph, P, G);
+  k_cellmv<<<nb, kThreads, 0, s>>>(G);
+  k_stale<<<1, 32, 0, s>>>(G);
+  k_tgrad<<<nb, kThreads, 0, s>>>(G);
+  k_f1own<<<nb, kThreads, 0, s>>>(ph, G);
+  k_f1gather<<<nb, kThreads, 0, s>>>(ph, G);
+  G2_CUDA(c, cudaGetLastError());
+  return GAMMA_OK;
+}
+
+// one step's launches on the context's stream
+int enqueue_step(gamma_2d *c) {
+  const Phys ph = phys_of(c->cfg);
+  const Params2 P = params_of(c->par);
+  const Grid2 &G = c->G;
+  cudaStream_t s = c->stream;
+  const int nb = blocks_of(c->NC);
+  const int nrest = std::max(1, c->cfg.ntheta - 1);
+  k_regrid_check<<<c->cfg.ntheta, kThreads, 0, s>>>(P, G, c->d_flags);
+  k_regrid_live<<<1, 32, 0, s>>>(ph, P, G, c->d_stats, c->d_flags);
+  k_regrid_rest<<<(nrest + 31) / 32, 32, 0, s>>>(ph, P, G, c->d_stats, c->d_flags);
+  for (int stage = 1; stage <= 3; ++stage) {
+    k_ghosts<<<c->NJ, kThreads, 0, s>>>(G, stage == 1);
+    k_mv<<<nb, kThreads, 0, s>>>(ph, P, G);
+    k_cellmv<<<nb, kThreads, 0, s>>>(G);
+    k_stale<<<1, 32, 0, s>>>(G);
+    k_tgrad<<<nb, kThreads, 0, s>>>(G);
+    k_f1own<<<nb, kThreads, 0, s>>>(ph, G);
+    k_f1gather<<<nb, kThreads, 0, s>>>(ph, G);
+    if (stage == 1) {
+      k_dtpart<<<nb, kThreads, 0, s>>>(G);
+      k_dtfinal<<<1, kThreads, 0, s>>>(G, nb, c->cfg.cfl);
+    }
+    k_iface<<<nb, kThreads, 0, s>>>(G, stage);
+    k_update<<<nb, kThreads, 0, s>>>(ph, P, G, stage, c->d_stats);
+  }
+  k_advance<<<1, 32, 0, s>>>(G, c->d_stats);
+  G2_CUDA(c, cudaGetLastError());
+  return GAMMA_OK;
+}
+
+}  // namespace
+
+#define GAMMA_API __attribute__((visibility("default")))
+
+extern "C" {
+
+GAMMA_API int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta, const double *dtheta,
+                              gamma_2d_t **out) {
+  if (!cfg || !out || !theta || !dtheta) return GAMMA_ERR_INVALID;
+  *out = nullptr;
+  if (cfg->ngst != 2 || cfg->ntheta < 1 || cfg->nmax < 8 || !(cfg->gamma_ad > 1.) || !(cfg->cfl > 0.) ||
+      cfg->nq != 10)
+    return GAMMA_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GAMMA_ERR_NO_DEVICE;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess || prop.major != 10) return GAMMA_ERR_NO_DEVICE;
+
+  gamma_2d *c = new gamma_2d();
+  c->cfg = *cfg;
+  const int ng = cfg->ngst;
+  c->NJ = cfg->ntheta + 2 * ng;
+  c->cap = cfg->nmax + 2 * ng;
+  c->NC = (long long)c->NJ * c->cap;
+  const long long NC = c->NC;
+  // per-track angular factors; ghost tracks as updateGhosts shifts them
+  // (2d.cpp:259-287: by the first active track's dtheta below, the last's above)
+  const int jL = ng - 1, jR = c->NJ - ng;
+  c->tg.assign((size_t)c->NJ * TG_WORDS, 0.);
+  for (int j = 0; j < c->NJ; ++j) {
+    double th, dth;
+    if (j <= jL) {
+      th = theta[0];
+      dth = dtheta[0];
+      th -= (jL - j + 1) * dtheta[0];
+    } else if (j >= jR) {
+      th = theta[cfg->ntheta - 1];
+      dth = dtheta[cfg->ntheta - 1];
+      th += (j - jR + 1) * dtheta[cfg->ntheta - 1];
+    } else {
+      th = theta[j - ng];
+      dth = dtheta[j - ng];
+    }
+    fill_track_geo(th, dth, &c->tg[(size_t)j * TG_WORDS]);
+  }
+
+  auto bail = [&](cudaError_t e, const char *what) {
+    fail(c, e, what);
+    gamma_2d_destroy(c);
+    return GAMMA_ERR_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+  if ((e = cudaEventCreate(&c->ev0)) != cudaSuccess) return bail(e, "event");
+  if ((e = cudaEventCreate(&c->ev1)) != cudaSuccess) return bail(e, "event");
+  auto alloc = [&](size_t bytes, void **p) -> cudaError_t {
+    cudaError_t ee = cudaMalloc(p, std::max<size_t>(bytes, 16));
+    if (ee == cudaSuccess) {
+      c->allocs.push_back(*p);
+      ee = cudaMemsetAsync(*p, 0, std::max<size_t>(bytes, 16), c->stream);
+    }
+    return ee;
+  };
+  Grid2 &G = c->G;
+  G.NJ = c->NJ;
+  G.cap = c->cap;
+  G.ngst = ng;
+  G.NC = NC;
+  const size_t d = sizeof(double), q = NQ;
+#define G2_ALLOC(ptr, bytes) \
+  if ((e = alloc((bytes), (void **)&(ptr))) != cudaSuccess) return bail(e, "cudaMalloc " #ptr)
+  double *tg_d;
+  G2_ALLOC(G.ntrack, c->NJ * sizeof(int));
+  G2_ALLOC(tg_d, c->tg.size() * d);
+  G.tg = tg_d;
+  G2_ALLOC(G.prim, q * NC * d);
+  G2_ALLOC(G.x, NC * d);
+  G2_ALLOC(G.dx, NC * d);
+  G2_ALLOC(G.dtl, NC * d);
+  G2_ALLOC(G.sd, NC * d);
+  G2_ALLOC(G.pspec, NC * d);
+  G2_ALLOC(G.shocked, NC);
+  G2_ALLOC(G.gmv, q * NC * d);
+  G2_ALLOC(G.gf1, q * NC * d);
+  G2_ALLOC(G.gf1n, q * NC * d);
+  G2_ALLOC(G.nbr, 4 * NC * sizeof(int));
+  G2_ALLOC(G.cons0, q * NC * d);
+  G2_ALLOC(G.dV0, NC * d);
+  G2_ALLOC(G.f1lo, q * NC * d);
+  G2_ALLOC(G.f1hi, q * NC * d);
+  G2_ALLOC(G.xI, NC * d);
+  G2_ALLOC(G.xI0, NC * d);
+  G2_ALLOC(G.xIm, NC * d);
+  G2_ALLOC(G.v, NC * d);
+  G2_ALLOC(G.lL, NC * d);
+  G2_ALLOC(G.lR, NC * d);
+  G2_ALLOC(G.flx, q * NC * d);
+  G2_ALLOC(G.stale_n, c->NJ * sizeof(int));
+  G2_ALLOC(G.stale_id, (size_t)c->NJ * KMAX_STALE * sizeof(int));
+  G2_ALLOC(G.t, d);
+  G2_ALLOC(G.dt, d);
+  G2_ALLOC(G.it, sizeof(long long));
+  G2_ALLOC(G.status, sizeof(int));
+  G2_ALLOC(G.red, (size_t)blocks_of(NC) * d);
+  G2_ALLOC(G.rprim, q * NC * d);
+  G2_ALLOC(G.rgmv, q * NC * d);
+  G2_ALLOC(G.rgf1, q * NC * d);
+  G2_ALLOC(G.rx, NC * d);
+  G2_ALLOC(G.rdx, NC * d);
+  G2_ALLOC(G.rdtl, NC * d);
+  G2_ALLOC(G.rxI, NC * d);
+  G2_ALLOC(G.rnbr, 4 * NC * sizeof(int));
+  G2_ALLOC(c->d_stats, sizeof(Stats2));
+  G2_ALLOC(c->d_flags, (size_t)c->NJ * sizeof(int) + 4 * d + 8);
+#undef G2_ALLOC
+  if ((e = cudaMemcpyAsync(tg_d, c->tg.data(), c->tg.size() * d, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+    return bail(e, "copy track factors");
+  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "sync");
+  *out = c;
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_2d_layout(const gamma_2d_t *ctx, int *ntracks, int *cap) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  if (ntracks) *ntracks = ctx->NJ;
+  if (cap) *cap = ctx->cap;
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_2d_set_params(gamma_2d_t *ctx, const gamma_2d_params_t *params) {
+  if (!ctx || !params) return GAMMA_ERR_INVALID;
+  ctx->par = *params;
+  if (ctx->exec) {  // the graph holds the old values: capture again on the next step
+    cudaGraphExecDestroy(ctx->exec);
+    cudaGraphDestroy(ctx->graph);
+    ctx->exec = nullptr;
+    ctx->graph = nullptr;
+  }
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_2d_upload(gamma_2d_t *ctx, const int *ntrack, const double *prim, const double *x,
+                              const double *dx, const double *dt_loc, const double *xI, const double *grad_mv,
+                              const double *grad_f1, const int *nbr, double t, long long it, int run_ghosts) {
+  if (!ctx || !ntrack || !prim || !x || !dx || !xI) return GAMMA_ERR_INVALID;
+  gamma_2d *c = ctx;
+  for (int j = 0; j < c->NJ; ++j)
+    if (ntrack[j] > c->cap || ntrack[j] < 2 * c->cfg.ngst + 3) return GAMMA_ERR_CAPACITY;
+  const Grid2 &G = c->G;
+  const size_t NC = (size_t)c->NC, d = sizeof(double);
+  cudaStream_t s = c->stream;
+  G2_CUDA(c, cudaMemcpyAsync(G.ntrack, ntrack, c->NJ * sizeof(int), cudaMemcpyHostToDevice, s));
+  G2_CUDA(c, cudaMemcpyAsync(G.prim, prim, NQ * NC * d, cudaMemcpyHostToDevice, s));
+  G2_CUDA(c, cudaMemcpyAsync(G.x, x, NC * d, cudaMemcpyHostToDevice, s));
+  G2_CUDA(c, cudaMemcpyAsync(G.dx, dx, NC * d, cudaMemcpyHostToDevice, s));
+  G2_CUDA(c, cudaMemcpyAsync(G.xI, xI, NC * d, cudaMemcpyHostToDevice, s));
+  std::vector<double> inf, neg, zero;
+  std::vector<int> nb0;
+  if (dt_loc) {
+    G2_CUDA(c, cudaMemcpyAsync(G.dtl, dt_loc, NC * d, cudaMemcpyHostToDevice, s));
+  } else {
+    inf.assign(NC, DT_INF);
+    G2_CUDA(c, cudaMemcpyAsync(G.dtl, inf.data(), NC * d, cudaMemcpyHostToDevice, s));
+  }
+  if (grad_mv) G2_CUDA(c, cudaMemcpyAsync(G.gmv, grad_mv, NQ * NC * d, cudaMemcpyHostToDevice, s));
+  else G2_CUDA(c, cudaMemsetAsync(G.gmv, 0, NQ * NC * d, s));
+  if (grad_f1) G2_CUDA(c, cudaMemcpyAsync(G.gf1, grad_f1, NQ * NC * d, cudaMemcpyHostToDevice, s));
+  else G2_CUDA(c, cudaMemsetAsync(G.gf1, 0, NQ * NC * d, s));
+  if (nbr) {
+    G2_CUDA(c, cudaMemcpyAsync(G.nbr, nbr, 4 * NC * sizeof(int), cudaMemcpyHostToDevice, s));
+  } else {  // no neighbours yet (a Cell's lists start empty)
+    nb0.assign(4 * NC, 0);
+    for (size_t k = 0; k < NC; ++k) nb0[k] = nb0[2 * NC + k] = -1;
+    G2_CUDA(c, cudaMemcpyAsync(G.nbr, nb0.data(), 4 * NC * sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  neg.assign(NC, -1.);  // Cell::Cell: Sd = -1, pspec = 0, isShocked = false
+  G2_CUDA(c, cudaMemcpyAsync(G.sd, neg.data(), NC * d, cudaMemcpyHostToDevice, s));
+  G2_CUDA(c, cudaMemsetAsync(G.pspec, 0, NC * d, s));
+  G2_CUDA(c, cudaMemsetAsync(G.shocked, 0, NC, s));
+  G2_CUDA(c, cudaMemcpyAsync(G.t, &t, d, cudaMemcpyHostToDevice, s));
+  G2_CUDA(c, cudaMemcpyAsync(G.it, &it, sizeof(long long), cudaMemcpyHostToDevice, s));
+  G2_CUDA(c, cudaMemsetAsync(G.dt, 0, d, s));
+  G2_CUDA(c, cudaMemsetAsync(G.status, 0, sizeof(int), s));
+  if (run_ghosts) {  // the updateGhosts before Simu::run's loop (simu.cpp:74)
+    k_ghosts<<<c->NJ, kThreads, 0, s>>>(G, 0);
+    G2_CUDA(c, cudaGetLastError());
+  }
+  G2_CUDA(c, cudaStreamSynchronize(s));  // host staging vectors go out of scope
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_2d_step(gamma_2d_t *ctx, int nsteps, gamma_step_stats_t *stats) {
+  if (!ctx || nsteps < 0) return GAMMA_ERR_INVALID;
+  gamma_2d *c = ctx;
+  G2_CUDA(c, cudaMemsetAsync(c->d_stats, 0, sizeof(Stats2), c->stream));
+  if (!c->exec && nsteps > 0) {
+    G2_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_step(c);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc != GAMMA_OK) return rc;
+    if (e != cudaSuccess) return fail(c, e, "cudaStreamEndCapture");
+    c->graph = g;
+    G2_CUDA(c, cudaGraphInstantiate(&c->exec, c->graph, 0));
+  }
+  G2_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  for (int k = 0; k < nsteps; ++k) G2_CUDA(c, cudaGraphLaunch(c->exec, c->stream));
+  G2_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  if (stats) {
+    Stats2 h;
+    int status = 0;
+    G2_CUDA(c, cudaMemcpyAsync(&h, c->d_stats, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    G2_CUDA(c, cudaMemcpyAsync(&status, c->G.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    G2_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    G2_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    stats->c2p_calls = h.c2p_calls;
+    stats->c2p_iters = h.c2p_iters;
+    stats->c2p_fallbacks = h.c2p_fallbacks;
+    stats->zone_updates = h.zone_updates;
+    stats->splits = h.splits;
+    stats->merges = h.merges;
+    stats->c2p_max_iters = (int)h.c2p_max_iters;
+    stats->status = status == 30 ? GAMMA_ERR_NEG_DT : (status ? GAMMA_ERR_INVALID : GAMMA_OK);
+    stats->device_ms = ms;
+  }
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_2d_download(gamma_2d_t *ctx, int *ntrack, double *t, double *dt, long long *it, int *status,
+                                double *prim, double *x, double *dx, double *dt_loc, double *xI, double *grad_mv,
+                                double *grad_f1, int *nbr, double *sd, double *pspec, unsigned char *shocked) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  gamma_2d *c = ctx;
+  const Grid2 &G = c->G;
+  const size_t NC = (size_t)c->NC, d = sizeof(double);
+  cudaStream_t s = c->stream;
+  int st = 0;
+  if (ntrack) G2_CUDA(c, cudaMemcpyAsync(ntrack, G.ntrack, c->NJ * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (t) G2_CUDA(c, cudaMemcpyAsync(t, G.t, d, cudaMemcpyDeviceToHost, s));
+  if (dt) G2_CUDA(c, cudaMemcpyAsync(dt, G.dt, d, cudaMemcpyDeviceToHost, s));
+  if (it) G2_CUDA(c, cudaMemcpyAsync(it, G.it, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  G2_CUDA(c, cudaMemcpyAsync(&st, G.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (prim) G2_CUDA(c, cudaMemcpyAsync(prim, G.prim, NQ * NC * d, cudaMemcpyDeviceToHost, s));
+  if (x) G2_CUDA(c, cudaMemcpyAsync(x, G.x, NC * d, cudaMemcpyDeviceToHost, s));
+  if (dx) G2_CUDA(c, cudaMemcpyAsync(dx, G.dx, NC * d, cudaMemcpyDeviceToHost, s));
+  if (dt_loc) G2_CUDA(c, cudaMemcpyAsync(dt_loc, G.dtl, NC * d, cudaMemcpyDeviceToHost, s));
+  if (xI) G2_CUDA(c, cudaMemcpyAsync(xI, G.xI, NC * d, cudaMemcpyDeviceToHost, s));
+  if (grad_mv) G2_CUDA(c, cudaMemcpyAsync(grad_mv, G.gmv, NQ * NC * d, cudaMemcpyDeviceToHost, s));
+  if (grad_f1) G2_CUDA(c, cudaMemcpyAsync(grad_f1, G.gf1, NQ * NC * d, cudaMemcpyDeviceToHost, s));
+  if (nbr) G2_CUDA(c, cudaMemcpyAsync(nbr, G.nbr, 4 * NC * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (sd) G2_CUDA(c, cudaMemcpyAsync(sd, G.sd, NC * d, cudaMemcpyDeviceToHost, s));
+  if (pspec) G2_CUDA(c, cudaMemcpyAsync(pspec, G.pspec, NC * d, cudaMemcpyDeviceToHost, s));
+  if (shocked) G2_CUDA(c, cudaMemcpyAsync(shocked, G.shocked, NC, cudaMemcpyDeviceToHost, s));
+  G2_CUDA(c, cudaStreamSynchronize(s));
+  if (status) *status = st == 30 ? GAMMA_ERR_NEG_DT : (st ? GAMMA_ERR_INVALID : GAMMA_OK);
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_2d_prepare(gamma_2d_t *ctx) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  const int rc = enqueue_prepare(ctx);
+  if (rc != GAMMA_OK) return rc;
+  G2_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_2d_download_fluxes(gamma_2d_t *ctx, double *v, double *lL, double *lR, double *flux,
+                                       double *f1lo, double *f1hi, double *grad_f1_stage) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  gamma_2d *c = ctx;
+  const Grid2 &G = c->G;
+  const size_t NC = (size_t)c->NC, d = sizeof(double);
+  cudaStream_t s = c->stream;
+  if (v) G2_CUDA(c, cudaMemcpyAsync(v, G.v, NC * d, cudaMemcpyDeviceToHost, s));
+  if (lL) G2_CUDA(c, cudaMemcpyAsync(lL, G.lL, NC * d, cudaMemcpyDeviceToHost, s));
+  if (lR) G2_CUDA(c, cudaMemcpyAsync(lR, G.lR, NC * d, cudaMemcpyDeviceToHost, s));
+  if (flux) G2_CUDA(c, cudaMemcpyAsync(flux, G.flx, NQ * NC * d, cudaMemcpyDeviceToHost, s));
+  if (f1lo) G2_CUDA(c, cudaMemcpyAsync(f1lo, G.f1lo, NQ * NC * d, cudaMemcpyDeviceToHost, s));
+  if (f1hi) G2_CUDA(c, cudaMemcpyAsync(f1hi, G.f1hi, NQ * NC * d, cudaMemcpyDeviceToHost, s));
+  if (grad_f1_stage) G2_CUDA(c, cudaMemcpyAsync(grad_f1_stage, G.gf1n, NQ * NC * d, cudaMemcpyDeviceToHost, s));
+  G2_CUDA(c, cudaStreamSynchronize(s));
+  return GAMMA_OK;
+}
+
+GAMMA_API void *gamma_2d_stream(gamma_2d_t *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+GAMMA_API const char *gamma_2d_last_error(const gamma_2d_t *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+GAMMA_API void gamma_2d_destroy(gamma_2d_t *ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->exec) cudaGraphExecDestroy(ctx->exec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  for (void *p : ctx->allocs) cudaFree(p);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+}  // extern "C"

@@ -294,23 +294,15 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
   return f;
 }
 
-// FluidState::cons2prim (rel_sph.cpp:213-320; rel_cart.cpp:125-229).
-// On entry prim holds the previous primitives (pressure warm start); on exit
-// prim holds the recovered primitives and cons is rewritten by prim2cons.
+// Pressure root of the cons2prim driver (rel_sph.cpp:243-286): the bracket,
+// its no-solution tests and the warm start pCand are the reference's; the
+// Brent search is replaced by safeguarded Newton-Raphson.  Returns the
+// pressure the reference would go on with (pCand itself where it finds none).
 template <class Cfg>
-GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
-  const double D = cons[DEN];
-  const double tau = cons[TAU];
-  const double E = D + tau;
-  const double ss = cons[SS1];
-  double S2 = 0.;
-  S2 += ss * ss;
-  const double S = Cfg::FAST ? fabs(ss) : sqrt(S2);
+GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double E, double pCand, C2PStats *st) {
   auto fval = [&](double p, double *df, double *l2) -> double {
     return Cfg::FAST ? c2p_f<Cfg>(ph, p, D, S2, E, df, l2) : c2p_f_ref<Cfg>(ph, p, D, S, E, df, l2);
   };
-
-  double pCand = Cfg::SPH ? fmax(1.e-13, prim[PPP]) : prim[PPP];
   int iters = 0, fallback = 0;
   const double f_init = fval(pCand, nullptr, nullptr);
   if (fabs(f_init) > 0.) {
@@ -368,6 +360,22 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
     st->iters = iters;
     st->fallback = fallback;
   }
+  return pCand;
+}
+
+// FluidState::cons2prim (rel_sph.cpp:213-320; rel_cart.cpp:125-229).
+// On entry prim holds the previous primitives (pressure warm start); on exit
+// prim holds the recovered primitives and cons is rewritten by prim2cons.
+template <class Cfg>
+GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
+  const double D = cons[DEN];
+  const double tau = cons[TAU];
+  const double E = D + tau;
+  const double ss = cons[SS1];
+  double S2 = 0.;
+  S2 += ss * ss;
+  const double S = Cfg::FAST ? fabs(ss) : sqrt(S2);
+  const double pCand = c2p_pressure<Cfg>(ph, D, S, S2, E, Cfg::SPH ? fmax(1.e-13, prim[PPP]) : prim[PPP], st);
 
   double p = pCand;
   double rho, uu;
@@ -453,7 +461,9 @@ GB_HD Waves compute_lambda_ref(const Phys &ph, const FState<Cfg> &L, const FStat
   if (linear) {
     w.lS = mhll / (Ehll + Fhllm);
   } else {
-    double delta = pow(Ehll + Fhllm, 2.) - 4. * FhllE * mhll;
+    // pow(x, 2.) of the C library is the correctly rounded square: x*x
+    const double ef = Ehll + Fhllm;
+    double delta = ef * ef - 4. * FhllE * mhll;
     w.lS = ((Ehll + Fhllm) - sqrt(delta)) / (2. * FhllE);
   }
   return w;

@@ -1,0 +1,895 @@
+// The 2D (r, theta) moving-mesh step of GAMMA as per-element functions.
+//
+// A run is a set of NJ theta tracks (ngst ghost tracks on each side), each a
+// 1D moving mesh in r of at most `cap` cells (ghosts included).  Cell (j, i)
+// lives at flat index g = j * cap + i, which is also the reference's cell id
+// (Cell::nde_id, src/Dimensions/2d.cpp:100-106), so the neighbour lists can be
+// stored as (first id, count).  Interface (j, i) is the right edge of cell
+// (j, i).  Per step (src/simu.cpp:79-105, src/Timestep/rk3.cpp:98-194):
+//
+//   regrid (per track) -> [reset shocks] -> per stage:
+//     ghosts            updateGhosts (2d.cpp:241-321)
+//     mv_interface      reconstructStates(MV) + computeLambda + kinematics +
+//                       computeFlux + measureShock (2d.cpp:436-470, 735-767)
+//     cell_mv           update_dt(MV) and computeNeighbors (2d.cpp:534-606, 769-777)
+//     trans_grad        computeTransGradients (2d.cpp:366-430)
+//     f1_own/f1_gather  the theta-direction fluxes between tracks (2d.cpp:779-839)
+//     [stage 1: dt = CFL min dt_loc, detectShock]
+//     iface_move, update_cell   Grid::update + the RK3 combines (2d.cpp:861-882,
+//                       rk3.cpp:98-194)
+//   -> inject particles.
+//
+// Fields the reference keeps in its Cell records across stages and steps are
+// kept here too, because they feed later results: the moving-direction and
+// transverse gradients (grad_mv, grad_f1) and the neighbour lists.  In the
+// reference the ghost cells 0 and ntrack-1 of each track are copies of an edge
+// cell made before the neighbour lists are rebuilt, so they use the lists and
+// gradients of an earlier stage (and, in ghost tracks, lists that point into
+// other tracks); the transverse gradient of the upper cell of a theta
+// interface is the one from the previous stage (track j+1 is processed after
+// track j).  Each of these is reproduced.
+#pragma once
+
+#include "physics2d.cuh"
+
+namespace gb {
+namespace d2 {
+
+constexpr int KMAX_STALE = 8;  // foreign stale contributors per target track
+
+// Problem hooks of the theta-wedge blast wave (src/Initial/Tests/BM.cpp)
+struct Params2 {
+  double split_DR, merge_DR;            // checkCellForRegrid ratios for lfac >= 2
+  double split_DR_slow, merge_DR_slow;  // ... and for lfac < 2
+  double v_out;                         // outer ghost-interface velocity
+  double it_hold;                       // v_out -> 0 once it > it_hold and the flow has stopped
+  double Nalpha, Nmp, Nme;              // synchrotron constants (normalised)
+};
+
+struct Grid2 {
+  int NJ, cap, ngst;
+  long long NC;  // NJ * cap: row stride of [q][g] arrays
+  int *ntrack;   // [NJ]
+  const double *tg;  // [NJ][TG_WORDS] angular factors of each track (TrackGeo)
+  // cells
+  double *prim;       // [NQ][NC]
+  double *x, *dx;     // r and dr (Cell::G)
+  double *dtl, *sd, *pspec;
+  uint8_t *shocked;
+  double *gmv, *gf1, *gf1n;  // [NQ][NC] grad_mv, grad_f1 (persistent), grad_f1 of this stage
+  int *nbr;                  // [4][NC]: first id and count towards track j-1, then j+1
+  double *cons0, *dV0;       // [NQ][NC], [NC]: S0.cons and G0.dV (copyState0)
+  double *f1lo, *f1hi;       // [NQ][NC]: flux[0][F1], flux[1][F1]
+  // interfaces
+  double *xI, *xI0, *xIm;    // position, step-start position, position after the stage's move
+  double *v, *lL, *lR;
+  double *flx;               // [NQ][NC] MV flux (times dA)
+  // foreign stale contributors: stale_n[t], stale_id[t * KMAX_STALE + k]
+  int *stale_n, *stale_id;
+  // run scalars
+  double *t, *dt;
+  long long *it;
+  int *status;               // 30: negative CFL candidate; 40: stale table overflow
+  double *red;               // partial minima of dt_loc
+  // regrid scratch (one track of records per track)
+  double *rprim, *rgmv, *rgf1;  // [NQ][NC]
+  double *rx, *rdx, *rdtl, *rxI;
+  int *rnbr;                 // [4][NC]
+  unsigned long long *stats;  // c2p calls, c2p iters, fallbacks, zone updates, splits, merges, max iters
+};
+
+GB_HD int iL_of(const Grid2 &G) { return G.ngst - 1; }
+GB_HD int jL_of(const Grid2 &G) { return G.ngst - 1; }
+GB_HD int jR_of(const Grid2 &G) { return G.NJ - G.ngst; }
+
+GB_HD double cen_r(double r, double dr) {
+  double r2 = r * r;
+  double dr2 = dr * dr;
+  return 3. * r * (r2 + dr2) / (3 * r2 + dr2);
+}
+
+GB_HD TrackGeo tgeo(const Grid2 &G, int j) { return track_geo(G.tg + (long long)j * TG_WORDS); }
+
+GB_HD Geom cell_geom(const Grid2 &G, int j, long long g) { return make_geom(G.x[g], G.dx[g], tgeo(G, j)); }
+
+GB_HD void load_prim(const Grid2 &G, long long g, double *p) {
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) p[q] = G.prim[q * G.NC + g];
+}
+
+// ---------------------------------------------------------------------------
+// Ghost tracks and ghost cells (Grid::updateGhosts, 2d.cpp:241-321).  One
+// track per call, threads tid of nth.  `reset`: the step's first call, right
+// after Cell::resetShock of every cell.  The source cells of a ghost track are
+// never written in the same pass (only active cells are copied).
+
+GB_HD void copy_cell(const Grid2 &G, long long d, long long s, bool reset) {
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    G.prim[q * G.NC + d] = G.prim[q * G.NC + s];
+    G.gmv[q * G.NC + d] = G.gmv[q * G.NC + s];
+    G.gf1[q * G.NC + d] = G.gf1[q * G.NC + s];
+  }
+  G.x[d] = G.x[s];
+  G.dx[d] = G.dx[s];
+  G.dtl[d] = G.dtl[s];
+  if (reset) {
+    G.sd[d] = -1.;
+    G.pspec[d] = 0.;
+    G.shocked[d] = 0;
+  } else {
+    G.sd[d] = G.sd[s];
+    G.pspec[d] = G.pspec[s];
+    G.shocked[d] = G.shocked[s];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) G.nbr[k * G.NC + d] = G.nbr[k * G.NC + s];
+}
+
+// phase 0 (reset only): Cell::resetShock on the track's cells
+GB_HD void ghosts_reset(const Grid2 &G, int j, int tid, int nth) {
+  const long long o = (long long)j * G.cap;
+  for (int i = tid; i < G.cap; i += nth) {
+    G.sd[o + i] = -1.;
+    G.pspec[o + i] = 0.;
+    G.shocked[o + i] = 0;
+  }
+}
+
+// phase 1: a ghost track takes the active cells and interfaces of the edge track
+GB_HD void ghosts_tracks(const Grid2 &G, int j, int tid, int nth, bool reset) {
+  const int jL = jL_of(G), jR = jR_of(G);
+  if (j > jL && j < jR) return;
+  const int src = j <= jL ? jL + 1 : jR - 1;
+  const int n = G.ntrack[src];
+  const int iL = iL_of(G), iR = n - G.ngst;
+  if (tid == 0) G.ntrack[j] = n;
+  const long long o = (long long)j * G.cap, os = (long long)src * G.cap;
+  for (int i = iL + 1 + tid; i <= iR - 1; i += nth) copy_cell(G, o + i, os + i, reset);
+  for (int i = iL + tid; i <= iR - 1; i += nth) G.xI[o + i] = G.xI[os + i];
+}
+
+// phase 2: ghost cells and ghost interfaces of the track (after phase 1)
+GB_HD void ghosts_cells(const Grid2 &G, int j, int tid, int nth) {
+  const int n = G.ntrack[j];
+  const int iL = iL_of(G), iR = n - G.ngst;
+  const long long o = (long long)j * G.cap;
+  const long long eL = o + iL + 1, eR = o + iR - 1;
+  for (int i = tid; i <= iL; i += nth) {
+    copy_cell(G, o + i, eL, false);
+    G.x[o + i] = G.x[eL] - (iL - i + 1) * G.dx[eL];
+  }
+  for (int i = iR + tid; i < n; i += nth) {
+    copy_cell(G, o + i, eR, false);
+    G.x[o + i] = G.x[eR] + (i - iR + 1) * G.dx[eR];
+  }
+  for (int i = tid; i <= iL - 1; i += nth) G.xI[o + i] = G.xI[o + iL + 1] - (iL - i + 1) * G.dx[eL];
+  for (int i = iR + tid; i <= n - 2; i += nth) G.xI[o + i] = G.xI[o + iR - 1] + (i - iR) * G.dx[eR];
+}
+
+// ---------------------------------------------------------------------------
+// Moving-direction interfaces (one per call): reconstructStates(MV),
+// computeLambda, updateKinematics + userKinematics, computeFlux, measureShock.
+
+// userKinematics of BM.cpp:198-218: the outer ghost interfaces move at v_out
+// until, after it_hold steps, the flow ten cells inside the outer edge of the
+// first active track has stopped.
+GB_HD double outer_velocity(const Grid2 &G, const Params2 &P, long long it) {
+  const int jt = jL_of(G) + 1;
+  const int iR = G.ntrack[jt] - G.ngst;
+  const long long g = (long long)jt * G.cap + iR - 10;
+  if (G.prim[UU1 * G.NC + g] < 1.e-3 && (double)it > P.it_hold) return 0.;
+  return P.v_out;
+}
+
+// cell state as prepForUpdate leaves it: prim2cons and state2flux at the cell's r
+GB_HD void cell_state(const Phys &ph, const Grid2 &G, long long g, int dim, St &S) {
+  load_prim(G, g, S.prim);
+  fill(ph, S, dim, G.x[g]);
+}
+
+GB_HD void mv_interface(const Phys &ph, const Params2 &P, const Grid2 &G, int j, int i, long long it) {
+  const int n = G.ntrack[j];
+  if (i > n - 2) return;
+  const long long o = (long long)j * G.cap, g = o + i;
+  const double xI = G.xI[g];
+  St L, R;
+  if (i == 0 || i == n - 2) {
+    cell_state(ph, G, g, MV, L);
+    cell_state(ph, G, g + 1, MV, R);
+  } else {
+    const double cLL = cen_r(G.x[g - 1], G.dx[g - 1]), cL = cen_r(G.x[g], G.dx[g]);
+    const double cR = cen_r(G.x[g + 1], G.dx[g + 1]), cRR = cen_r(G.x[g + 2], G.dx[g + 2]);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const double qLL = G.prim[q * G.NC + g - 1], qL = G.prim[q * G.NC + g];
+      const double qR = G.prim[q * G.NC + g + 1], qRR = G.prim[q * G.NC + g + 2];
+      double gL = (qL - qLL) / (cL - cLL);
+      const double gN = (qR - qL) / (cR - cL);
+      double gR = (qRR - qR) / (cRR - cR);
+      gL = minmod(gL, gN);
+      gR = minmod(gR, gN);
+      // grad_mv stored in the cells; cell i from its right interface, except
+      // the last reconstructed cell n-2, which only has its left one
+      G.gmv[q * G.NC + g] = gL;
+      if (i == n - 3) G.gmv[q * G.NC + g + 1] = gR;
+      L.prim[q] = qL + gL * (xI - cL);
+      R.prim[q] = qR + gR * (xI - cR);
+    }
+    fill(ph, L, MV, xI);
+    fill(ph, R, MV, xI);
+  }
+  const Waves w = compute_lambda(ph, L, R, MV, xI);
+  double v = ph.vi * w.lS;
+  if (i >= n - 1 - G.ngst) v = outer_velocity(G, P, it);
+  G.lL[g] = w.lL;
+  G.lR[g] = w.lR;
+  G.v[g] = v;
+  double fl[NQ];
+  hllc_flux(L, R, w, v, dA_r(xI, tgeo(G, j)), MV, xI, fl);
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) G.flx[q * G.NC + g] = fl[q];
+  // measureShock, moving direction: forward shocks only, into the left cell
+  double Sd;
+  if (compute_Sd(ph, L, R, MV, false, &Sd)) {
+    if (P_SPEC > G.pspec[g]) G.pspec[g] = P_SPEC;
+  }
+  G.sd[g] = fmax(G.sd[g], Sd);
+}
+
+// ---------------------------------------------------------------------------
+// Per cell after the interfaces: update_dt(MV) (cell.cpp:47-74) and the
+// neighbour lists (computeNeighbors, 2d.cpp:534-606) of cells 1..ntrack-2.
+//
+// The reference scans the interfaces of track j-/+1 with a cursor carried from
+// cell to cell.  With those interfaces sorted, the cursor at the start of cell
+// i is min(LB(x_{i-1} + dx_{i-1}/2), n'-2) (LB: first interface >= the value),
+// which gives every list without the scan.
+
+GB_HD int lower_bound(const double *X, int n, double v) {  // first k in [0, n) with X[k] >= v, or n
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (X[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+GB_HD void neighbour_list(const Grid2 &G, int j, int i, int jn, int *first, int *count) {
+  const long long o = (long long)j * G.cap, g = o + i;
+  const int np = G.ntrack[jn];
+  const double *X = G.xI + (long long)jn * G.cap;  // np-1 interfaces
+  const double xjL = G.x[g] - G.dx[g] / 2.;
+  const double xjR = G.x[g] + G.dx[g] / 2.;
+  int s = 0;
+  if (i > 1) {
+    const double xpR = G.x[g - 1] + G.dx[g - 1] / 2.;
+    s = lower_bound(X, np - 1, xpR);
+    if (s > np - 2) s = np - 2;
+  }
+  const int b = (X[s] > xjL && s > 0) ? s - 1 : s;
+  if (X[b] < xjR) {
+    int e = lower_bound(X, np - 1, xjR) - 1;
+    if (e > np - 2) e = np - 2;
+    *first = jn * G.cap + b + 1;
+    *count = e - b + 1;
+  } else {
+    *first = jn * G.cap + b + 1;  // empty: kept ordered for the gather's search
+    *count = 0;
+  }
+}
+
+GB_HD void cell_mv(const Grid2 &G, int j, int i) {
+  const int n = G.ntrack[j];
+  if (i < 1 || i > n - 2) return;
+  const long long g = (long long)j * G.cap + i;
+  // Cell::update_dt, moving direction
+  const double a = G.dx[g];
+  double dL = (G.lR[g - 1] > G.v[g]) ? a / (G.lR[g - 1] - G.v[g]) : DT_INF;
+  double dR = (G.lL[g] < G.v[g - 1]) ? a / (G.v[g - 1] - G.lL[g]) : DT_INF;
+  const double cand = fmin(dL, dR);
+  if (cand < 0) *G.status = 30;
+  else G.dtl[g] = fmin(G.dtl[g], cand);
+  // neighbour lists
+  int f0 = -1, c0 = 0, f1 = -1, c1 = 0;
+  if (j != 0) neighbour_list(G, j, i, j - 1, &f0, &c0);
+  if (j != G.NJ - 1) neighbour_list(G, j, i, j + 1, &f1, &c1);
+  G.nbr[0 * G.NC + g] = f0;
+  G.nbr[1 * G.NC + g] = c0;
+  G.nbr[2 * G.NC + g] = f1;
+  G.nbr[3 * G.NC + g] = c1;
+}
+
+// ---------------------------------------------------------------------------
+// Transverse gradient of cell (j, i), j <= NJ-2 (computeTransGradients).
+// The theta position of the interface with an upper neighbour stays at the
+// cell centre there (the reference's `else if (d==0)` never moves it).
+
+GB_HD void overlap(const Grid2 &G, long long g0, long long gn, double *xm, double *w) {
+  const double xL0 = G.x[g0] - G.dx[g0] / 2., xR0 = G.x[g0] + G.dx[g0] / 2.;
+  const double xLn = G.x[gn] - G.dx[gn] / 2., xRn = G.x[gn] + G.dx[gn] / 2.;
+  *xm = (fmax(xL0, xLn) + fmin(xR0, xRn)) / 2.;
+  *w = fmax(0., fmin(xR0, xRn) - fmax(xL0, xLn));
+}
+
+GB_HD void trans_grad(const Grid2 &G, int j, int i) {
+  const int n = G.ntrack[j];
+  if (i >= n) return;
+  const long long g0 = (long long)j * G.cap + i;
+  if (j == G.NJ - 1) {  // never recomputed: keeps its copied value
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) G.gf1n[q * G.NC + g0] = G.gf1[q * G.NC + g0];
+    return;
+  }
+  const double cr0 = cen_r(G.x[g0], G.dx[g0]);
+  const TrackGeo t0 = tgeo(G, j);
+  const double ct0 = t0.cen_t;
+  double avg[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) avg[q] = 0.;
+  double dAtot = 0.;
+  // pass 1: dA-weighted average; pass 2: minmod with each neighbour's gradient
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int d = 0; d < 2; ++d) {
+      const int first = G.nbr[(2 * d) * G.NC + g0], cnt = G.nbr[(2 * d + 1) * G.NC + g0];
+      for (int k = 0; k < cnt; ++k) {
+        const long long gn = first + k;
+        const int jn = (int)(gn / G.cap);
+        double xm, w;
+        overlap(G, g0, gn, &xm, &w);
+        // theta of the interface: th - dth/2 below, th (unmoved) above
+        const double dA = dA_t(xm, w, d == 0 ? t0.s_lo : t0.s_mid);
+        if (pass == 0) dAtot += dA;
+        const double dxmL = xm - cr0;
+        const double dxmR = xm - cen_r(G.x[gn], G.dx[gn]);
+        const double dcen = tgeo(G, jn).cen_t - ct0;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          const double qL = G.prim[q * G.NC + g0] + G.gmv[q * G.NC + g0] * dxmL;
+          const double qR = G.prim[q * G.NC + gn] + G.gmv[q * G.NC + gn] * dxmR;
+          const double grad = (qR - qL) / dcen;
+          if (pass == 0) avg[q] += grad * dA;
+          else avg[q] = minmod(avg[q], grad);
+        }
+      }
+    }
+    if (pass == 0) {
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) avg[q] /= dAtot;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) G.gf1n[q * G.NC + g0] = avg[q];
+}
+
+// ---------------------------------------------------------------------------
+// Theta-direction interface between c0 = (j, i) and its upper neighbour gn
+// (the body of the F1 loop of Grid::computeFluxes, 2d.cpp:800-837).
+
+struct F1Result {
+  double flux[NQ];
+  double sd_fwd, sd_rev;
+  bool have_fwd, have_rev;
+};
+
+GB_HD void f1_interface(const Phys &ph, const Grid2 &G, int j, long long g0, long long gn, F1Result &out) {
+  const int jn = (int)(gn / G.cap);
+  const TrackGeo t0 = tgeo(G, j);
+  const double jpos = t0.th + t0.dth / 2.;
+  double xm, w;
+  overlap(G, g0, gn, &xm, &w);
+  const double dA = dA_t(xm, w, t0.s_hi);
+  St L, R;
+  const bool pc = j == 0 || j == G.NJ - 2 || G.nbr[1 * G.NC + g0] == 0 || G.nbr[3 * G.NC + gn] == 0;
+  if (pc) {
+    cell_state(ph, G, g0, F1, L);
+    cell_state(ph, G, gn, F1, R);
+  } else {
+    // the upper cell's transverse gradient: this stage's if the reference's
+    // track-by-track loop has reached it already, else the previous stage's
+    const double *gR = (jn < j || (jn == j && gn < g0)) ? G.gf1n : G.gf1;
+    const double dxmL = xm - cen_r(G.x[g0], G.dx[g0]);
+    const double dxmR = xm - cen_r(G.x[gn], G.dx[gn]);
+    const double dxfL = jpos - t0.cen_t;
+    const double dxfR = jpos - tgeo(G, jn).cen_t;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const double qL = G.prim[q * G.NC + g0] + G.gmv[q * G.NC + g0] * dxmL;
+      const double qR = G.prim[q * G.NC + gn] + G.gmv[q * G.NC + gn] * dxmR;
+      L.prim[q] = qL + G.gf1n[q * G.NC + g0] * dxfL;  // this stage's (computed first)
+      R.prim[q] = qR + gR[q * G.NC + gn] * dxfR;
+    }
+    fill(ph, L, F1, xm);
+    fill(ph, R, F1, xm);
+  }
+  const Waves wv = compute_lambda(ph, L, R, F1, xm);
+  hllc_flux(L, R, wv, 0., dA, F1, xm, out.flux);
+  out.have_fwd = compute_Sd(ph, L, R, F1, false, &out.sd_fwd);
+  out.have_rev = compute_Sd(ph, R, L, F1, true, &out.sd_rev);
+}
+
+// c0's side: flux[1][F1] and forward shocks, over c0's upper neighbours in order
+GB_HD void f1_own(const Phys &ph, const Grid2 &G, int j, int i) {
+  if (j > G.NJ - 2 || i >= G.ntrack[j]) return;
+  const long long g0 = (long long)j * G.cap + i;
+  const int first = G.nbr[2 * G.NC + g0], cnt = G.nbr[3 * G.NC + g0];
+  double acc[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) acc[q] = 0.;
+  double sd = G.sd[g0], ps = G.pspec[g0];
+  for (int k = 0; k < cnt; ++k) {
+    F1Result r;
+    f1_interface(ph, G, j, g0, first + k, r);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) acc[q] += r.flux[q];
+    sd = fmax(sd, r.sd_fwd);
+    if (r.have_fwd && P_SPEC > ps) ps = P_SPEC;
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) G.f1hi[q * G.NC + g0] = acc[q];
+  G.sd[g0] = sd;
+  G.pspec[g0] = ps;
+}
+
+// Foreign stale contributors: cells 0 and ntrack-1 whose (copied) upper list
+// points into a track other than j+1.  One thread builds the table in
+// (j, i) order.
+GB_HD void stale_table(const Grid2 &G) {
+  for (int t = 0; t < G.NJ; ++t) G.stale_n[t] = 0;
+  for (int j = 0; j <= G.NJ - 2; ++j) {
+    const int n = G.ntrack[j];
+    const int cells[2] = {0, n - 1};
+    for (int c = 0; c < 2; ++c) {
+      const long long g = (long long)j * G.cap + cells[c];
+      const int first = G.nbr[2 * G.NC + g], cnt = G.nbr[3 * G.NC + g];
+      if (cnt <= 0) continue;
+      const int t = first / G.cap;
+      if (t == j + 1 || t < 0 || t >= G.NJ) continue;
+      const int k = G.stale_n[t];
+      if (k >= KMAX_STALE) {
+        *G.status = 40;
+        continue;
+      }
+      G.stale_id[t * KMAX_STALE + k] = (int)g;
+      G.stale_n[t] = k + 1;
+    }
+  }
+}
+
+// cn's side: flux[0][F1] and reverse shocks, summed over the cells whose upper
+// list holds cn, in the reference's (j, i) order.
+GB_HD void f1_gather(const Phys &ph, const Grid2 &G, int t, int k) {
+  if (k >= G.ntrack[t]) return;
+  const long long gn = (long long)t * G.cap + k;
+  double acc[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) acc[q] = 0.;
+  double sd = G.sd[gn], ps = G.pspec[gn];
+  auto add = [&](int j, long long g0) {
+    const int first = G.nbr[2 * G.NC + g0], cnt = G.nbr[3 * G.NC + g0];
+    if (!(cnt > 0 && gn >= first && gn < (long long)first + cnt)) return;
+    F1Result r;
+    f1_interface(ph, G, j, g0, gn, r);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) acc[q] += r.flux[q];
+    sd = fmax(sd, r.sd_rev);
+    // the reference's spectral-index local keeps the forward value when the
+    // reverse test returns early
+    if ((r.have_rev || r.have_fwd) && P_SPEC > ps) ps = P_SPEC;
+  };
+  const int ns = G.stale_n[t];
+  // foreign stale contributors from tracks below t-1
+  for (int s = 0; s < ns; ++s) {
+    const long long g0 = G.stale_id[t * KMAX_STALE + s];
+    const int j = (int)(g0 / G.cap);
+    if (j < t - 1) add(j, g0);
+  }
+  if (t >= 1) {
+    const int j = t - 1;
+    const int n = G.ntrack[j];
+    const long long o = (long long)j * G.cap;
+    add(j, o);  // cell 0 (its list may be stale)
+    // fresh lists of cells 1..n-2: starts are non-decreasing, so the cells
+    // holding gn end at the last start <= gn and form a run downwards
+    int lo = 1, hi = n - 2;  // last i in [1, n-2] with first_i <= gn
+    int last = 0;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      if (G.nbr[2 * G.NC + o + mid] <= gn) {
+        last = mid;
+        lo = mid + 1;
+      } else {
+        hi = mid - 1;
+      }
+    }
+    // (list ends are non-decreasing too; empty lists only occur at the start)
+    int begin = last;
+    while (begin >= 1) {
+      const long long g0 = o + begin;
+      const int first = G.nbr[2 * G.NC + g0], cnt = G.nbr[3 * G.NC + g0];
+      if (cnt > 0 && (long long)first + cnt > gn) --begin;
+      else break;
+    }
+    for (int i = begin + 1; i <= last; ++i) add(j, o + i);
+    if (n - 1 > 0) add(j, o + n - 1);  // cell ntrack-1 (stale)
+  }
+  // foreign stale contributors from track t and above
+  for (int s = 0; s < ns; ++s) {
+    const long long g0 = G.stale_id[t * KMAX_STALE + s];
+    const int j = (int)(g0 / G.cap);
+    if (j >= t) add(j, g0);
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) G.f1lo[q * G.NC + gn] = acc[q];
+  G.sd[gn] = sd;
+  G.pspec[gn] = ps;
+}
+
+// ---------------------------------------------------------------------------
+// Stage 1 after the fluxes: detectShock and collect_dt's reset (the minimum is
+// reduced separately).
+
+GB_HD double collect_cell(const Grid2 &G, int j, int i) {
+  if (i >= G.ntrack[j]) return DT_INF;
+  const long long g = (long long)j * G.cap + i;
+  const double d = G.dtl[g];
+  G.dtl[g] = DT_INF;
+  G.shocked[g] = G.sd[g] > DETECT_SHOCK_THRESHOLD ? 1 : 0;
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// Grid::update and the RK3 combines.
+//
+// iface_move: Interface::move of every interface of the active tracks; at
+// stage 1 copyState0 first keeps x0; at stages 2, 3 interfaces iLbnd..iRbnd-1
+// then take the combined position (rk3.cpp:121-131, 159-168).  xIm keeps the
+// moved position for Cell::update.
+GB_HD void iface_move(const Grid2 &G, int j, int i, int stage) {
+  const int n = G.ntrack[j];
+  if (i > n - 2) return;
+  const long long g = (long long)j * G.cap + i;
+  if (stage == 1) G.xI0[g] = G.xI[g];
+  const int jL = jL_of(G), jR = jR_of(G);
+  if (j <= jL || j >= jR) return;
+  const double dt = *G.dt;
+  double x = G.xI[g];
+  x += dt * G.v[g];
+  G.xIm[g] = x;
+  const int iL = iL_of(G), iR = n - G.ngst;
+  if (stage == 2 && i >= iL && i <= iR - 1) x = 3. / 4. * G.xI0[g] + 1. / 4. * x;
+  if (stage == 3 && i >= iL && i <= iR - 1) x = 1. / 3. * G.xI0[g] + 2. / 3. * x;
+  G.xI[g] = x;
+}
+
+// Cell::update (cell.cpp:102-127) of an active cell, the stage's combine and
+// cons2prim; at stage 3 the particle injection of every cell (run after
+// evolve by Simu::run).  Every cell copies this stage's grad_f1 into the
+// persistent one.
+GB_HD void update_cell(const Phys &ph, const Params2 &P, const Grid2 &G, int j, int i, int stage,
+                       unsigned long long *c2p) {
+  const int n = G.ntrack[j];
+  if (i >= n) return;
+  const long long g = (long long)j * G.cap + i;
+  const int jL = jL_of(G), jR = jR_of(G);
+  const int iL = iL_of(G), iR = n - G.ngst;
+  const bool active_track = j > jL && j < jR;
+  double prim[NQ];
+  load_prim(G, g, prim);
+  if (active_track) {
+    const double dt = *G.dt;
+    if (i >= iL + 1 && i <= iR - 1) {
+      const Geom G0 = cell_geom(G, j, g);
+      double cons[NQ];
+      prim2cons(ph, prim, cons, G0.r);
+      if (stage == 1) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) G.cons0[q * G.NC + g] = cons[q];
+        G.dV0[g] = G0.dV;
+      }
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) cons[q] *= G0.dV;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) cons[q] += (G.flx[q * G.NC + g - 1] - G.flx[q * G.NC + g]) * dt;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) cons[q] += (G.f1lo[q * G.NC + g] - G.f1hi[q * G.NC + g]) * dt;
+      const TrackGeo tj = tgeo(G, j);
+      source_terms(ph, prim, G0, tj, dt, cons);
+      {  // Cell::radiativeSourceTerms
+        const SynchConst sc{P.Nalpha, P.Nmp, P.Nme};
+        const double dg = radiative_source<Cfg2>(ph, sc, prim, G0.dV, dt);
+        cons[GMX] += dg;
+        cons[GMN] += dg;
+      }
+      const double xL = G.xIm[g - 1], xR = G.xIm[g];
+      const Geom G1 = make_geom((xR + xL) / 2., (xR - xL), tj);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) cons[q] /= G1.dV;
+      C2PStats cs;
+      cons2prim(ph, cons, prim, G1.cen_r, &cs);
+      c2p[0] += 1;
+      c2p[1] += cs.iters;
+      c2p[2] += cs.fallback;
+      if ((unsigned long long)cs.iters > c2p[3]) c2p[3] = cs.iters;
+      double xn = G1.r, dxn = G1.dr;
+      if (stage > 1) {
+        const double w0 = stage == 2 ? 3. / 4. : 1. / 3.;
+        const double w1 = stage == 2 ? 1. / 4. : 2. / 3.;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) cons[q] = w0 * G.cons0[q * G.NC + g] * G.dV0[g] + w1 * cons[q] * G1.dV;
+        const double cL = G.xI[g - 1], cR = G.xI[g];  // combined positions
+        const Geom G2 = make_geom((cR + cL) / 2., (cR - cL), tj);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) cons[q] /= G2.dV;
+        cons2prim(ph, cons, prim, G2.r, &cs);
+        c2p[0] += 1;
+        c2p[1] += cs.iters;
+        c2p[2] += cs.fallback;
+        if ((unsigned long long)cs.iters > c2p[3]) c2p[3] = cs.iters;
+        xn = G2.r;
+        dxn = G2.dr;
+      }
+      G.x[g] = xn;
+      G.dx[g] = dxn;
+    } else if (stage > 1 && i >= 1 && i <= n - 2) {
+      // CellGeomFromInterfacePos also moves the ghost cells 1 and ntrack-2
+      const double cL = G.xI[g - 1], cR = G.xI[g];
+      G.x[g] = (cR + cL) / 2.;
+      G.dx[g] = (cR - cL);
+    }
+  }
+  if (stage == 3) {
+    const SynchConst sc{P.Nalpha, P.Nmp, P.Nme};
+    inject_particles(ph, sc, prim, G.shocked[g] != 0, G.pspec[g]);
+  }
+  if (active_track || stage == 3) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) G.prim[q * G.NC + g] = prim[q];
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) G.gf1[q * G.NC + g] = G.gf1n[q * G.NC + g];
+}
+
+// ---------------------------------------------------------------------------
+// Regrid of one active track (Grid::regrid body, 2d.cpp:609-832, with the
+// checkCellForRegrid of BM.cpp:246-278), one thread.  The reference walks the
+// active cells with a live right bound and edits the track in place; here the
+// same walk streams the new track into the scratch rows and copies it back.
+// A cell is the reference's whole Cell record: state, geometry, dt_loc, the
+// two gradients and the neighbour lists move with it.
+
+struct Rec {
+  double prim[NQ], gmv[NQ], gf1[NQ];
+  double x, dx, dtl;
+  int nbr[4];
+  double rifx;  // position of the right interface
+};
+
+GB_HD void rec_load(const Grid2 &G, long long g, bool has_rif, Rec &c) {
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    c.prim[q] = G.prim[q * G.NC + g];
+    c.gmv[q] = G.gmv[q * G.NC + g];
+    c.gf1[q] = G.gf1[q * G.NC + g];
+  }
+  c.x = G.x[g];
+  c.dx = G.dx[g];
+  c.dtl = G.dtl[g];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) c.nbr[k] = G.nbr[k * G.NC + g];
+  c.rifx = has_rif ? G.xI[g] : 0.;
+}
+
+GB_HD void rec_store(const Grid2 &G, long long g, const Rec &c) {
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    G.rprim[q * G.NC + g] = c.prim[q];
+    G.rgmv[q * G.NC + g] = c.gmv[q];
+    G.rgf1[q * G.NC + g] = c.gf1[q];
+  }
+  G.rx[g] = c.x;
+  G.rdx[g] = c.dx;
+  G.rdtl[g] = c.dtl;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) G.rnbr[k * G.NC + g] = c.nbr[k];
+  G.rxI[g] = c.rifx;
+}
+
+struct Target {
+  double rmin, rmax;
+  int nact;
+};
+
+GB_HD int regrid_decision(const Params2 &P, const Rec &c, double target_dr) {
+  double dr = c.dx;
+  double split_DR = P.split_DR, merge_DR = P.merge_DR;
+  if (lfac(c.prim) < 2.) {
+    split_DR = P.split_DR_slow;
+    merge_DR = P.merge_DR_slow;
+  }
+  if (dr > split_DR * target_dr) return SPLIT;
+  if (dr < merge_DR * target_dr) return MERGE;
+  return SKIP;
+}
+
+// `live`: the track is the one the criterion measures itself against (its
+// bounds and active count change as it is regridded); otherwise `fixed`.
+GB_HD void regrid_track(const Phys &ph, const Params2 &P, const Grid2 &G, int j, bool live, Target fixed,
+                        unsigned long long *nsplit, unsigned long long *nmerge, unsigned long long *c2p) {
+  const int ng = G.ngst, iL = ng - 1;
+  const int n0 = G.ntrack[j];
+  const long long o = (long long)j * G.cap;
+  const TrackGeo tj = tgeo(G, j);
+  int ntrack = n0, iR = n0 - ng;
+  int out = 0;     // output position of the next emitted cell
+  bool changed = false;
+  Rec prev, cur, nxt;
+  auto emit = [&](const Rec &c) {
+    rec_store(G, o + out, c);
+    ++out;
+  };
+  for (int k = 0; k < iL; ++k) {
+    Rec c;
+    rec_load(G, o + k, true, c);
+    emit(c);
+  }
+  rec_load(G, o + iL, true, prev);
+  rec_load(G, o + iL + 1, iL + 1 <= n0 - 2, cur);
+  int k = iL + 2;  // next original cell (position i+1)
+  int i = iL + 1;
+  // current x at position pos (for the live bounds)
+  auto x_at = [&](int pos) -> double {
+    if (pos < out) return G.rx[o + pos];
+    if (pos == i - 1) return prev.x;
+    if (pos == i) return cur.x;
+    return G.x[o + k + (pos - i - 1)];
+  };
+  while (i <= iR - 1) {
+    Target T = fixed;
+    if (live) {
+      T.rmin = x_at(iL + 1);
+      T.rmax = x_at(iR - 1);
+      T.nact = ntrack - 2 * ng;
+    }
+    const double target_dr = (T.rmax - T.rmin) / T.nact;
+    const int action = regrid_decision(P, cur, target_dr);
+    if (action == SPLIT && ntrack < G.cap - 1) {
+      rec_load(G, o + k, k <= n0 - 2, nxt);
+      // Grid::split (2d.cpp:685-764)
+      double gC[NQ];
+      const double cenL = cen_r(prev.x, prev.dx), cenC = cen_r(cur.x, cur.dx), cenR = cen_r(nxt.x, nxt.dx);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const double gL = (cur.prim[q] - prev.prim[q]) / (cenC - cenL);
+        const double gR = (nxt.prim[q] - cur.prim[q]) / (cenR - cenC);
+        gC[q] = minmod(gL, gR);
+      }
+      const double x_old = cur.x, dl_old = cur.dx;
+      Rec A = cur, B = nxt;  // the right half reuses the record of the old right neighbour
+      A.x = x_old - dl_old / 4.;
+      B.x = x_old + dl_old / 4.;
+      A.dx = dl_old / 2.;
+      B.dx = dl_old / 2.;
+      const double xL = cen_r(A.x, A.dx), xR = cen_r(B.x, B.dx);
+      const double xI = A.x + A.dx / 2.;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const double Sc = cur.prim[q];
+        A.prim[q] = Sc + gC[q] * (xL - xI);
+        B.prim[q] = Sc + gC[q] * (xR - xI);
+      }
+      A.rifx = x_old;
+      B.rifx = cur.rifx;
+      emit(prev);
+      prev = A;
+      cur = B;
+      ++ntrack;
+      ++iR;
+      ++i;
+      ++*nsplit;
+      changed = true;
+      continue;
+    }
+    if (action == MERGE && ntrack > 2 * ng + 2) {
+      rec_load(G, o + k, k <= n0 - 2, nxt);
+      // Grid::merge (2d.cpp:767-832)
+      const bool left = (prev.dx < nxt.dx && i != ng) || i == (ntrack - 2 * ng) + ng - 1;
+      const Rec &vic = left ? prev : nxt;
+      double cc[NQ], cv[NQ], cons[NQ];
+      prim2cons(ph, cur.prim, cc, cur.x);
+      prim2cons(ph, vic.prim, cv, vic.x);
+      const double dV_loc = make_geom(cur.x, cur.dx, tj).dV;
+      const double dV_vic = make_geom(vic.x, vic.dx, tj).dV;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) cons[q] = (cc[q] * dV_loc + cv[q] * dV_vic) / (dV_loc + dV_vic);
+      Rec M = cur;
+      if (left) M.x = ((vic.x - vic.dx / 2.) + (cur.x + cur.dx / 2.)) / 2.;
+      else M.x = ((vic.x + vic.dx / 2.) + (cur.x - cur.dx / 2.)) / 2.;
+      M.dx = cur.dx + vic.dx;
+      C2PStats cs;
+      cons2prim(ph, cons, M.prim, M.x, &cs);
+      c2p[0] += 1;
+      c2p[1] += cs.iters;
+      c2p[2] += cs.fallback;
+      if ((unsigned long long)cs.iters > c2p[3]) c2p[3] = cs.iters;
+      if (left) {
+        M.rifx = cur.rifx;
+        emit(M);
+        prev = nxt;
+      } else {
+        M.rifx = nxt.rifx;
+        emit(prev);
+        prev = M;
+      }
+      rec_load(G, o + k + 1, k + 1 <= n0 - 2, cur);
+      k += 2;
+      --ntrack;
+      --iR;
+      ++i;
+      ++*nmerge;
+      changed = true;
+      continue;
+    }
+    emit(prev);
+    prev = cur;
+    rec_load(G, o + k, k <= n0 - 2, cur);
+    ++k;
+    ++i;
+  }
+  emit(prev);
+  emit(cur);
+  for (; k < n0; ++k) {
+    Rec c;
+    rec_load(G, o + k, k <= n0 - 2, c);
+    emit(c);
+  }
+  if (!changed) return;
+  G.ntrack[j] = out;
+  for (int p = 0; p < out; ++p) {
+    const long long gp = o + p;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      G.prim[q * G.NC + gp] = G.rprim[q * G.NC + gp];
+      G.gmv[q * G.NC + gp] = G.rgmv[q * G.NC + gp];
+      G.gf1[q * G.NC + gp] = G.rgf1[q * G.NC + gp];
+    }
+    G.x[gp] = G.rx[gp];
+    G.dx[gp] = G.rdx[gp];
+    G.dtl[gp] = G.rdtl[gp];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) G.nbr[kk * G.NC + gp] = G.rnbr[kk * G.NC + gp];
+    if (p <= out - 2) G.xI[gp] = G.rxI[gp];
+  }
+}
+
+// Whether any active cell of track j would act against target T (the
+// per-cell decision in the original context).  A track with no action leaves
+// the regrid untouched, and a live track with no action keeps its target.
+GB_HD bool regrid_needed(const Params2 &P, const Grid2 &G, int j, const Target &T, int tid, int nth) {
+  const int n = G.ntrack[j], iL = iL_of(G), iR = n - G.ngst;
+  const long long o = (long long)j * G.cap;
+  const double target_dr = (T.rmax - T.rmin) / T.nact;
+  bool any = false;
+  for (int i = iL + 1 + tid; i <= iR - 1; i += nth) {
+    Rec c;
+    for (int q = 0; q < NQ; ++q) c.prim[q] = (q == UU1 || q == UU2) ? G.prim[q * G.NC + o + i] : 0.;
+    c.dx = G.dx[o + i];
+    const int a = regrid_decision(P, c, target_dr);
+    if ((a == SPLIT && n < G.cap - 1) || (a == MERGE && n > 2 * G.ngst + 2)) any = true;
+  }
+  return any;
+}
+
+GB_HD Target track_target(const Grid2 &G, int j) {
+  const int n = G.ntrack[j];
+  const long long o = (long long)j * G.cap;
+  Target T;
+  T.rmin = G.x[o + iL_of(G) + 1];
+  T.rmax = G.x[o + n - G.ngst - 1];
+  T.nact = n - 2 * G.ngst;
+  return T;
+}
+
+}  // namespace d2
+}  // namespace gb

@@ -212,6 +212,77 @@ int gamma_gpu_cons2prim_guess(const gamma_config_t *cfg, double *cons, double *p
  * reference's warm start.  Merges during regrid keep the warm start. */
 int gamma_gpu_set_guess(gamma_ctx_t *ctx, const float *params);
 
+/* ---- 2D runs (r, theta): NUM_D = 2, spherical, rel_sph, shock detection and
+ * local synchrotron (NUM_Q = 10) --------------------------------------------
+ * Replaces the 2D Grid members (src/Dimensions/2d.cpp: initialise 59-95,
+ * updateGhosts 241-321, computeNeighbors 534-606, regrid 609-832,
+ * movDir_ComputeLambda/updateKinematics/computeFluxes 735-839, collect_dt
+ * 842-859, update 861-882) with the theta-wedge blast-wave hooks of
+ * src/Initial/Tests/BM.cpp, and Grid::evolve (src/Timestep/rk3.cpp:98-194).
+ *
+ * A run has NJ = ntheta + 2 ngst tracks (ghost tracks included) of cap =
+ * nmax + 2 ngst cells.  Per-cell arrays have NJ*cap entries, cell (j, i) at
+ * j*cap + i (the reference's Cell::nde_id); per-cell [q] arrays are [NUM_Q][NJ*cap]
+ * in the reference's slot order; interface (j, i) is the right edge of cell
+ * (j, i).  nbr: [4][NJ*cap], the neighbour list of each cell towards track j-1
+ * (first cell id, count) then towards j+1 (Cell::neigh). */
+typedef struct {
+  int ntheta;   /* active theta tracks (Grid::ncell[F1]) */
+  int nmax;     /* active-cell capacity per track (s_par::nmax) */
+  int ngst;     /* 2 */
+  int nq;       /* 10 */
+  int eos;      /* GAMMA_EOS_* */
+  double gamma_ad, cfl, vi;
+} gamma_2d_config_t;
+
+/* the problem module's constants (BM.cpp userKinematics, checkCellForRegrid)
+ * and the normalised synchrotron constants (constants.cpp:12-20) */
+typedef struct {
+  double split_DR, merge_DR;            /* lfac >= 2 */
+  double split_DR_slow, merge_DR_slow;  /* lfac < 2 */
+  double v_out;                         /* outer ghost-interface velocity */
+  double it_hold;                       /* v_out -> 0 after it_hold steps once the flow stops */
+  double Nalpha, Nmp, Nme;
+} gamma_2d_params_t;
+
+typedef struct gamma_2d gamma_2d_t;
+
+/* theta, dtheta: centre and width of each active track (Cell::G.x[F1], dx[F1]) */
+int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta, const double *dtheta, gamma_2d_t **out);
+int gamma_2d_layout(const gamma_2d_t *ctx, int *ntracks, int *cap);
+int gamma_2d_set_params(gamma_2d_t *ctx, const gamma_2d_params_t *params);
+
+/* Host -> device state.  grad_mv, grad_f1, nbr and dt_loc may be NULL (a new
+ * grid: zero gradients, empty lists, dt_loc = 1e15).  run_ghosts = 1 runs the
+ * updateGhosts that precedes Simu::run's loop (simu.cpp:74). */
+int gamma_2d_upload(gamma_2d_t *ctx, const int *ntrack, const double *prim, const double *x, const double *dx,
+                    const double *dt_loc, const double *xI, const double *grad_mv, const double *grad_f1,
+                    const int *nbr, double t, long long it, int run_ghosts);
+
+/* nsteps iterations of the Simu::run loop body (simu.cpp:79-105), one CUDA
+ * graph launch each.  With stats == NULL the call only enqueues the work. */
+int gamma_2d_step(gamma_2d_t *ctx, int nsteps, gamma_step_stats_t *stats);
+
+/* Device -> host state; any pointer may be NULL. */
+int gamma_2d_download(gamma_2d_t *ctx, int *ntrack, double *t, double *dt, long long *it, int *status,
+                      double *prim, double *x, double *dx, double *dt_loc, double *xI, double *grad_mv,
+                      double *grad_f1, int *nbr, double *sd, double *pspec, unsigned char *shocked);
+
+/* Diagnostics: the first part of one loop iteration only -- regrid,
+ * resetShock, updateGhosts and prepForUpdate (simu.cpp:81-89) -- after which
+ * gamma_2d_download and gamma_2d_download_fluxes return the stage-1 state:
+ * interface velocity, lambda_L, lambda_R and moving-direction flux (per
+ * interface), the theta fluxes flux[0][F1] / flux[1][F1] and this stage's
+ * grad_f1 (per cell, [NUM_Q][NJ*cap]).  Continuing with gamma_2d_step after it
+ * is not a reference step. */
+int gamma_2d_prepare(gamma_2d_t *ctx);
+int gamma_2d_download_fluxes(gamma_2d_t *ctx, double *v, double *lL, double *lR, double *flux, double *f1lo,
+                             double *f1hi, double *grad_f1_stage);
+
+void *gamma_2d_stream(gamma_2d_t *ctx);
+const char *gamma_2d_last_error(const gamma_2d_t *ctx);
+void gamma_2d_destroy(gamma_2d_t *ctx);
+
 /* The context's CUDA stream (a cudaStream_t). */
 void *gamma_gpu_stream(gamma_ctx_t *ctx);
 

@@ -95,7 +95,16 @@ int oracle_brent_iterate(oracle_brent *s) {
   return 0;
 }
 
+/* Process-wide replacement of the callers' relative stopping tolerance (0:
+ * keep theirs).  Lets the compiled reference, whose cons2prim stops at a fixed
+ * 1e-13 bracket, be run to convergence so that its solver noise can be told
+ * apart from differences in the rest of the step. */
+static double g_epsrel_override = 0.0;
+
+void oracle_brent_override_epsrel(double epsrel) { g_epsrel_override = epsrel; }
+
 int oracle_brent_continue(double lo, double hi, double epsabs, double epsrel) {
+  if (g_epsrel_override > 0.0) epsrel = g_epsrel_override;
   double min_abs;
   if ((lo > 0.0 && hi > 0.0) || (lo < 0.0 && hi < 0.0))
     min_abs = fmin(fabs(lo), fabs(hi));

@@ -38,6 +38,8 @@ int oracle_brent_set(oracle_brent *s, oracle_fn f, void *params, double lo, doub
 int oracle_brent_iterate(oracle_brent *s);
 /* 1 while |hi-lo| >= epsabs + epsrel*min(|lo|,|hi|) (0 if the bracket spans 0). */
 int oracle_brent_continue(double lo, double hi, double epsabs, double epsrel);
+/* Replace every caller's relative tolerance by epsrel (> 0), or restore them (0). */
+void oracle_brent_override_epsrel(double epsrel);
 
 #ifdef __cplusplus
 }

@@ -16,6 +16,7 @@
 #include "simu.h"
 #include "mpisetup.h"
 #include "constants.h"
+#include "../brent.h"
 
 #define REF_API extern "C" __attribute__((visibility("default")))
 
@@ -142,3 +143,50 @@ REF_API int ref_snapshot(int j, double *prim, double *x, double *dx, double *th,
 /* Grid::computeNeighbors alone (src/Dimensions/2d.cpp:534-606), for tests of
  * the neighbour search on the current grid. */
 REF_API void ref_compute_neighbors(void) { g_simu->grid.computeNeighbors(false); }
+
+/* The first part of one loop iteration, for checks of intermediate results:
+ * what = 1: regrid, resetShock, updateGhosts;  what = 2: ... and prepForUpdate
+ * (the stage-1 fluxes);  what = 3: ... and the stage-1 update. */
+REF_API int ref_partial(int what) {
+  Simu &s = *g_simu;
+  s.grid.regrid();
+#if SHOCK_DETECTION_ == ENABLED_
+  s.grid.apply(&Cell::resetShock);
+#endif
+  s.grid.updateGhosts(s.it, s.t);
+  if (what >= 2) s.grid.prepForUpdate(s.it, s.t);
+  if (what >= 3) {  // the first stage of Grid::evolve (rk3.cpp:101-105)
+#if SHOCK_DETECTION_ == ENABLED_
+    s.grid.apply(&Cell::detectShock);
+#endif
+    s.dt = CFL_ * s.grid.collect_dt();
+    s.grid.copyState0();
+    s.grid.update(s.dt);
+  }
+  return 0;
+}
+
+/* Cell::flux of the cells i < ntrack of track j: out[((s*2 + d)*NUM_Q + q)*cap + i]
+ * (s: left/right side, d: MV/F1), and the interfaces' velocity, lambda_L,
+ * lambda_R and flux: iface[(k*cap + i)], k = 0: v, 1: lL, 2: lR, 3+q: flux[q]. */
+REF_API int ref_fluxes(int j, double *out, double *iface, int cap) {
+  Grid &g = g_simu->grid;
+  const int n = g.ntrack[j];
+  if (n > cap) return -1;
+  for (int i = 0; i < n; ++i)
+    for (int s = 0; s < 2; ++s)
+      for (int d = 0; d < 2; ++d)
+        for (int q = 0; q < NUM_Q; ++q) out[((s * 2 + d) * NUM_Q + q) * cap + i] = g.Ctot[j][i].flux[s][d][q];
+  for (int i = 0; i < n - 1; ++i) {
+    Interface &I = g.Itot[j][i];
+    iface[0 * cap + i] = I.v;
+    iface[1 * cap + i] = I.lL;
+    iface[2 * cap + i] = I.lR;
+    for (int q = 0; q < NUM_Q; ++q) iface[(3 + q) * cap + i] = I.flux[q];
+  }
+  return n;
+}
+
+/* Stopping tolerance of the cons2prim root search (the reference's is 1e-13,
+ * rel_sph.cpp:281); 0 restores it. */
+REF_API void ref_set_c2p_epsrel(double epsrel) { oracle_brent_override_epsrel(epsrel); }

@@ -73,6 +73,10 @@ class RefJet2D:
         lib.ref_set_param.argtypes = [ctypes.c_char_p, ctypes.c_double]
         lib.ref_set_param.restype = ctypes.c_int
         lib.ref_jet2d_derived.argtypes = [_dp]
+        lib.ref_partial.argtypes = [ctypes.c_int]
+        lib.ref_set_c2p_epsrel.argtypes = [ctypes.c_double]
+        lib.ref_fluxes.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int]
+        lib.ref_fluxes.restype = ctypes.c_int
         self.lib = lib
         self.nq = lib.ref_nq()
 
@@ -90,11 +94,26 @@ class RefJet2D:
     def init(self):
         self.lib.ref_init()
 
+    def set_c2p_epsrel(self, epsrel: float):
+        """cons2prim's Brent stopping tolerance (1e-13 in the reference; 0 restores it)"""
+        self.lib.ref_set_c2p_epsrel(float(epsrel))
+
     def step(self, n: int = 1):
         self.lib.ref_step(int(n))
 
     def regrid(self):
         self.lib.ref_regrid()
+
+    def partial(self, what: int):
+        """regrid, resetShock, updateGhosts (what=1) and prepForUpdate (what=2)"""
+        self.lib.ref_partial(int(what))
+
+    def fluxes(self, j: int, cap: int):
+        """(cell fluxes [side, dim, q, i], interface v, lL, lR, flux[q]) of track j"""
+        out = np.zeros(2 * 2 * self.nq * cap)
+        itf = np.zeros((3 + self.nq) * cap)
+        n = self.lib.ref_fluxes(int(j), _ptr(out), _ptr(itf), int(cap))
+        return out.reshape(2, 2, self.nq, cap)[..., :n], itf.reshape(3 + self.nq, cap)[:, :n - 1]
 
     def compute_neighbors(self):
         self.lib.ref_compute_neighbors()
@@ -129,10 +148,12 @@ class RefJet2D:
 
 
 def _worker(args):
-    params, snap_at, nsteps = args
+    params, snap_at, nsteps, epsrel = args
     sim = RefJet2D()
     sim.set_params(**params)
     sim.init()
+    if epsrel:
+        sim.set_c2p_epsrel(epsrel)
     out = {}
     done = 0
     for s in sorted(snap_at):
@@ -145,10 +166,12 @@ def _worker(args):
     return out
 
 
-def run_isolated(params: dict, snap_at=(0,), nsteps: int = 0):
-    """Run one configuration in a fresh spawned process; returns {step: Grid2D}."""
+def run_isolated(params: dict, snap_at=(0,), nsteps: int = 0, c2p_epsrel: float = 0.):
+    """Run one configuration in a fresh spawned process; returns {step: Grid2D}.
+    c2p_epsrel > 0 replaces the reference's cons2prim stopping tolerance after
+    the initial state is built."""
     import multiprocessing as mp
 
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
-        return pool.apply(_worker, ((params, tuple(snap_at), nsteps),))
+        return pool.apply(_worker, ((params, tuple(snap_at), nsteps, c2p_epsrel),))

@@ -12,11 +12,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     src = open(os.path.join(ROOT, "include", "gamma_gpu.h")).read()
-    return sorted(set(re.findall(r"\b(gamma_(?:gpu|mlp)_\w+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(gamma_(?:gpu|mlp|2d)_\w+)\s*\(", src)))
 
 
 def test_header_matches_binding_list():
-    assert declared_symbols() == sorted(gpu.EXPORTS)
+    from gamma_b200 import gpu2d
+    assert declared_symbols() == sorted(gpu.EXPORTS + gpu2d.EXPORTS)
 
 
 def test_library_exports_every_declared_symbol():
