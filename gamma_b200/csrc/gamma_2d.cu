@@ -44,54 +44,48 @@ __device__ void add_stats(Stats2 *S, unsigned long long calls, unsigned long lon
   }
 }
 
-// Per active track (one block each): does any cell act against the first
-// active track's current target?  flags[j] = 1 if so.
-__global__ void k_regrid_check(Params2 P, Grid2 G, int *flags) {
+// Per active track (one block each, from track j0 on): does any cell act
+// against the first active track's current target?  flags[j] = 1 if so.  Run
+// once before the first active track is regridded (for that track) and once
+// after it (for the others, against its final target).
+__global__ void k_regrid_check(Params2 P, Grid2 G, int *flags, int j0) {
   __shared__ int s_any;
-  const int j = jL_of(G) + 1 + blockIdx.x;
+  const int j = j0 + blockIdx.x;
   if (threadIdx.x == 0) s_any = 0;
   __syncthreads();
   const Target T = track_target(G, jL_of(G) + 1);
   if (regrid_needed(P, G, j, T, threadIdx.x, blockDim.x)) s_any = 1;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    flags[j] = s_any;
-    if (j == jL_of(G) + 1) {  // the reference target of the other tracks if this one does not change
-      double *t0 = reinterpret_cast<double *>(flags + ((G.NJ + 1) & ~1));
-      t0[0] = T.rmin;
-      t0[1] = T.rmax;
-      t0[2] = (double)T.nact;
+  if (threadIdx.x == 0) flags[j] = s_any;
+}
+
+// Regrid of active tracks j0, j0+1, ... (one block each) that have an action:
+// warp 0 plans the walk, the block moves the records.  live: the block's track
+// is the one the criterion measures (run alone, first).
+__global__ void k_regrid(Phys ph, Params2 P, Grid2 G, Stats2 *S, const int *flags, int j0, int live) {
+  const int j = j0 + blockIdx.x;
+  if (!flags[j]) return;
+  __shared__ int s_plan[3];
+  const int n0 = G.ntrack[j];
+  if (threadIdx.x < 32) {
+    const Target T = live ? Target{0., 0., 1} : track_target(G, jL_of(G) + 1);
+    const PlanOut R = regrid_plan(ph, P, G, j, live != 0, T);
+    if (threadIdx.x == 0) {
+      s_plan[0] = R.nnew;
+      s_plan[1] = R.nseg;
+      s_plan[2] = R.first;
+      if (R.splits) atomicAdd(&S->splits, R.splits);
+      if (R.merges) atomicAdd(&S->merges, R.merges);
+      if (R.c2p[0]) {
+        atomicAdd(&S->c2p_calls, R.c2p[0]);
+        atomicAdd(&S->c2p_iters, R.c2p[1]);
+        if (R.c2p[2]) atomicAdd(&S->c2p_fallbacks, R.c2p[2]);
+        atomicMax(&S->c2p_max_iters, R.c2p[3]);
+      }
     }
   }
-}
-
-__global__ void k_regrid_live(Phys ph, Params2 P, Grid2 G, Stats2 *S, const int *flags) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  if (!flags[jL_of(G) + 1]) return;
-  unsigned long long c2p[4] = {0, 0, 0, 0}, ns = 0, nm = 0;
-  Target none{0., 0., 1};
-  regrid_track(ph, P, G, jL_of(G) + 1, true, none, &ns, &nm, c2p);
-  S->splits += ns;
-  S->merges += nm;
-  S->c2p_calls += c2p[0];
-  S->c2p_iters += c2p[1];
-  S->c2p_fallbacks += c2p[2];
-  if (c2p[3] > S->c2p_max_iters) S->c2p_max_iters = c2p[3];
-}
-
-// the other active tracks, one thread each, against the first active track
-__global__ void k_regrid_rest(Phys ph, Params2 P, Grid2 G, Stats2 *S, const int *flags) {
-  const int j = jL_of(G) + 2 + blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long c2p[4] = {0, 0, 0, 0}, ns = 0, nm = 0;
-  if (j <= jR_of(G) - 1) {
-    const Target T = track_target(G, jL_of(G) + 1);
-    const double *t0 = reinterpret_cast<const double *>(flags + ((G.NJ + 1) & ~1));
-    const bool same = T.rmin == t0[0] && T.rmax == t0[1] && (double)T.nact == t0[2];
-    if (flags[j] || !same) regrid_track(ph, P, G, j, false, T, &ns, &nm, c2p);
-  }
-  if (ns) atomicAdd(&S->splits, ns);
-  if (nm) atomicAdd(&S->merges, nm);
-  add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3]);
+  __syncthreads();
+  regrid_execute(G, j, n0, s_plan[0], s_plan[1], s_plan[2]);
 }
 
 __global__ void k_ghosts(Grid2 G, int reset) {
@@ -122,8 +116,13 @@ __global__ void k_cellmv(Grid2 G) {
   if (cell_of(G, &j, &i)) cell_mv(G, j, i);
 }
 
+// foreign stale contributors: clear, then one thread per track appends
+__global__ void k_stale_clear(Grid2 G) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < G.NJ; t += gridDim.x * blockDim.x) G.stale_n[t] = 0;
+}
 __global__ void k_stale(Grid2 G) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) stale_table(G);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j <= G.NJ - 2) stale_append(G, j);
 }
 
 __global__ void k_tgrad(Grid2 G) {
@@ -204,7 +203,7 @@ struct gamma_2d {
   std::vector<void *> allocs;
   Grid2 G{};
   Stats2 *d_stats = nullptr;
-  int *d_flags = nullptr;  // [NJ] regrid flags, then 3 doubles: the first active track's target
+  int *d_flags = nullptr;  // [NJ] regrid flags
   std::vector<double> tg;  // host copy of the per-track factors
   std::string err;
 };
@@ -256,14 +255,17 @@ int enqueue_prepare(gamma_2d *c) {
   const Grid2 &G = c->G;
   cudaStream_t s = c->stream;
   const int nb = blocks_of(c->NC);
-  const int nrest = std::max(1, c->cfg.ntheta - 1);
-  k_regrid_check<<<c->cfg.ntheta, kThreads, 0, s>>>(P, G, c->d_flags);
-  k_regrid_live<<<1, 32, 0, s>>>(ph, P, G, c->d_stats, c->d_flags);
-  k_regrid_rest<<<(nrest + 31) / 32, 32, 0, s>>>(ph, P, G, c->d_stats, c->d_flags);
+  k_regrid_check<<<1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst);
+  k_regrid<<<1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst, 1);
+  if (c->cfg.ntheta > 1) {
+    k_regrid_check<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst + 1);
+    k_regrid<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst + 1, 0);
+  }
   k_ghosts<<<c->NJ, kThreads, 0, s>>>(G, 1);
   k_mv<<<nb, kThreads, 0, s>>>(ph, P, G);
   k_cellmv<<<nb, kThreads, 0, s>>>(G);
-  k_stale<<<1, 32, 0, s>>>(G);
+  k_stale_clear<<<(c->NJ + 255) / 256, 256, 0, s>>>(G);
+  k_stale<<<(c->NJ + 127) / 128, 128, 0, s>>>(G);
   k_tgrad<<<nb, kThreads, 0, s>>>(G);
   k_f1own<<<nb, kThreads, 0, s>>>(ph, G);
   k_f1gather<<<nb, kThreads, 0, s>>>(ph, G);
@@ -278,15 +280,18 @@ int enqueue_step(gamma_2d *c) {
   const Grid2 &G = c->G;
   cudaStream_t s = c->stream;
   const int nb = blocks_of(c->NC);
-  const int nrest = std::max(1, c->cfg.ntheta - 1);
-  k_regrid_check<<<c->cfg.ntheta, kThreads, 0, s>>>(P, G, c->d_flags);
-  k_regrid_live<<<1, 32, 0, s>>>(ph, P, G, c->d_stats, c->d_flags);
-  k_regrid_rest<<<(nrest + 31) / 32, 32, 0, s>>>(ph, P, G, c->d_stats, c->d_flags);
+  k_regrid_check<<<1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst);
+  k_regrid<<<1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst, 1);
+  if (c->cfg.ntheta > 1) {
+    k_regrid_check<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst + 1);
+    k_regrid<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst + 1, 0);
+  }
   for (int stage = 1; stage <= 3; ++stage) {
     k_ghosts<<<c->NJ, kThreads, 0, s>>>(G, stage == 1);
     k_mv<<<nb, kThreads, 0, s>>>(ph, P, G);
     k_cellmv<<<nb, kThreads, 0, s>>>(G);
-    k_stale<<<1, 32, 0, s>>>(G);
+    k_stale_clear<<<(c->NJ + 255) / 256, 256, 0, s>>>(G);
+    k_stale<<<(c->NJ + 127) / 128, 128, 0, s>>>(G);
     k_tgrad<<<nb, kThreads, 0, s>>>(G);
     k_f1own<<<nb, kThreads, 0, s>>>(ph, G);
     k_f1gather<<<nb, kThreads, 0, s>>>(ph, G);
@@ -416,6 +421,9 @@ GAMMA_API int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta,
   G2_ALLOC(G.rdtl, NC * d);
   G2_ALLOC(G.rxI, NC * d);
   G2_ALLOC(G.rnbr, 4 * NC * sizeof(int));
+  G2_ALLOC(G.rdV, NC * d);
+  G2_ALLOC(G.rseg, 2 * NC * sizeof(int));
+  G2_ALLOC(G.rnbr2, 4 * NC * sizeof(int));
   G2_ALLOC(c->d_stats, sizeof(Stats2));
   G2_ALLOC(c->d_flags, (size_t)c->NJ * sizeof(int) + 4 * d + 8);
 #undef G2_ALLOC

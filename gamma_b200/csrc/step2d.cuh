@@ -75,6 +75,9 @@ struct Grid2 {
   double *rprim, *rgmv, *rgf1;  // [NQ][NC]
   double *rx, *rdx, *rdtl, *rxI;
   int *rnbr;                 // [4][NC]
+  double *rdV;               // [NC] new cells' right interface (original index, or -1)
+  int *rseg;                 // [2 NC]: per track, cap segment starts then cap sources
+  int *rnbr2;                // [4][NC]
   unsigned long long *stats;  // c2p calls, c2p iters, fallbacks, zone updates, splits, merges, max iters
 };
 
@@ -433,28 +436,33 @@ GB_HD void f1_own(const Phys &ph, const Grid2 &G, int j, int i) {
 }
 
 // Foreign stale contributors: cells 0 and ntrack-1 whose (copied) upper list
-// points into a track other than j+1.  One thread builds the table in
-// (j, i) order.
+// points into a track other than j+1.  Each track appends its own (stale_n
+// cleared first); the gather puts a target's entries in (j, i) order.
+GB_HD void stale_append(const Grid2 &G, int j) {
+  const int n = G.ntrack[j];
+  const int cells[2] = {0, n - 1};
+  for (int c = 0; c < 2; ++c) {
+    const long long g = (long long)j * G.cap + cells[c];
+    const int first = G.nbr[2 * G.NC + g], cnt = G.nbr[3 * G.NC + g];
+    if (cnt <= 0) continue;
+    const int t = first / G.cap;
+    if (t == j + 1 || t < 0 || t >= G.NJ) continue;
+#ifdef __CUDA_ARCH__
+    const int k = atomicAdd(&G.stale_n[t], 1);
+#else
+    const int k = G.stale_n[t]++;
+#endif
+    if (k >= KMAX_STALE) {
+      *G.status = 40;
+      continue;
+    }
+    G.stale_id[t * KMAX_STALE + k] = (int)g;
+  }
+}
+
 GB_HD void stale_table(const Grid2 &G) {
   for (int t = 0; t < G.NJ; ++t) G.stale_n[t] = 0;
-  for (int j = 0; j <= G.NJ - 2; ++j) {
-    const int n = G.ntrack[j];
-    const int cells[2] = {0, n - 1};
-    for (int c = 0; c < 2; ++c) {
-      const long long g = (long long)j * G.cap + cells[c];
-      const int first = G.nbr[2 * G.NC + g], cnt = G.nbr[3 * G.NC + g];
-      if (cnt <= 0) continue;
-      const int t = first / G.cap;
-      if (t == j + 1 || t < 0 || t >= G.NJ) continue;
-      const int k = G.stale_n[t];
-      if (k >= KMAX_STALE) {
-        *G.status = 40;
-        continue;
-      }
-      G.stale_id[t * KMAX_STALE + k] = (int)g;
-      G.stale_n[t] = k + 1;
-    }
-  }
+  for (int j = 0; j <= G.NJ - 2; ++j) stale_append(G, j);
 }
 
 // cn's side: flux[0][F1] and reverse shocks, summed over the cells whose upper
@@ -478,10 +486,21 @@ GB_HD void f1_gather(const Phys &ph, const Grid2 &G, int t, int k) {
     // reverse test returns early
     if ((r.have_rev || r.have_fwd) && P_SPEC > ps) ps = P_SPEC;
   };
-  const int ns = G.stale_n[t];
-  // foreign stale contributors from tracks below t-1
+  // foreign stale contributors, sorted by cell id (= (j, i) order)
+  int ns = G.stale_n[t];
+  if (ns > KMAX_STALE) ns = KMAX_STALE;
+  int sid[KMAX_STALE];
   for (int s = 0; s < ns; ++s) {
-    const long long g0 = G.stale_id[t * KMAX_STALE + s];
+    int v = G.stale_id[t * KMAX_STALE + s], p = s;
+    while (p > 0 && sid[p - 1] > v) {
+      sid[p] = sid[p - 1];
+      --p;
+    }
+    sid[p] = v;
+  }
+  // ... from tracks below t-1
+  for (int s = 0; s < ns; ++s) {
+    const long long g0 = sid[s];
     const int j = (int)(g0 / G.cap);
     if (j < t - 1) add(j, g0);
   }
@@ -514,9 +533,9 @@ GB_HD void f1_gather(const Phys &ph, const Grid2 &G, int t, int k) {
     for (int i = begin + 1; i <= last; ++i) add(j, o + i);
     if (n - 1 > 0) add(j, o + n - 1);  // cell ntrack-1 (stale)
   }
-  // foreign stale contributors from track t and above
+  // ... from track t and above
   for (int s = 0; s < ns; ++s) {
-    const long long g0 = G.stale_id[t * KMAX_STALE + s];
+    const long long g0 = sid[s];
     const int j = (int)(g0 / G.cap);
     if (j >= t) add(j, g0);
   }
@@ -890,6 +909,387 @@ GB_HD Target track_target(const Grid2 &G, int j) {
   T.nact = n - 2 * G.ngst;
   return T;
 }
+
+#ifdef __CUDACC__
+// ---------------------------------------------------------------------------
+// The same regrid walk on the GPU, planned by one warp and executed by the
+// block.  The plan reads only what the criterion needs (dr, u_r, u_theta) for
+// most cells: 32 lanes test the next 32 original cells against the current
+// target at once, and the walk jumps to the first that acts (with no action
+// in between, neither the target nor any position changes).  Splits and merges
+// are done by lane 0 on full records, whose results go to the scratch rows
+// as "new" cells.  The new track is a list of segments -- runs of original
+// cells or single new cells -- which all threads then expand from the first
+// changed position on.  Scratch per track: seg_start / seg_src (2 cap ints
+// from j*cap in rnbr rows 0-1 ... ), new cells in the r* rows at j*cap + id.
+
+struct Desc {  // a cell as the planner sees it
+  int orig;     // original index, or -1 - id for a new cell
+  double x, dx, u1, u2;
+};
+
+__device__ __forceinline__ Desc desc_orig(const Grid2 &G, long long o, int m) {
+  Desc d;
+  d.orig = m;
+  d.x = G.x[o + m];
+  d.dx = G.dx[o + m];
+  d.u1 = G.prim[UU1 * G.NC + o + m];
+  d.u2 = G.prim[UU2 * G.NC + o + m];
+  return d;
+}
+
+__device__ __forceinline__ int decide(const Params2 &P, double dx, double u1, double u2, double target_dr) {
+  double u = 0.;
+  u += u1 * u1;
+  u += u2 * u2;
+  u = sqrt(u);
+  const double lf = sqrt(1 + u * u);
+  double split_DR = P.split_DR, merge_DR = P.merge_DR;
+  if (lf < 2.) {
+    split_DR = P.split_DR_slow;
+    merge_DR = P.merge_DR_slow;
+  }
+  if (dx > split_DR * target_dr) return SPLIT;
+  if (dx < merge_DR * target_dr) return MERGE;
+  return SKIP;
+}
+
+// full record of a planner cell (original or new)
+__device__ void load_rec(const Grid2 &G, long long o, int n0, const Desc &d, Rec &c, int *rif) {
+  if (d.orig >= 0) {
+    rec_load(G, o + d.orig, d.orig <= n0 - 2, c);
+    *rif = d.orig <= n0 - 2 ? d.orig : -1;
+  } else {
+    const long long g = o + (-1 - d.orig);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      c.prim[q] = G.rprim[q * G.NC + g];
+      c.gmv[q] = G.rgmv[q * G.NC + g];
+      c.gf1[q] = G.rgf1[q * G.NC + g];
+    }
+    c.x = G.rx[g];
+    c.dx = G.rdx[g];
+    c.dtl = G.rdtl[g];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c.nbr[k] = G.rnbr[k * G.NC + g];
+    c.rifx = G.rxI[g];
+    *rif = (int)G.rdV[g];
+  }
+}
+
+// store a new cell; returns its descriptor
+__device__ Desc store_new(const Grid2 &G, long long o, int id, const Rec &c, int rif) {
+  const long long g = o + id;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    G.rprim[q * G.NC + g] = c.prim[q];
+    G.rgmv[q * G.NC + g] = c.gmv[q];
+    G.rgf1[q * G.NC + g] = c.gf1[q];
+  }
+  G.rx[g] = c.x;
+  G.rdx[g] = c.dx;
+  G.rdtl[g] = c.dtl;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) G.rnbr[k * G.NC + g] = c.nbr[k];
+  G.rxI[g] = c.rifx;
+  G.rdV[g] = (double)rif;  // right interface: original index, or -1 (position in rxI)
+  Desc d;
+  d.orig = -1 - id;
+  d.x = c.x;
+  d.dx = c.dx;
+  d.u1 = c.prim[UU1];
+  d.u2 = c.prim[UU2];
+  return d;
+}
+
+struct PlanOut {
+  int nnew, nseg, first;
+  unsigned long long splits, merges;
+  unsigned long long c2p[4];
+};
+
+// warp 0 of the block; returns the plan (valid in lane 0)
+__device__ PlanOut regrid_plan(const Phys &ph, const Params2 &P, const Grid2 &G, int j, bool live, Target fixed) {
+  const int lane = threadIdx.x & 31;
+  const int ng = G.ngst, iL = ng - 1;
+  const int n0 = G.ntrack[j];
+  const long long o = (long long)j * G.cap;
+  int *seg_start = G.rseg + 2 * o;
+  int *seg_src = seg_start + G.cap;
+  const TrackGeo tj = tgeo(G, j);
+  PlanOut R{};
+  int ntrack = n0, iR = n0 - ng;
+  int out = 0, nseg = 0, nid = 0, first = 1 << 30, run_next = -2;
+  double x_first = G.x[o + iL + 1];  // current x at position iL+1 (the live bound)
+  auto emit_range = [&](int k0, int k1) {  // originals [k0, k1) at out..
+    if (k1 <= k0) return;
+    if (!(nseg > 0 && run_next == k0)) {
+      if (lane == 0) {
+        seg_start[nseg] = out;
+        seg_src[nseg] = k0;
+      }
+      ++nseg;
+    }
+    if (out != k0 && out < first) first = out;
+    if (out <= iL + 1 && out + (k1 - k0) > iL + 1) x_first = G.x[o + k0 + (iL + 1 - out)];
+    out += k1 - k0;
+    run_next = k1;
+  };
+  auto emit = [&](const Desc &d) {
+    if (d.orig >= 0) {
+      emit_range(d.orig, d.orig + 1);
+      return;
+    }
+    if (lane == 0) {
+      seg_start[nseg] = out;
+      seg_src[nseg] = d.orig;
+    }
+    ++nseg;
+    run_next = -2;
+    if (out < first) first = out;
+    if (out == iL + 1) x_first = d.x;
+    ++out;
+  };
+  emit_range(0, iL);
+  Desc prev = desc_orig(G, o, iL), cur = desc_orig(G, o, iL + 1);
+  int k = iL + 2;
+  int i = iL + 1;
+  while (i <= iR - 1) {
+    Target T = fixed;
+    if (live) {
+      T.rmin = (iL + 1 == i - 1) ? prev.x : ((iL + 1 == i) ? cur.x : x_first);
+      const int pr = iR - 1;
+      T.rmax = (pr == i) ? cur.x : ((pr == i - 1) ? prev.x : G.x[o + k + (pr - i - 1)]);
+      T.nact = ntrack - 2 * ng;
+    }
+    const double target_dr = (T.rmax - T.rmin) / T.nact;
+    int act;
+    if (cur.orig >= 0) {
+      // lanes test originals cur.orig + lane at positions i + lane
+      const int m = cur.orig + lane;
+      const bool valid = i + lane <= iR - 1;
+      int a = SKIP;
+      if (valid) a = decide(P, G.dx[o + m], G.prim[UU1 * G.NC + o + m], G.prim[UU2 * G.NC + o + m], target_dr);
+      const bool acts = valid && ((a == SPLIT && ntrack < G.cap - 1) || (a == MERGE && ntrack > 2 * ng + 2));
+      const unsigned ball = __ballot_sync(0xffffffffu, acts);
+      const unsigned vball = __ballot_sync(0xffffffffu, valid);
+      const int f = ball ? __ffs(ball) - 1 : __popc(vball);
+      if (f > 0) {  // f no-op cells at positions i .. i+f-1
+        emit(prev);
+        emit_range(cur.orig, cur.orig + f - 1);
+        const int c0 = cur.orig;
+        prev = desc_orig(G, o, c0 + f - 1);
+        cur = desc_orig(G, o, c0 + f);
+        k = c0 + f + 1;
+        i += f;
+        continue;
+      }
+      act = __shfl_sync(0xffffffffu, a, 0);
+    } else {
+      act = decide(P, cur.dx, cur.u1, cur.u2, target_dr);
+      if (!((act == SPLIT && ntrack < G.cap - 1) || (act == MERGE && ntrack > 2 * ng + 2))) act = SKIP;
+    }
+    if (act == SPLIT) {
+      // Grid::split (2d.cpp:685-764), by lane 0
+      Desc dA, dB;
+      if (lane == 0) {
+        Rec L, C, N;
+        int rL, rC, rN;
+        load_rec(G, o, n0, prev, L, &rL);
+        load_rec(G, o, n0, cur, C, &rC);
+        load_rec(G, o, n0, desc_orig(G, o, k), N, &rN);
+        double gC[NQ];
+        const double cenL = cen_r(L.x, L.dx), cenC = cen_r(C.x, C.dx), cenR = cen_r(N.x, N.dx);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          const double gL = (C.prim[q] - L.prim[q]) / (cenC - cenL);
+          const double gR = (N.prim[q] - C.prim[q]) / (cenR - cenC);
+          gC[q] = minmod(gL, gR);
+        }
+        const double x_old = C.x, dl_old = C.dx;
+        Rec A = C, B = N;
+        A.x = x_old - dl_old / 4.;
+        B.x = x_old + dl_old / 4.;
+        A.dx = dl_old / 2.;
+        B.dx = dl_old / 2.;
+        const double xL = cen_r(A.x, A.dx), xR = cen_r(B.x, B.dx);
+        const double xI = A.x + A.dx / 2.;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          const double Sc = C.prim[q];
+          A.prim[q] = Sc + gC[q] * (xL - xI);
+          B.prim[q] = Sc + gC[q] * (xR - xI);
+        }
+        A.rifx = x_old;
+        B.rifx = C.rifx;
+        dA = store_new(G, o, nid, A, -1);
+        dB = store_new(G, o, nid + 1, B, rC);
+      }
+      nid += 2;
+      emit(prev);
+      prev.orig = __shfl_sync(0xffffffffu, dA.orig, 0);
+      prev.x = __shfl_sync(0xffffffffu, dA.x, 0);
+      prev.dx = __shfl_sync(0xffffffffu, dA.dx, 0);
+      prev.u1 = __shfl_sync(0xffffffffu, dA.u1, 0);
+      prev.u2 = __shfl_sync(0xffffffffu, dA.u2, 0);
+      cur.orig = __shfl_sync(0xffffffffu, dB.orig, 0);
+      cur.x = __shfl_sync(0xffffffffu, dB.x, 0);
+      cur.dx = __shfl_sync(0xffffffffu, dB.dx, 0);
+      cur.u1 = __shfl_sync(0xffffffffu, dB.u1, 0);
+      cur.u2 = __shfl_sync(0xffffffffu, dB.u2, 0);
+      ++ntrack;
+      ++iR;
+      ++i;
+      ++R.splits;
+      continue;
+    }
+    if (act == MERGE) {
+      // Grid::merge (2d.cpp:767-832), by lane 0
+      const Desc nxt = desc_orig(G, o, k);
+      const bool left = (prev.dx < nxt.dx && i != ng) || i == (ntrack - 2 * ng) + ng - 1;
+      Desc dM;
+      if (lane == 0) {
+        Rec C, V;
+        int rC, rV;
+        load_rec(G, o, n0, cur, C, &rC);
+        load_rec(G, o, n0, left ? prev : nxt, V, &rV);
+        double cc[NQ], cv[NQ], cons[NQ];
+        prim2cons(ph, C.prim, cc, C.x);
+        prim2cons(ph, V.prim, cv, V.x);
+        const double dV_loc = make_geom(C.x, C.dx, tj).dV;
+        const double dV_vic = make_geom(V.x, V.dx, tj).dV;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) cons[q] = (cc[q] * dV_loc + cv[q] * dV_vic) / (dV_loc + dV_vic);
+        Rec M = C;
+        if (left) M.x = ((V.x - V.dx / 2.) + (C.x + C.dx / 2.)) / 2.;
+        else M.x = ((V.x + V.dx / 2.) + (C.x - C.dx / 2.)) / 2.;
+        M.dx = C.dx + V.dx;
+        C2PStats cs;
+        cons2prim(ph, cons, M.prim, M.x, &cs);
+        R.c2p[0] += 1;
+        R.c2p[1] += cs.iters;
+        R.c2p[2] += cs.fallback;
+        if ((unsigned long long)cs.iters > R.c2p[3]) R.c2p[3] = cs.iters;
+        int rM;
+        if (left) {
+          M.rifx = C.rifx;
+          rM = rC;
+        } else {
+          M.rifx = V.rifx;
+          rM = rV;
+        }
+        dM = store_new(G, o, nid, M, rM);
+      }
+      nid += 1;
+      dM.orig = __shfl_sync(0xffffffffu, dM.orig, 0);
+      dM.x = __shfl_sync(0xffffffffu, dM.x, 0);
+      dM.dx = __shfl_sync(0xffffffffu, dM.dx, 0);
+      dM.u1 = __shfl_sync(0xffffffffu, dM.u1, 0);
+      dM.u2 = __shfl_sync(0xffffffffu, dM.u2, 0);
+      if (left) {
+        emit(dM);
+        prev = nxt;
+      } else {
+        emit(prev);
+        prev = dM;
+      }
+      cur = desc_orig(G, o, k + 1);
+      k += 2;
+      --ntrack;
+      --iR;
+      ++i;
+      ++R.merges;
+      continue;
+    }
+    emit(prev);
+    prev = cur;
+    cur = desc_orig(G, o, k);
+    ++k;
+    ++i;
+  }
+  emit(prev);
+  emit(cur);
+  emit_range(k, n0);
+  R.nnew = out;
+  R.nseg = nseg;
+  R.first = first;
+  return R;
+}
+
+// all threads of the block: expand the plan from the first changed position
+__device__ void regrid_execute(const Grid2 &G, int j, int n0, int nnew, int nseg, int first) {
+  const long long o = (long long)j * G.cap;
+  const int *seg_start = G.rseg + 2 * o;
+  const int *seg_src = seg_start + G.cap;
+  if (first >= nnew && nnew == n0) return;
+  // stage the new track from `first` in the rows of a second scratch (the
+  // gf1n rows: overwritten by the next transverse-gradient pass anyway) ...
+  // positions >= first are written to t*, then copied back
+  double *tp = G.gf1n;  // [NQ][NC]: prim
+  double *tgm = G.cons0;  // [NQ][NC]: grad_mv
+  double *tgf = G.f1lo;   // [NQ][NC]: grad_f1
+  double *tx = G.xI0, *tdx = G.xIm, *tdtl = G.v, *txI = G.lL;
+  int *tnb = G.rnbr2;     // [4][NC]
+  for (int p = first + threadIdx.x; p < nnew; p += blockDim.x) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (seg_start[mid] <= p) lo = mid;
+      else hi = mid - 1;
+    }
+    const int src = seg_src[lo];
+    const long long gp = o + p;
+    if (src >= 0) {
+      const long long gk = o + src + (p - seg_start[lo]);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        tp[q * G.NC + gp] = G.prim[q * G.NC + gk];
+        tgm[q * G.NC + gp] = G.gmv[q * G.NC + gk];
+        tgf[q * G.NC + gp] = G.gf1[q * G.NC + gk];
+      }
+      tx[gp] = G.x[gk];
+      tdx[gp] = G.dx[gk];
+      tdtl[gp] = G.dtl[gk];
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) tnb[kk * G.NC + gp] = G.nbr[kk * G.NC + gk];
+      txI[gp] = G.xI[gk];
+    } else {
+      const long long gn = o + (-1 - src);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        tp[q * G.NC + gp] = G.rprim[q * G.NC + gn];
+        tgm[q * G.NC + gp] = G.rgmv[q * G.NC + gn];
+        tgf[q * G.NC + gp] = G.rgf1[q * G.NC + gn];
+      }
+      tx[gp] = G.rx[gn];
+      tdx[gp] = G.rdx[gn];
+      tdtl[gp] = G.rdtl[gn];
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) tnb[kk * G.NC + gp] = G.rnbr[kk * G.NC + gn];
+      const int rif = (int)G.rdV[gn];
+      txI[gp] = rif >= 0 ? G.xI[o + rif] : G.rxI[gn];
+    }
+  }
+  __syncthreads();
+  for (int p = first + threadIdx.x; p < nnew; p += blockDim.x) {
+    const long long gp = o + p;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      G.prim[q * G.NC + gp] = tp[q * G.NC + gp];
+      G.gmv[q * G.NC + gp] = tgm[q * G.NC + gp];
+      G.gf1[q * G.NC + gp] = tgf[q * G.NC + gp];
+    }
+    G.x[gp] = tx[gp];
+    G.dx[gp] = tdx[gp];
+    G.dtl[gp] = tdtl[gp];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) G.nbr[kk * G.NC + gp] = tnb[kk * G.NC + gp];
+    if (p <= nnew - 2) G.xI[gp] = txI[gp];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) G.ntrack[j] = nnew;
+}
+#endif  // __CUDACC__
 
 }  // namespace d2
 }  // namespace gb

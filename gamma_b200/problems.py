@@ -336,3 +336,154 @@ def unpack(out: dict, r: int, offsets) -> TrackState:
     return TrackState(n, 0, out["prim"][:, o:o + n].copy(), out["x"][o:o + n].copy(), out["dx"][o:o + n].copy(),
                       out["xI"][o:o + n - 1].copy(), out["dt_loc"][o:o + n].copy(), float(out["t"][r]),
                       int(out["it"][r]))
+
+
+@dataclass
+class Jet2dSetup:
+    """2D spherical (r, theta) blast wave on a wedge of theta tracks: the
+    Blandford-McKee profile in the tracks whose centre lies below th_jet, cold
+    ambient medium elsewhere.  The hooks follow src/Initial/Tests/BM.cpp (2D):
+    uniform radial cells over [r_lo, r_hi] R_shock, LORENTZ_ == 1 start
+    (Gamma_shock^2 given), ambient beyond the shock, checkCellForRegrid against
+    the first active track's mean spacing, outer ghost interfaces at v_out.
+    The state it builds is what Simu::initialise leaves (initialGeometry,
+    initialValues, mpi_distribute, prepForRun: v2u + interfaceGeomFromCellPos,
+    radiation_initGammas); the ghost tracks and cells are filled on the device
+    (gamma_2d_upload with run_ghosts = 1, the updateGhosts before the loop)."""
+
+    n0: float = 1.0
+    eta: float = 1.e-10
+    Etot: float = 1.e53
+    n_ext: float = 1.0
+    lfac_shock2: float = 2.e4
+    Rscale: float = 1.e17
+    k: float = 0.0
+    ncell: int = 400
+    ntheta: int = 16
+    nmax: int = 800
+    ngst: int = 2
+    r_lo: float = 0.9
+    r_hi: float = 1.1
+    th_min: float = 0.0
+    th_max: float = 0.2
+    th_jet: float = 0.1
+    nbins: int = 1
+    split_DR: float = 5.0
+    merge_DR: float = 0.3
+    split_DR_slow: float = 20.0
+    merge_DR_slow: float = 1.2
+    v_out: float = 1.05
+    it_hold: float = 1000.0
+    gamma_ad: float = 4. / 3.
+
+    nq = 10
+
+    def derived(self) -> dict:
+        """BM.cpp:13-55 (LORENTZ_ == 1) and normalizeConstants (constants.cpp:12-20)."""
+        G, k = self.gamma_ad, self.k
+        d = {"rhoNorm": self.n0 * MP, "lNorm": C_LIGHT, "vNorm": C_LIGHT}
+        d["pNorm"] = d["rhoNorm"] * d["vNorm"] * d["vNorm"]
+        d["lfacShock2"] = self.lfac_shock2
+        d["tstart"] = math.pow(self.Etot * (17.) / (8. * PI * self.n_ext * MP * math.pow(C_LIGHT, 5.) *
+                                                  d["lfacShock2"]), 1. / 3.)
+        d["RShock"] = C_LIGHT * d["tstart"] * (1. - 1. / (1. + 2. * (4. - k) * d["lfacShock2"]))
+        d["rhoa"] = self.n_ext * MP * math.pow(d["RShock"] / self.Rscale, -k)
+        d["pa"] = d["rhoa"] * self.eta * C_LIGHT * C_LIGHT
+        d["ha"] = C_LIGHT * C_LIGHT + d["pa"] * G / (G - 1.) / d["rhoa"]
+        d["pf"] = 2. / 3. * d["lfacShock2"] * d["ha"] * d["rhoa"]
+        d["lfacf"] = math.sqrt(max(1., .5 * d["lfacShock2"]))
+        d["Df"] = 2. * d["lfacShock2"] * d["rhoa"]
+        d["Nalpha"] = ALPHA_SYN / (1. / (d["rhoNorm"] * d["vNorm"] * d["lNorm"]))
+        d["Nmp"] = MP / (d["rhoNorm"] * math.pow(d["lNorm"], 3))
+        d["Nme"] = ME / (d["rhoNorm"] * math.pow(d["lNorm"], 3))
+        return d
+
+    def theta(self):
+        """centre and width of each active track (BM.cpp:110-118)"""
+        n = self.ntheta
+        th = np.array([self.th_min + (self.th_max - self.th_min) * (j + 0.5) / n for j in range(n)])
+        dth = np.full(n, (self.th_max - self.th_min) / n)
+        return th, dth
+
+    def params(self):
+        from .gpu2d import Params2D
+        d = self.derived()
+        return Params2D(self.split_DR, self.merge_DR, self.split_DR_slow, self.merge_DR_slow, self.v_out,
+                        self.it_hold, d["Nalpha"], d["Nmp"], d["Nme"])
+
+    def _radial_profiles(self, d):
+        """(r, dr, BM primitives, ambient primitives) of one track's active cells"""
+        n, k = self.ncell, self.k
+        lNorm, RS = d["lNorm"], d["RShock"]
+        rmin = self.r_lo * RS / lNorm
+        rmax = self.r_hi * RS / lNorm
+        dr = (rmax - rmin) / n
+        r = np.array([rmin + (i + 0.5) * dr for i in range(n)])
+        bm = np.zeros((self.nq, n))
+        amb = np.zeros((self.nq, n))
+        for i in range(n):
+            r_d, dr_d = r[i] * lNorm, dr * lNorm
+            rho = self.n_ext * MP * math.pow(r_d / self.Rscale, -k)
+            amb[RHO, i], amb[UU1, i], amb[PPP, i] = rho / d["rhoNorm"], 0., self.eta * rho * C_LIGHT * C_LIGHT / d["pNorm"]
+            amb[TR1, i] = 1.
+            if r_d > RS:
+                bm[:, i] = amb[:, i]
+                continue
+            ddx = dr_d / self.nbins
+            xl = r_d - dr_d / 2.
+            xr = xl + ddx
+            dV = 4. / 3. * PI * (math.pow(r_d + dr_d / 2., 3) - math.pow(r_d - dr_d / 2., 3))
+            rr = v = p = 0.
+            for _ in range(self.nbins):
+                x = (xr + xl) / 2.
+                ddV = 4. / 3. * PI * (xr * xr * xr - xl * xl * xl)
+                chi = (1. + 2. * (4. - k) * d["lfacShock2"]) * (1. - x / (C_LIGHT * d["tstart"]))
+                dp = d["pf"] * math.pow(chi, -(17. - 4. * k) / (12. - 3. * k))
+                dlfac = math.sqrt(d["lfacf"] * d["lfacf"] / chi + 1)
+                dD = d["Df"] * math.pow(chi, -(7. - 2. * k) / (4. - k))
+                rr += dD / dlfac * ddV / dV
+                v += C_LIGHT * math.sqrt(1. - 1. / (dlfac * dlfac)) * ddV / dV
+                p += dp * ddV / dV
+                xl = xr
+                xr += ddx
+            bm[RHO, i], bm[UU1, i], bm[PPP, i], bm[TR1, i] = rr / d["rhoNorm"], v / d["vNorm"], p / d["pNorm"], 2.
+        # prepForRun: v2u (2d.cpp:1153-1172; the theta velocity is zero)
+        for prof in (bm, amb):
+            for i in range(n):
+                vv = math.sqrt(0. + prof[UU1, i] * prof[UU1, i] + 0. * 0.)
+                prof[UU1, i] *= 1. / math.sqrt(1. - vv * vv)
+            # radiation_initGammas (radiation_sph.cpp:246-260)
+            for i in range(n):
+                u = math.sqrt(0. + prof[UU1, i] * prof[UU1, i] + 0. * 0.)
+                lf = math.sqrt(1 + u * u)
+                rho = prof[RHO, i]
+                lim = lf * math.pow(rho, 4. / 3.)
+                for q in (GMX, GMN):
+                    if prof[q, i] > lim / (lf * rho) or prof[q, i] <= 0.:
+                        prof[q, i] = lim / (lf * rho)
+        return r, dr, bm, amb
+
+    def initial_state(self):
+        from .gpu2d import State2D
+        d = self.derived()
+        g, n = self.ngst, self.ncell
+        NJ, cap = self.ntheta + 2 * g, self.nmax + 2 * g
+        NC = NJ * cap
+        r, dr, bm, amb = self._radial_profiles(d)
+        prim = np.zeros((self.nq, NC))
+        prim[RHO] = 1.
+        prim[PPP] = 1.
+        x, dx, xI = np.zeros(NC), np.zeros(NC), np.zeros(NC)
+        th, _ = self.theta()
+        iL = g - 1
+        for jj in range(self.ntheta):
+            o = (jj + g) * cap
+            a = slice(o + g, o + g + n)
+            prim[:, a] = bm if th[jj] <= self.th_jet else amb
+            x[a], dx[a] = r, dr
+            # interfaceGeomFromCellPos (2d.cpp:1055-1076): right edges, and the
+            # left edge of the first active cell at index iLbnd
+            xI[o + g:o + g + n] = r + dr / 2.
+            xI[o + iL] = r[0] - dr / 2.
+        ntrack = np.full(NJ, n + 2 * g, np.int32)
+        return State2D(NJ, cap, ntrack, prim, x, dx, xI, None, None, None, None, d["tstart"], 0)
