@@ -97,23 +97,55 @@ __global__ void k_ghosts(Grid2 G, int reset) {
   ghosts_cells(G, j, threadIdx.x, blockDim.x);
 }
 
-// flat (track, cell) index of a thread; false past the last cell
-__device__ __forceinline__ bool cell_of(const Grid2 &G, int *j, int *i) {
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= G.NC) return false;
-  *j = (int)(g / G.cap);
-  *i = (int)(g % G.cap);
-  return true;
+// Per-cell passes run over the live cells only: pref[j] = cells of tracks < j
+// (rebuilt after every ghost pass, when the track lengths are final for the
+// stage), and a fixed grid strides over [0, pref[NJ]).
+__global__ void k_prefix(Grid2 G) {
+  __shared__ int part[1024];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int chunk = (G.NJ + nt - 1) / nt;
+  const int j0 = t * chunk, j1 = min(G.NJ, j0 + chunk);
+  int sum = 0;
+  for (int j = j0; j < j1; ++j) sum += G.ntrack[j];
+  part[t] = sum;
+  __syncthreads();
+  for (int off = 1; off < nt; off <<= 1) {  // inclusive scan
+    const int v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - sum;
+  for (int j = j0; j < j1; ++j) {
+    G.pref[j] = run;
+    run += G.ntrack[j];
+  }
+  if (t == nt - 1) G.pref[G.NJ] = part[t];
 }
 
+__device__ __forceinline__ void cell_at(const Grid2 &G, long long g, int *j, int *i) {
+  int lo = 0, hi = G.NJ - 1;  // last track with pref[track] <= g
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (G.pref[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  *j = lo;
+  *i = (int)(g - G.pref[lo]);
+}
+
+#define FOR_LIVE_CELLS(G, j, i)                                                                     \
+  for (long long g_ = blockIdx.x * (long long)blockDim.x + threadIdx.x, n_ = (G).pref[(G).NJ]; g_ < n_; \
+       g_ += (long long)gridDim.x * blockDim.x)                                                     \
+    if (int j = 0, i = 0; cell_at((G), g_, &j, &i), true)
+
 __global__ void k_mv(Phys ph, Params2 P, Grid2 G) {
-  int j, i;
-  if (cell_of(G, &j, &i)) mv_interface(ph, P, G, j, i, *G.it);
+  const long long it = *G.it;
+  FOR_LIVE_CELLS(G, j, i) mv_interface(ph, P, G, j, i, it);
 }
 
 __global__ void k_cellmv(Grid2 G) {
-  int j, i;
-  if (cell_of(G, &j, &i)) cell_mv(G, j, i);
+  FOR_LIVE_CELLS(G, j, i) cell_mv(G, j, i);
 }
 
 // foreign stale contributors: clear, then one thread per track appends
@@ -126,26 +158,22 @@ __global__ void k_stale(Grid2 G) {
 }
 
 __global__ void k_tgrad(Grid2 G) {
-  int j, i;
-  if (cell_of(G, &j, &i)) trans_grad(G, j, i);
+  FOR_LIVE_CELLS(G, j, i) trans_grad(G, j, i);
 }
 
 __global__ void k_f1own(Phys ph, Grid2 G) {
-  int j, i;
-  if (cell_of(G, &j, &i)) f1_own(ph, G, j, i);
+  FOR_LIVE_CELLS(G, j, i) f1_own(ph, G, j, i);
 }
 
 __global__ void k_f1gather(Phys ph, Grid2 G) {
-  int j, i;
-  if (cell_of(G, &j, &i)) f1_gather(ph, G, j, i);
+  FOR_LIVE_CELLS(G, j, i) f1_gather(ph, G, j, i);
 }
 
 // detectShock and collect_dt: per-block minima, then one block
 __global__ void k_dtpart(Grid2 G) {
   __shared__ double red[kThreads / 32];
-  int j, i;
   double m = DT_INF;
-  if (cell_of(G, &j, &i)) m = collect_cell(G, j, i);
+  FOR_LIVE_CELLS(G, j, i) m = fmin(m, collect_cell(G, j, i));
   for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
   __syncthreads();
@@ -169,14 +197,12 @@ __global__ void k_dtfinal(Grid2 G, int nblocks, double cfl) {
 }
 
 __global__ void k_iface(Grid2 G, int stage) {
-  int j, i;
-  if (cell_of(G, &j, &i)) iface_move(G, j, i, stage);
+  FOR_LIVE_CELLS(G, j, i) iface_move(G, j, i, stage);
 }
 
 __global__ void k_update(Phys ph, Params2 P, Grid2 G, int stage, Stats2 *S) {
-  int j, i;
   unsigned long long c2p[4] = {0, 0, 0, 0};
-  if (cell_of(G, &j, &i)) update_cell(ph, P, G, j, i, stage, c2p);
+  FOR_LIVE_CELLS(G, j, i) update_cell(ph, P, G, j, i, stage, c2p);
   add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3]);
 }
 
@@ -247,6 +273,14 @@ Params2 params_of(const gamma_2d_params_t &q) {
 
 int blocks_of(long long n) { return (int)((n + kThreads - 1) / kThreads); }
 
+// fixed grid of the per-cell passes (they stride over the live cells)
+int cell_blocks(const gamma_2d *c) {
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  return std::max(1, std::min(blocks_of(c->NC), nsm * 8));
+}
+
 // The first part of a step: regrid, reset shocks, ghosts and the stage-1
 // fluxes (everything before collect_dt).
 int enqueue_prepare(gamma_2d *c) {
@@ -254,7 +288,7 @@ int enqueue_prepare(gamma_2d *c) {
   const Params2 P = params_of(c->par);
   const Grid2 &G = c->G;
   cudaStream_t s = c->stream;
-  const int nb = blocks_of(c->NC);
+  const int nb = cell_blocks(c);
   k_regrid_check<<<1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst);
   k_regrid<<<1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst, 1);
   if (c->cfg.ntheta > 1) {
@@ -262,6 +296,7 @@ int enqueue_prepare(gamma_2d *c) {
     k_regrid<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst + 1, 0);
   }
   k_ghosts<<<c->NJ, kThreads, 0, s>>>(G, 1);
+  k_prefix<<<1, 1024, 0, s>>>(G);
   k_mv<<<nb, kThreads, 0, s>>>(ph, P, G);
   k_cellmv<<<nb, kThreads, 0, s>>>(G);
   k_stale_clear<<<(c->NJ + 255) / 256, 256, 0, s>>>(G);
@@ -279,7 +314,7 @@ int enqueue_step(gamma_2d *c) {
   const Params2 P = params_of(c->par);
   const Grid2 &G = c->G;
   cudaStream_t s = c->stream;
-  const int nb = blocks_of(c->NC);
+  const int nb = cell_blocks(c);
   k_regrid_check<<<1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst);
   k_regrid<<<1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst, 1);
   if (c->cfg.ntheta > 1) {
@@ -288,6 +323,7 @@ int enqueue_step(gamma_2d *c) {
   }
   for (int stage = 1; stage <= 3; ++stage) {
     k_ghosts<<<c->NJ, kThreads, 0, s>>>(G, stage == 1);
+    k_prefix<<<1, 1024, 0, s>>>(G);
     k_mv<<<nb, kThreads, 0, s>>>(ph, P, G);
     k_cellmv<<<nb, kThreads, 0, s>>>(G);
     k_stale_clear<<<(c->NJ + 255) / 256, 256, 0, s>>>(G);
@@ -413,6 +449,8 @@ GAMMA_API int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta,
   G2_ALLOC(G.it, sizeof(long long));
   G2_ALLOC(G.status, sizeof(int));
   G2_ALLOC(G.red, (size_t)blocks_of(NC) * d);
+  G2_ALLOC(G.pref, ((size_t)c->NJ + 1) * sizeof(int));
+  G2_ALLOC(G.seg, (size_t)SEG_WORDS * KSEG * NC * d);
   G2_ALLOC(G.rprim, q * NC * d);
   G2_ALLOC(G.rgmv, q * NC * d);
   G2_ALLOC(G.rgf1, q * NC * d);

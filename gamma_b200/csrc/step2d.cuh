@@ -36,6 +36,8 @@ namespace gb {
 namespace d2 {
 
 constexpr int KMAX_STALE = 8;  // foreign stale contributors per target track
+constexpr int KSEG = 4;        // theta interfaces kept per cell for the gather (longer lists recompute)
+constexpr int SEG_WORDS = NQ + 2;  // flux[NQ], reverse Sd, flags (1: forward computed, 2: reverse)
 
 // Problem hooks of the theta-wedge blast wave (src/Initial/Tests/BM.cpp)
 struct Params2 {
@@ -71,6 +73,8 @@ struct Grid2 {
   long long *it;
   int *status;               // 30: negative CFL candidate; 40: stale table overflow
   double *red;               // partial minima of dt_loc
+  int *pref;                 // [NJ+1] cells of tracks before j (the live-cell index)
+  double *seg;               // [SEG_WORDS][KSEG * NC]: theta interfaces of each cell's upper list
   // regrid scratch (one track of records per track)
   double *rprim, *rgmv, *rgf1;  // [NQ][NC]
   double *rx, *rdx, *rdtl, *rxI;
@@ -428,6 +432,13 @@ GB_HD void f1_own(const Phys &ph, const Grid2 &G, int j, int i) {
     for (int q = 0; q < NQ; ++q) acc[q] += r.flux[q];
     sd = fmax(sd, r.sd_fwd);
     if (r.have_fwd && P_SPEC > ps) ps = P_SPEC;
+    if (k < KSEG && G.seg) {  // kept for the upper cell's gather
+      const long long sl = g0 * KSEG + k, SN = G.NC * KSEG;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) G.seg[q * SN + sl] = r.flux[q];
+      G.seg[NQ * SN + sl] = r.sd_rev;
+      G.seg[(NQ + 1) * SN + sl] = (r.have_fwd ? 1. : 0.) + (r.have_rev ? 2. : 0.);
+    }
   }
 #pragma unroll
   for (int q = 0; q < NQ; ++q) G.f1hi[q * G.NC + g0] = acc[q];
@@ -478,7 +489,18 @@ GB_HD void f1_gather(const Phys &ph, const Grid2 &G, int t, int k) {
     const int first = G.nbr[2 * G.NC + g0], cnt = G.nbr[3 * G.NC + g0];
     if (!(cnt > 0 && gn >= first && gn < (long long)first + cnt)) return;
     F1Result r;
-    f1_interface(ph, G, j, g0, gn, r);
+    const long long k = gn - first;
+    if (k < KSEG && G.seg) {  // solved by the owning cell's pass
+      const long long sl = g0 * KSEG + k, SN = G.NC * KSEG;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) r.flux[q] = G.seg[q * SN + sl];
+      r.sd_rev = G.seg[NQ * SN + sl];
+      const int fl = (int)G.seg[(NQ + 1) * SN + sl];
+      r.have_fwd = (fl & 1) != 0;
+      r.have_rev = (fl & 2) != 0;
+    } else {
+      f1_interface(ph, G, j, g0, gn, r);
+    }
 #pragma unroll
     for (int q = 0; q < NQ; ++q) acc[q] += r.flux[q];
     sd = fmax(sd, r.sd_rev);
