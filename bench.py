@@ -201,6 +201,79 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+JET2D = dict(ntheta=512, ncell=12000, nmax=12000)  # tracks settle at ~3,000-4,000 cells after the first regrid
+
+
+def _jet2d_cpu_worker(args):
+    """The reference's own 2D step (oracle/_ref/libref_jet2d.so) on a narrower wedge."""
+    params, steps, warmup = args
+    sys.path.insert(0, ROOT)
+    from oracle.refsim2d import RefJet2D
+    s = RefJet2D()
+    s.set_params(**params)
+    s.init()
+    s.step(warmup)
+    n0 = sum(t.ntrack - 4 for t in s.snapshot().tracks[2:-2])
+    t0 = time.perf_counter()
+    s.step(steps)
+    dt = time.perf_counter() - t0
+    n1 = sum(t.ntrack - 4 for t in s.snapshot().tracks[2:-2])
+    return steps * 0.5 * (n0 + n1), dt
+
+
+def jet2d_arm(args, dev_index):
+    """2D (r, theta) blast wave with a jet-like cap: 512 theta tracks over
+    [0, 0.2] rad, BM profile (Gamma_shock^2 = 2e4) inside 0.1 rad, cold ambient
+    outside, the reference problem module's regrid ratios (tracks settle at a
+    few thousand cells), shock detection and synchrotron on."""
+    import torch
+
+    from gamma_b200 import gpu2d, problems
+    s = problems.Jet2dSetup(**JET2D)
+    th, dth = s.theta()
+    g = gpu2d.Grid2DGPU(s.ntheta, s.nmax, th, dth)
+    g.set_params(s.params())
+    g.upload(s.initial_state(), run_ghosts=True)
+    for _ in range(max(args.warmup, 3)):
+        g.step(1, stats=False)
+    st = g.step(1)
+    assert st["status"] == 0, st
+    zones = st["zone_updates"]
+    stream = torch.cuda.ExternalStream(g.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(dev_index) as clk:
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            g.step(args.steps, stats=False)
+            e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out = g.download()
+    g.close()
+    n = out.ntrack[2:-2]
+    res = {"workload": f"{s.ntheta} theta tracks over [{s.th_min}, {s.th_max}] rad, BM cap below {s.th_jet} rad, "
+                       f"{s.ncell} initial cells per track (reference regrid ratios), NUM_Q=10, regrid + shock "
+                       "detection + synchrotron on",
+           "value": zones * args.steps / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / args.steps,
+           "zones_per_step": zones, "cells_per_track": [int(n.min()), int(n.max())],
+           "c2p_mean_newton_iters": st["c2p_iters"] / max(st["c2p_calls"], 1), "clocks": clk.summary()}
+    lib = os.path.join(ROOT, "oracle", "_ref", "libref_jet2d.so")
+    if not args.no_cpu_baseline and os.path.exists(lib):
+        import multiprocessing as mp
+        # a 16-track wedge with 1,200 initial cells per track (the reference moves
+        # whole Cell records for every merge, so its first regrid grows with the
+        # square of the track length; per-zone step cost does not), single-threaded:
+        # its 2D flux loop accumulates into neighbour cells from several threads
+        p = dict(ncell=1200, ntrack=16, nmax=1200)
+        with mp.get_context("spawn").Pool(1) as pool:
+            z, t = pool.apply(_jet2d_cpu_worker, ((p, 10, 3),))
+        res["cpu_baseline"] = {"value": z / t, "unit": "zone-updates/s", "cores": 1, "kind": "reference",
+                               "sample": "the same wedge with 16 tracks of 1,200 initial cells, 10 steps after 3 "
+                                         "warm-up steps, one thread"}
+    return res
+
+
 def learned_arm(args, g, pk, upload, stream, plain_prim, zones_per_step, plain_per_launch, plain_stats,
                 max_over_ranks, barrier, ws):
     """The same workload with the learned cons2prim starting pressure.
@@ -374,6 +447,8 @@ def run_gpu_arm(args):
     if not args.no_learned:
         line["learned_guess"] = learned_arm(args, g, pk, upload, stream, out_prim, zones_per_step, per_launch,
                                             stats0, max_over_ranks, barrier, ws)
+    if not args.no_2d:
+        line["jet2d"] = jet2d_arm(args, local)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         setups_cpu = setups
         cores = os.cpu_count() or 1
@@ -395,6 +470,7 @@ def main():
     ap.add_argument("--impl", default="gamma", choices=["gamma", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned cons2prim guess arm")
+    ap.add_argument("--no-2d", action="store_true", help="skip the 2D (r, theta) workload")
     ap.add_argument("--ntubes", type=int, default=NTUBES, help="smaller batches for profiling captures")
     args = ap.parse_args()
     if args.impl == "reference":
