@@ -217,6 +217,22 @@ GAMMA_API int gamma_mlp_train(float *params, const float *x, const float *y, lon
   return rc;
 }
 
+GAMMA_API int gamma_mlp_loss_grad(const float *params, const float *x, const float *y, int n, float *grad,
+                                  float *loss, void *stream) {
+  if (!params || !x || !y || !grad || n <= 0) return GAMMA_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t smem = sizeof(gb::mlp::TrainSmem);
+  if (cudaFuncSetAttribute(gb::mlp::grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return GAMMA_ERR_CUDA;
+  if (cudaMemsetAsync(grad, 0, NPARAM * sizeof(float), s) != cudaSuccess) return GAMMA_ERR_CUDA;
+  if (loss && cudaMemsetAsync(loss, 0, sizeof(float), s) != cudaSuccess) return GAMMA_ERR_CUDA;
+  const int grid = std::max(1, std::min((n + gb::mlp::TB - 1) / gb::mlp::TB, sm_count()));
+  // the samples in order (multiplier 1, offset 0), one mini-batch of n
+  gb::mlp::grad_kernel<<<grid, gb::mlp::TB, smem, s>>>(params, x, y, n, 1, 0, 0, n, grad, loss);
+  return cudaGetLastError() == cudaSuccess ? GAMMA_OK : GAMMA_ERR_CUDA;
+}
+
 GAMMA_API int gamma_mlp_forward(const float *params, const float *x, long long n, float *out, int tensor_cores,
                                 void *stream) {
   if (!params || !x || !out || n < 0) return GAMMA_ERR_INVALID;

@@ -33,6 +33,7 @@ EXPORTS = (
     "gamma_gpu_download", "gamma_gpu_cons2prim", "gamma_gpu_stream", "gamma_gpu_strerror",
     "gamma_gpu_last_error", "gamma_gpu_destroy",
     "gamma_mlp_param_count", "gamma_mlp_init", "gamma_mlp_pairs", "gamma_mlp_train", "gamma_mlp_forward",
+    "gamma_mlp_loss_grad",
     "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess",
 )
 
@@ -127,12 +128,13 @@ def lib() -> ctypes.CDLL:
         L.gamma_mlp_train.argtypes = [v, v, v, ctypes.c_longlong, ctypes.POINTER(MlpTrain),
                                       ctypes.POINTER(ctypes.c_float), v]
         L.gamma_mlp_forward.argtypes = [v, v, ctypes.c_longlong, v, ctypes.c_int, v]
+        L.gamma_mlp_loss_grad.argtypes = [v, v, v, ctypes.c_int, v, v, v]
         L.gamma_gpu_cons2prim_guess.argtypes = [ctypes.POINTER(Config), v, v, ctypes.c_int, v, v, v]
         L.gamma_gpu_set_guess.argtypes = [v, v]
         for name in ("gamma_gpu_create", "gamma_gpu_layout", "gamma_gpu_set_params", "gamma_gpu_upload",
                      "gamma_gpu_step", "gamma_gpu_regrid", "gamma_gpu_download", "gamma_gpu_cons2prim",
                      "gamma_mlp_param_count", "gamma_mlp_init", "gamma_mlp_pairs", "gamma_mlp_train",
-                     "gamma_mlp_forward", "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess"):
+                     "gamma_mlp_forward", "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess", "gamma_mlp_loss_grad"):
             getattr(L, name).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -302,6 +304,14 @@ def mlp_train(params_ptr: int, x_ptr: int, y_ptr: int, n: int, epochs: int = 8, 
                               ctypes.byref(tc), loss.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                               ctypes.c_void_p(stream) if stream else None))
     return loss[:int(epochs)]
+
+
+def mlp_loss_grad(params_ptr: int, x_ptr: int, y_ptr: int, n: int, grad_ptr: int, loss_ptr: int = 0,
+                  stream: int = 0):
+    """Gradient (and loss) of the training objective over n samples, on device arrays."""
+    _ok(lib().gamma_mlp_loss_grad(ctypes.c_void_p(params_ptr), ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+                                  int(n), ctypes.c_void_p(grad_ptr), ctypes.c_void_p(loss_ptr) if loss_ptr else None,
+                                  ctypes.c_void_p(stream) if stream else None))
 
 
 def mlp_forward(params_ptr: int, x_ptr: int, n: int, out_ptr: int, tensor_cores: bool, stream: int = 0):

@@ -198,6 +198,12 @@ int gamma_mlp_pairs(const gamma_config_t *cfg, const double *prim, long long n_s
 int gamma_mlp_train(float *params, const float *x, const float *y, long long n, const gamma_mlp_train_t *tc,
                     float *loss_per_epoch, void *stream);
 
+/* The training kernel's gradient of the mean squared error over n samples
+ * (device pointers; grad: gamma_mlp_param_count() floats; loss may be NULL),
+ * for checking the hand-written backward pass. */
+int gamma_mlp_loss_grad(const float *params, const float *x, const float *y, int n, float *grad, float *loss,
+                        void *stream);
+
 /* Network outputs for n inputs: FP32 (tensor_cores = 0) or the BF16
  * tensor-core path used inside the step (tensor_cores = 1). */
 int gamma_mlp_forward(const float *params, const float *x, long long n, float *out, int tensor_cores,

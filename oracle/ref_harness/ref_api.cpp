@@ -14,6 +14,7 @@
 #include "simu.h"
 #include "mpisetup.h"
 #include "constants.h"
+#include "../brent.h"
 
 #define REF_API extern "C" __attribute__((visibility("default")))
 
@@ -205,3 +206,7 @@ REF_API void ref_riemann(const double *primL, const double *primR, const double 
     for (int q = 0; q < NUM_Q; ++q) flux[q * n + k] = I.flux[q];
   }
 }
+
+/* Stopping tolerance of the cons2prim root search (the reference's is 1e-13,
+ * rel_sph.cpp:281 / rel_cart.cpp:193); 0 restores it. */
+REF_API void ref_set_c2p_epsrel(double epsrel) { oracle_brent_override_epsrel(epsrel); }

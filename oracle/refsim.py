@@ -74,6 +74,8 @@ class RefSim:
         if hasattr(lib, "ref_set_param"):
             lib.ref_set_param.argtypes = [ctypes.c_char_p, ctypes.c_double]
             lib.ref_set_param.restype = ctypes.c_int
+        if hasattr(lib, "ref_set_c2p_epsrel"):
+            lib.ref_set_c2p_epsrel.argtypes = [ctypes.c_double]
         if hasattr(lib, "ref_bm1d_derived"):
             lib.ref_bm1d_derived.argtypes = [_dp]
         self.lib = lib
@@ -90,6 +92,10 @@ class RefSim:
 
     def init(self):
         self.lib.ref_init()
+
+    def set_c2p_epsrel(self, epsrel: float):
+        """cons2prim's Brent stopping tolerance (1e-13 in the reference; 0 restores it)"""
+        self.lib.ref_set_c2p_epsrel(float(epsrel))
 
     def bm1d_derived(self) -> dict:
         out = np.zeros(8)
@@ -166,10 +172,12 @@ class RefSim:
 
 
 def _worker(args):
-    kind, params, nsteps, snap_at = args
+    kind, params, nsteps, snap_at, epsrel = args
     sim = RefSim(kind)
     sim.set_params(**params)
     sim.init()
+    if epsrel:
+        sim.set_c2p_epsrel(epsrel)
     out = {0: sim.snapshot()} if 0 in snap_at else {}
     done = 0
     for s in sorted(x for x in snap_at if x > 0):
@@ -181,10 +189,12 @@ def _worker(args):
     return out
 
 
-def run_isolated(kind: str, params: dict, nsteps: int, snap_at=(0,)):
-    """Run one configuration in a fresh spawned process; returns {step: Snapshot}."""
+def run_isolated(kind: str, params: dict, nsteps: int, snap_at=(0,), c2p_epsrel: float = 0.):
+    """Run one configuration in a fresh spawned process; returns {step: Snapshot}.
+    c2p_epsrel > 0 replaces the reference's cons2prim stopping tolerance after
+    the initial state is built."""
     import multiprocessing as mp
 
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
-        return pool.apply(_worker, ((kind, params, nsteps, tuple(snap_at)),))
+        return pool.apply(_worker, ((kind, params, nsteps, tuple(snap_at), c2p_epsrel),))

@@ -81,6 +81,53 @@ def test_forward_fp32_and_tensor_core_paths(gpu_available):
     assert np.max(np.abs(got_b - want)) <= 5e-2
 
 
+def _grad_np(P, x, y):
+    """FP64 backward pass of loss = sum((out - y)^2) / (2 n) for the same network"""
+    W1, b1, W2, b2, W3, b3 = _unpack(P.astype(np.float64))
+    n = x.shape[0]
+    z1 = x @ W1.T + b1
+    s1 = 1 / (1 + np.exp(-z1))
+    h1 = z1 * s1
+    z2 = h1 @ W2.T + b2
+    s2 = 1 / (1 + np.exp(-z2))
+    h2 = z2 * s2
+    out = h2 @ W3.T + b3
+    d3 = (out - y) / n
+    gW3, gb3 = d3.T @ h2, d3.sum(0)
+    d2 = (d3 @ W3) * (s2 + z2 * s2 * (1 - s2))
+    gW2, gb2 = d2.T @ h1, d2.sum(0)
+    d1 = (d2 @ W2) * (s1 + z1 * s1 * (1 - s1))
+    gW1, gb1 = d1.T @ x, d1.sum(0)
+    loss = 0.5 * np.sum((out - y) ** 2) / n
+    return np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3.ravel(), gb3]), loss
+
+
+def test_training_gradient_matches_cpu(gpu_available):
+    """The hand-written backward kernel (per-sample deltas staged in shared
+    memory, per-block parameter sums, atomics across blocks) against an FP64
+    NumPy backward pass of the same network on the same samples."""
+    import torch
+
+    from gamma_b200 import gpu
+    P = _params(5)
+    rng = np.random.default_rng(6)
+    n = 3001  # several blocks, the last one partial
+    x = rng.uniform(-1.5, 1.5, (n, 3)).astype(np.float32)
+    y = rng.uniform(-1.0, 2.0, (n, 2)).astype(np.float32)
+    dx, dy = torch.tensor(x, device="cuda"), torch.tensor(y, device="cuda")
+    grad = torch.zeros(gpu.mlp_param_count(), dtype=torch.float32, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    gpu.mlp_loss_grad(P.data_ptr(), dx.data_ptr(), dy.data_ptr(), n, grad.data_ptr(), loss.data_ptr())
+    torch.cuda.synchronize()
+    want, want_loss = _grad_np(P.cpu().numpy(), x.astype(np.float64), y.astype(np.float64))
+    got = grad.cpu().numpy().astype(np.float64)
+    # FP32 sums over 3001 samples: relative to the largest component of each block
+    for a, b in ((0, 192), (192, 256), (256, 4352), (4352, 4416), (4416, 4544), (4544, 4546)):
+        scale = max(np.max(np.abs(want[a:b])), 1e-12)
+        assert np.max(np.abs(got[a:b] - want[a:b])) <= 2e-4 * scale, (a, b)
+    assert abs(loss.item() - want_loss) <= 1e-5 * want_loss
+
+
 def test_training_pairs_from_states(gpu_available):
     import torch
 

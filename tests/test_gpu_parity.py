@@ -373,3 +373,44 @@ def test_full_size_batch_properties(gpu_available):
             for q in (0, 1, 2):
                 assert l1_rel(tr.prim[q, a], ref.prim[q, a]) <= 1e-10
     g.close()
+
+
+def test_synge_eos_bm1d(gpu_available):
+    """The Taub-Mathews (Synge) effective adiabatic index of rel_sph.cpp:37-52
+    in prim2cons, f(p), cons2prim's Newton derivative and the synchrotron
+    sources: the BM1D blast wave with EOS_ = SYNGE_EOS_ and Gamma = 5/3 against
+    the reference compiled that way (wave speeds and the shock detector keep
+    GAMMA_, as in the reference)."""
+    if not ref_available("bm1d_synge"):
+        pytest.skip("oracle/_ref/libref_bm1d_synge.so not built")
+    from oracle.refsim import run_isolated
+    gpu, problems = _gpu()
+    kw = dict(eta=1e-10, lorentz_mode=1, lfac_shock2=1e4, ncell=400, nmax=800, grid_log=1, r_lo=0.98, r_hi=1.02)
+    conv = run_isolated("bm1d_synge", kw, 1, snap_at=(0, 1), c2p_epsrel=1e-15)
+    plain = run_isolated("bm1d_synge", kw, 40, snap_at=(40,))
+    s = problems.Bm1dSetup(gamma_ad=5. / 3., **kw)
+    st0 = s.initial_state()
+    assert np.array_equal(st0.prim[:, 2:-2], conv[0].prim[:, 2:-2])
+    g = gpu.GammaGPU(gpu.config_sph(gamma_ad=5. / 3., eos=gpu.EOS_SYNGE), [s.capacity])
+    g.set_params([s.run_params()])
+    pk = problems.pack([st0], g.offsets, g.total, 10)
+    g.upload(pk["ntrack"], pk["prim"], pk["x"], pk["dx"], pk["xI"], pk["dt_loc"], pk["t"], pk["it"])
+    st = g.step(1)
+    assert st["status"] == 0
+    got = problems.unpack(g.download(), 0, g.offsets)
+    ref = conv[1]
+    assert got.ntrack == ref.ntrack
+    assert abs(got.t - ref.t) <= 1e-14 * ref.t
+    err = _tol_errors(got, ref, 5. / 3., 10)
+    assert err["x"] <= 1e-12 and err["xI"] <= 1e-12, err
+    for q in (0, 1, 4, 6, 7):
+        assert err[q] <= 1e-9, (q, err)
+    st = g.step(39)
+    assert st["status"] == 0 and st["c2p_fallbacks"] == 0
+    got = problems.unpack(g.download(), 0, g.offsets)
+    ref = plain[40]
+    assert got.ntrack == ref.ntrack
+    a = slice(2, got.ntrack - 2)
+    for q in (0, 1, 2):
+        assert l1_rel(got.prim[q, a], ref.prim[q, a]) <= 1e-8, q
+    g.close()
