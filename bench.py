@@ -38,6 +38,7 @@ sys.path.insert(0, ROOT)
 NTUBES = 4096
 SEED = 20241203
 B_ZU_NQ6 = 8 * (8 * (6 + 1) + 1)  # algorithmic bytes per zone-update (456 for NUM_Q = 6)
+B_ZU_NQ10 = 8 * (8 * (10 + 1) + 1)  # 712 for NUM_Q = 10
 METRIC = "zone-updates/s on 1 B200: plain vs batched+learned c2p at L1<=1e-8; HBM % peak"
 
 
@@ -229,7 +230,7 @@ def jet2d_arm(args, dev_index):
     import torch
 
     from gamma_b200 import gpu2d, problems
-    s = problems.Jet2dSetup(**JET2D)
+    s = problems.Jet2dSetup(**dict(JET2D, ntheta=args.ntheta))
     th, dth = s.theta()
     g = gpu2d.Grid2DGPU(s.ntheta, s.nmax, th, dth)
     g.set_params(s.params())
@@ -274,70 +275,235 @@ def jet2d_arm(args, dev_index):
     return res
 
 
-def learned_arm(args, g, pk, upload, stream, plain_prim, zones_per_step, plain_per_launch, plain_stats,
-                max_over_ranks, barrier, ws):
-    """The same workload with the learned cons2prim starting pressure.
+def train_guess(cfg, prim, rows_live, seed):
+    """Train the learned cons2prim starting pressure on device.
 
-    The network is trained here (training pairs: 1M states of the tubes after
-    the timed steps plus 1M drawn states); the result after K steps is compared
-    with the plain run's (L1 over all cells and stored slots)."""
+    Training pairs: up to 1M primitive states picked from the columns
+    `rows_live` of `prim` [nq][N] (host array) plus 1M drawn states.  Returns
+    the device parameter tensor and a summary."""
     import torch
 
     from gamma_b200 import gpu
     dev = torch.device("cuda", torch.cuda.current_device())
     t0 = time.perf_counter()
-    out = g.download()
-    rng = np.random.default_rng(SEED)
-    live = np.concatenate([np.arange(o, o + n) for o, n in zip(g.offsets, out["ntrack"])])
-    pick = np.sort(rng.choice(live, size=min(1_000_000, live.size), replace=False))
-    states = torch.tensor(np.ascontiguousarray(out["prim"][:, pick]), device=dev)
+    rng = np.random.default_rng(seed)
+    pick = np.sort(rng.choice(rows_live, size=min(1_000_000, rows_live.size), replace=False))
+    states = torch.tensor(np.ascontiguousarray(prim[:, pick]), device=dev)
     ns, nu = states.shape[1], 1_000_000
     x = torch.zeros((ns + nu, 3), dtype=torch.float32, device=dev)
     y = torch.zeros((ns + nu, 2), dtype=torch.float32, device=dev)
-    gpu.mlp_pairs(gpu.config_cart(), states.data_ptr(), ns, nu, SEED, x.data_ptr(), y.data_ptr())
+    gpu.mlp_pairs(cfg, states.data_ptr(), ns, nu, seed, x.data_ptr(), y.data_ptr())
     P = torch.zeros(gpu.mlp_param_count(), dtype=torch.float32, device=dev)
-    gpu.mlp_init(P.data_ptr(), SEED)
+    gpu.mlp_init(P.data_ptr(), seed)
     loss = gpu.mlp_train(P.data_ptr(), x.data_ptr(), y.data_ptr(), ns + nu, epochs=6, batch=8192)
     torch.cuda.synchronize()
-    train_s = time.perf_counter() - t0
+    return P, {"pairs": ns + nu, "from_states": ns, "drawn": nu, "epochs": len(loss),
+               "final_loss": float(loss[-1]), "seconds": time.perf_counter() - t0}
 
+
+def live_cells(offsets, ntrack):
+    return np.concatenate([np.arange(o, o + n) for o, n in zip(offsets, ntrack)])
+
+
+def l1_live(got, want, offsets, ntrack, rows):
+    """max over `rows` of the L1 relative difference over the active cells of every run."""
+    act = np.concatenate([np.arange(o + 2, o + n - 2) for o, n in zip(offsets, ntrack)])
+    return max(float(np.sum(np.abs(got[q, act] - want[q, act])) / max(np.sum(np.abs(want[q, act])), 1e-300))
+               for q in rows)
+
+
+def learned_arm(args, g, cfg, upload, stream, plain_out, rows, max_over_ranks, barrier, ws, plain_stats):
+    """The same workload with the learned cons2prim starting pressure.
+
+    The network is trained here (training pairs: up to 1M states of the runs
+    after the plain arm's steps plus 1M drawn states); the result after K steps
+    from the initial state is compared with the plain run's (L1 over the active
+    cells and stored slots; every run must keep the plain run's cell count)."""
+    import torch
+
+    out = g.download()
+    P, train = train_guess(cfg, out["prim"], live_cells(g.offsets, out["ntrack"]), SEED)
     g.set_guess(P.data_ptr())
     # results: K steps from the initial state, against the plain run's K steps
     upload()
     g.step(args.steps, stats=False)
-    got = g.download()["prim"]
-    rows = [0, 1, 2, 4, 5]
-    want = plain_prim.numpy()
-    l1 = max(float(np.sum(np.abs(got[q] - want[q])) / max(np.sum(np.abs(want[q])), 1e-300)) for q in rows)
+    got = g.download()
+    same = bool(np.array_equal(got["ntrack"], plain_out["ntrack"]))
+    l1 = l1_live(got["prim"], plain_out["prim"], g.offsets, plain_out["ntrack"], rows) if same else None
     # timing: same protocol as the plain arm
     upload()
     for _ in range(args.warmup):
         g.step(1, stats=False)
-    st = g.step(1)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    zones = 0
     barrier()
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
         ev[0].record(stream)
         for k in range(args.steps):
-            g.step(1, stats=False)
+            zones += g.step(1)["zone_updates"]
             ev[k + 1].record(stream)
     torch.cuda.synchronize()
     barrier()
     ms = max_over_ranks(sum(ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)))
+    st = g.step(1)
     g.set_guess(0)
     return {
-        "value": ws * zones_per_step * args.steps / (ms / 1e3), "unit": "zone-updates/s",
-        "ms_per_step": ms / args.steps,
+        "value": ws * zones / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / args.steps,
         "mean_newton_iters": st["c2p_iters"] / max(st["c2p_calls"], 1), "max_newton_iters": st["c2p_max_iters"],
         "fallbacks": st["c2p_fallbacks"],
         "plain_mean_newton_iters": plain_stats["c2p_iters"] / max(plain_stats["c2p_calls"], 1),
-        "l1_vs_plain": l1, "steps_compared": args.steps,
-        "training": {"pairs": ns + nu, "from_states": ns, "drawn": nu, "epochs": len(loss),
-                     "final_loss": float(loss[-1]), "seconds": train_s},
+        "l1_vs_plain": l1, "same_cell_counts": same, "steps_compared": args.steps, "training": train,
         "note": "network start replaces the previous-step pressure in every cons2prim of the step; "
                 "Newton still converges to the reference tolerance",
     }
+
+
+SWEEP_RUNS = 1024
+
+
+def sweep_setups(nruns=SWEEP_RUNS, seed=SEED):
+    """Parameter sweep of BM1D blast waves: log10 E_iso ~ U(50, 54) erg,
+    log10 n ~ U(-3, 1) cm^-3, N ~ U{1000..8000} log-spaced cells over
+    [0.9, 1.1] R_shock, Gamma_shock = 100, nmax = 2N."""
+    rng = np.random.default_rng(seed + 1)
+    E = 10. ** rng.uniform(50., 54., nruns)
+    n = 10. ** rng.uniform(-3., 1., nruns)
+    N = rng.integers(1000, 8001, nruns)
+    return [dict(eta=1e-10, lorentz_mode=1, lfac_shock2=1e4, Etot=float(E[i]), n_ext=float(n[i]), ncell=int(N[i]),
+                 nmax=2 * int(N[i]), grid_log=1, r_lo=0.9, r_hi=1.1) for i in range(nruns)]
+
+
+def _sweep_init(kws):
+    sys.path.insert(0, ROOT)
+    from gamma_b200 import problems
+    return [problems.Bm1dSetup(**kw).initial_state() for kw in kws]
+
+
+def _sweep_cpu_worker(args):
+    """The reference's own BM1D build (oracle/_ref/libref_bm1d.so) on some of the
+    sweep's runs: zone-updates of the timed steps and their seconds."""
+    kws, steps, warmup = args
+    sys.path.insert(0, ROOT)
+    from oracle.refsim import RefSim
+    zones, busy = 0, 0.0
+    for kw in kws:  # one process-wide Simu per library: re-initialised per run
+        s = RefSim("bm1d")
+        s.set_params(**kw)
+        s.init()
+        s.step(warmup)
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            s.step(1)
+            busy += time.perf_counter() - t0
+            zones += int(s.scalars()["nact"])
+    return zones, busy
+
+
+def sweep_cpu_baseline(kws, cores, warmup, steps=3):
+    import multiprocessing as mp
+    rng = np.random.default_rng(SEED + 2)
+    idx = rng.choice(len(kws), size=min(2 * cores, len(kws)), replace=False)
+    sample = [kws[i] for i in idx]
+    chunks = [sample[k::cores] for k in range(cores)]
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_sweep_cpu_worker, [(ch, steps, warmup) for ch in chunks if ch])
+    zones = sum(r[0] for r in res)
+    value = zones / max(r[1] for r in res)
+    return {"value": value, "unit": "zone-updates/s", "cores": cores, "kind": "reference",
+            "sample": f"{len(sample)} of the {len(kws)} runs (seeded), {steps} timed steps each after {warmup} "
+                      f"warm-up steps, {cores} processes; value = sample zone-updates / slowest process"}
+
+
+def sweep_arm(args, dev_index, max_over_ranks, barrier, ws):
+    """C4: independent BM1D runs of uneven size and parameters, one persistent
+    launch per step (one CTA per run, work queue longest-first), regrid, shock
+    detection and synchrotron on; plain and with the learned guess."""
+    import multiprocessing as mp
+
+    import torch
+
+    from gamma_b200 import gpu, problems
+    kws = sweep_setups(args.sweep_runs)
+    setups = [problems.Bm1dSetup(**k) for k in kws]
+    chunks = [kws[i::16] for i in range(16)]
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        parts = pool.map(_sweep_init, chunks)
+    states = [None] * len(kws)
+    for i in range(16):
+        states[i::16] = parts[i]
+    cfg = gpu.config_sph()
+    g = gpu.GammaGPU(cfg, [s.capacity for s in setups])
+    g.set_params([s.run_params() for s in setups])
+    pk = problems.pack(states, g.offsets, g.total, 10)
+    host = {k: torch.from_numpy(np.ascontiguousarray(pk[k])).pin_memory() for k in ("prim", "x", "dx", "dt_loc", "xI")}
+    out_prim = torch.empty_like(host["prim"]).pin_memory()
+    stream = torch.cuda.ExternalStream(g.stream)
+
+    def upload():
+        g.upload_ptrs(pk["ntrack"], pk["t"], pk["it"], host["prim"].data_ptr(), host["x"].data_ptr(),
+                      host["dx"].data_ptr(), host["dt_loc"].data_ptr(), host["xI"].data_ptr())
+
+    upload()
+    for _ in range(max(args.warmup, 3)):
+        g.step(1, stats=False)
+    stats0 = g.step(1)
+    assert stats0["status"] == 0, stats0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    zones = 0
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev_index) as clk:
+        with torch.cuda.stream(stream):
+            ev[0].record(stream)
+            for k in range(args.steps):
+                zones += g.step(1)["zone_updates"]
+                ev[k + 1].record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    per_launch = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    ms = max_over_ranks(sum(per_launch))
+    # end to end from pinned host memory: upload, K steps, download of the primitives
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    zones_e2e = 0
+    barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        upload()
+        for _ in range(args.steps):
+            zones_e2e += g.step(1)["zone_updates"]
+        nt_e2e = g.download_ptrs(out_prim.data_ptr())
+        e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    plain_out = {"ntrack": nt_e2e, "prim": out_prim.numpy().copy()}
+    peak, peak_kind = measured_peak_hbm()
+    achieved = B_ZU_NQ10 * (zones / args.steps) / (statistics.mean(per_launch) / 1e3) / 1e9
+    res = {"workload": f"{len(kws)} BM1D blast waves (spherical, Gamma=4/3, NUM_Q=10), log10 E_iso ~ U(50,54), "
+                       "log10 n ~ U(-3,1), N ~ U{1000..8000} log-spaced cells over [0.9,1.1] R_shock, "
+                       "Gamma_shock=100, nmax=2N; regrid + shock detection + synchrotron on; one RK3 step of "
+                       "every run per launch",
+           "runs": len(kws), "initial_zones": int(sum(k["ncell"] for k in kws)),
+           "value": ws * zones / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / args.steps,
+           "zones_per_step": zones / args.steps,
+           "e2e": {"value": ws * zones_e2e / (e2e_ms / 1e3), "unit": "zone-updates/s",
+                   "h2d_bytes_per_step": (sum(v.numel() * 8 for v in host.values()) - host["prim"].numel() * 8 // 10)
+                   / args.steps, "d2h_bytes_per_step": out_prim.numel() * 8 * 9 // 10 / args.steps},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_source": peak_kind, "bytes_per_zone_update": B_ZU_NQ10},
+           "c2p": {"mean_newton_iters": stats0["c2p_iters"] / max(stats0["c2p_calls"], 1),
+                   "max_newton_iters": stats0["c2p_max_iters"], "fallbacks": stats0["c2p_fallbacks"]},
+           "regrid_per_step": {"splits": stats0["splits"], "merges": stats0["merges"]},
+           "clocks": clk.summary(), "gpu_launches": args.steps}
+    if not args.no_learned:
+        res["learned_guess"] = learned_arm(args, g, cfg, upload, stream, plain_out, (0, 1, 2, 4, 5, 6, 7, 8, 9),
+                                           max_over_ranks, barrier, ws, stats0)
+    g.close()
+    if not args.no_cpu_baseline and ws == 1 and os.path.exists(os.path.join(ROOT, "oracle", "_ref",
+                                                                            "libref_bm1d.so")):
+        res["cpu_baseline"] = sweep_cpu_baseline(kws, os.cpu_count() or 1, max(args.warmup, 3))
+    return res
 
 
 def run_gpu_arm(args):
@@ -351,6 +517,30 @@ def run_gpu_arm(args):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    if args.workload != "all":  # one workload alone, as its own line (profiling captures)
+        if args.workload == "jet2d":
+            res = jet2d_arm(args, local)
+        elif args.workload == "sweep":
+            res = sweep_arm(args, local, max_over_ranks, barrier, ws)
+        if args.workload != "tubes":
+            if rank == 0:
+                print(json.dumps(dict({"metric": METRIC, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                                       "higher_is_better": True, "dtype": "f64", "data": "synthetic"}, **res)))
+            if ws > 1:
+                torch.distributed.destroy_process_group()
+            return
 
     setups = tube_setups(args.ntubes)
     states = [s.initial_state() for s in setups]
@@ -369,17 +559,6 @@ def run_gpu_arm(args):
                       host["dx"].data_ptr(), host["dt_loc"].data_ptr(), host["xI"].data_ptr())
 
     stream = torch.cuda.ExternalStream(g.stream)
-
-    def barrier():
-        if ws > 1:
-            torch.distributed.barrier()
-
-    def max_over_ranks(x):
-        if ws == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
 
     upload()
     for _ in range(args.warmup):
@@ -415,7 +594,7 @@ def run_gpu_arm(args):
         upload()
         for _ in range(args.steps):
             g.step(1, stats=False)
-        g.download_ptrs(out_prim.data_ptr())
+        nt_e2e = g.download_ptrs(out_prim.data_ptr())
         e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
@@ -445,10 +624,14 @@ def run_gpu_arm(args):
                 "max_newton_iters": stats0["c2p_max_iters"], "fallbacks": stats0["c2p_fallbacks"]},
     }
     if not args.no_learned:
-        line["learned_guess"] = learned_arm(args, g, pk, upload, stream, out_prim, zones_per_step, per_launch,
-                                            stats0, max_over_ranks, barrier, ws)
-    if not args.no_2d:
+        line["learned_guess"] = learned_arm(args, g, gpu.config_cart(), upload, stream,
+                                            {"ntrack": nt_e2e, "prim": out_prim.numpy().copy()}, (0, 1, 2, 4, 5),
+                                            max_over_ranks, barrier, ws, stats0)
+    g.close()
+    if not args.no_2d and args.workload == "all":
         line["jet2d"] = jet2d_arm(args, local)
+    if not args.no_sweep and args.workload == "all":
+        line["sweep"] = sweep_arm(args, local, max_over_ranks, barrier, ws)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         setups_cpu = setups
         cores = os.cpu_count() or 1
@@ -457,7 +640,6 @@ def run_gpu_arm(args):
         line["cpu_baseline"] = dict(info, value=v, unit="zone-updates/s")
     if rank == 0:
         print(json.dumps(line))
-    g.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
 
@@ -471,7 +653,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned cons2prim guess arm")
     ap.add_argument("--no-2d", action="store_true", help="skip the 2D (r, theta) workload")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the BM1D parameter sweep")
+    ap.add_argument("--workload", default="all", choices=["all", "tubes", "jet2d", "sweep"],
+                    help="one workload alone (profiling captures); 'all' prints the tube line with the others nested")
     ap.add_argument("--ntubes", type=int, default=NTUBES, help="smaller batches for profiling captures")
+    ap.add_argument("--ntheta", type=int, default=JET2D["ntheta"], help="theta tracks of the 2D workload")
+    ap.add_argument("--sweep-runs", type=int, default=SWEEP_RUNS, help="runs of the BM1D sweep")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)

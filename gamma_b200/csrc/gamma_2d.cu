@@ -22,6 +22,11 @@ using namespace gb::d2;
 namespace {
 
 constexpr int kThreads = 256;
+// resident blocks per SM asked of the heavy per-cell passes (interface solves,
+// cell update): their FP64 latency needs warps more than registers
+#ifndef GB2_MINB
+#define GB2_MINB 2
+#endif
 
 struct Stats2 {
   unsigned long long c2p_calls, c2p_iters, c2p_fallbacks, c2p_max_iters, splits, merges, zone_updates;
@@ -88,14 +93,25 @@ __global__ void k_regrid(Phys ph, Params2 P, Grid2 G, Stats2 *S, const int *flag
   regrid_execute(G, j, n0, s_plan[0], s_plan[1], s_plan[2]);
 }
 
-__global__ void k_ghosts(Grid2 G, int reset) {
-  const int j = blockIdx.x;
-  if (reset) ghosts_reset(G, j, threadIdx.x, blockDim.x);
-  __syncthreads();
-  ghosts_tracks(G, j, threadIdx.x, blockDim.x, reset != 0);
-  __syncthreads();
-  ghosts_cells(G, j, threadIdx.x, blockDim.x);
+// updateGhosts in two launches: (1) with `reset`, Cell::resetShock on every
+// slot, and the ghost tracks' copies of the edge tracks, flat over the slots;
+// (2) the ghost cells of every track (after the ghost tracks are complete).
+__global__ void k_ghosts_copy(Grid2 G, int reset) {
+  const long long nreset = reset ? G.NC : 0, ncopy = 2LL * G.ngst * G.cap;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nreset + ncopy;
+       t += (long long)gridDim.x * blockDim.x) {
+    if (t < nreset) {
+      G.sd[t] = -1.;
+      G.pspec[t] = 0.;
+      G.shocked[t] = 0;
+    } else {
+      const long long u = t - nreset;
+      ghosts_track_slot(G, (int)(u / G.cap), (int)(u % G.cap), reset != 0);
+    }
+  }
 }
+
+__global__ void k_ghost_cells(Grid2 G) { ghosts_cells(G, blockIdx.x, threadIdx.x, blockDim.x); }
 
 // Per-cell passes run over the live cells only: pref[j] = cells of tracks < j
 // (rebuilt after every ghost pass, when the track lengths are final for the
@@ -139,7 +155,7 @@ __device__ __forceinline__ void cell_at(const Grid2 &G, long long g, int *j, int
        g_ += (long long)gridDim.x * blockDim.x)                                                     \
     if (int j = 0, i = 0; cell_at((G), g_, &j, &i), true)
 
-__global__ void k_mv(Phys ph, Params2 P, Grid2 G) {
+__global__ void __launch_bounds__(kThreads, GB2_MINB) k_mv(Phys ph, Params2 P, Grid2 G) {
   const long long it = *G.it;
   FOR_LIVE_CELLS(G, j, i) mv_interface(ph, P, G, j, i, it);
 }
@@ -161,11 +177,11 @@ __global__ void k_tgrad(Grid2 G) {
   FOR_LIVE_CELLS(G, j, i) trans_grad(G, j, i);
 }
 
-__global__ void k_f1own(Phys ph, Grid2 G) {
+__global__ void __launch_bounds__(kThreads, GB2_MINB) k_f1own(Phys ph, Grid2 G) {
   FOR_LIVE_CELLS(G, j, i) f1_own(ph, G, j, i);
 }
 
-__global__ void k_f1gather(Phys ph, Grid2 G) {
+__global__ void __launch_bounds__(kThreads, GB2_MINB) k_f1gather(Phys ph, Grid2 G) {
   FOR_LIVE_CELLS(G, j, i) f1_gather(ph, G, j, i);
 }
 
@@ -200,7 +216,7 @@ __global__ void k_iface(Grid2 G, int stage) {
   FOR_LIVE_CELLS(G, j, i) iface_move(G, j, i, stage);
 }
 
-__global__ void k_update(Phys ph, Params2 P, Grid2 G, int stage, Stats2 *S) {
+__global__ void __launch_bounds__(kThreads, GB2_MINB) k_update(Phys ph, Params2 P, Grid2 G, int stage, Stats2 *S) {
   unsigned long long c2p[4] = {0, 0, 0, 0};
   FOR_LIVE_CELLS(G, j, i) update_cell(ph, P, G, j, i, stage, c2p);
   add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3]);
@@ -281,6 +297,11 @@ int cell_blocks(const gamma_2d *c) {
   return std::max(1, std::min(blocks_of(c->NC), nsm * 8));
 }
 
+int ghost_blocks(const gamma_2d *c, bool reset) {
+  const long long n = (reset ? c->NC : 0) + 2LL * c->cfg.ngst * c->cap;
+  return (int)std::max(1LL, std::min((n + kThreads - 1) / kThreads, 148LL * 8));
+}
+
 // The first part of a step: regrid, reset shocks, ghosts and the stage-1
 // fluxes (everything before collect_dt).
 int enqueue_prepare(gamma_2d *c) {
@@ -295,7 +316,8 @@ int enqueue_prepare(gamma_2d *c) {
     k_regrid_check<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst + 1);
     k_regrid<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst + 1, 0);
   }
-  k_ghosts<<<c->NJ, kThreads, 0, s>>>(G, 1);
+  k_ghosts_copy<<<ghost_blocks(c, true), kThreads, 0, s>>>(G, 1);
+  k_ghost_cells<<<c->NJ, 32, 0, s>>>(G);
   k_prefix<<<1, 1024, 0, s>>>(G);
   k_mv<<<nb, kThreads, 0, s>>>(ph, P, G);
   k_cellmv<<<nb, kThreads, 0, s>>>(G);
@@ -322,7 +344,8 @@ int enqueue_step(gamma_2d *c) {
     k_regrid<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst + 1, 0);
   }
   for (int stage = 1; stage <= 3; ++stage) {
-    k_ghosts<<<c->NJ, kThreads, 0, s>>>(G, stage == 1);
+    k_ghosts_copy<<<ghost_blocks(c, stage == 1), kThreads, 0, s>>>(G, stage == 1);
+    k_ghost_cells<<<c->NJ, 32, 0, s>>>(G);
     k_prefix<<<1, 1024, 0, s>>>(G);
     k_mv<<<nb, kThreads, 0, s>>>(ph, P, G);
     k_cellmv<<<nb, kThreads, 0, s>>>(G);
@@ -363,6 +386,8 @@ GAMMA_API int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta,
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess || prop.major != 10) return GAMMA_ERR_NO_DEVICE;
 
+  // neighbour lists hold pooled cell ids as int
+  if ((long long)(cfg->ntheta + 2 * cfg->ngst) * (cfg->nmax + 2 * cfg->ngst) >= (1LL << 31)) return GAMMA_ERR_INVALID;
   gamma_2d *c = new gamma_2d();
   c->cfg = *cfg;
   const int ng = cfg->ngst;
@@ -534,7 +559,8 @@ GAMMA_API int gamma_2d_upload(gamma_2d_t *ctx, const int *ntrack, const double *
   G2_CUDA(c, cudaMemsetAsync(G.dt, 0, d, s));
   G2_CUDA(c, cudaMemsetAsync(G.status, 0, sizeof(int), s));
   if (run_ghosts) {  // the updateGhosts before Simu::run's loop (simu.cpp:74)
-    k_ghosts<<<c->NJ, kThreads, 0, s>>>(G, 0);
+    k_ghosts_copy<<<ghost_blocks(c, false), kThreads, 0, s>>>(G, 0);
+    k_ghost_cells<<<c->NJ, 32, 0, s>>>(G);
     G2_CUDA(c, cudaGetLastError());
   }
   G2_CUDA(c, cudaStreamSynchronize(s));  // host staging vectors go out of scope

@@ -110,50 +110,59 @@ GB_HD void load_prim(const Grid2 &G, long long g, double *p) {
 // after Cell::resetShock of every cell.  The source cells of a ghost track are
 // never written in the same pass (only active cells are copied).
 
+// All loads are issued before the first store: the arrays are distinct, but
+// the compiler cannot prove it and would otherwise wait on each load in turn.
 GB_HD void copy_cell(const Grid2 &G, long long d, long long s, bool reset) {
+  double p[NQ], gm[NQ], gf[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
-    G.prim[q * G.NC + d] = G.prim[q * G.NC + s];
-    G.gmv[q * G.NC + d] = G.gmv[q * G.NC + s];
-    G.gf1[q * G.NC + d] = G.gf1[q * G.NC + s];
+    p[q] = G.prim[q * G.NC + s];
+    gm[q] = G.gmv[q * G.NC + s];
+    gf[q] = G.gf1[q * G.NC + s];
   }
-  G.x[d] = G.x[s];
-  G.dx[d] = G.dx[s];
-  G.dtl[d] = G.dtl[s];
-  if (reset) {
-    G.sd[d] = -1.;
-    G.pspec[d] = 0.;
-    G.shocked[d] = 0;
-  } else {
-    G.sd[d] = G.sd[s];
-    G.pspec[d] = G.pspec[s];
-    G.shocked[d] = G.shocked[s];
+  const double x = G.x[s], dx = G.dx[s], dtl = G.dtl[s];
+  double sd = -1., ps = 0.;
+  int sh = 0;
+  if (!reset) {
+    sd = G.sd[s];
+    ps = G.pspec[s];
+    sh = G.shocked[s];
   }
+  int nb[4];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) G.nbr[k * G.NC + d] = G.nbr[k * G.NC + s];
-}
-
-// phase 0 (reset only): Cell::resetShock on the track's cells
-GB_HD void ghosts_reset(const Grid2 &G, int j, int tid, int nth) {
-  const long long o = (long long)j * G.cap;
-  for (int i = tid; i < G.cap; i += nth) {
-    G.sd[o + i] = -1.;
-    G.pspec[o + i] = 0.;
-    G.shocked[o + i] = 0;
+  for (int k = 0; k < 4; ++k) nb[k] = G.nbr[k * G.NC + s];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    G.prim[q * G.NC + d] = p[q];
+    G.gmv[q * G.NC + d] = gm[q];
+    G.gf1[q * G.NC + d] = gf[q];
   }
+  G.x[d] = x;
+  G.dx[d] = dx;
+  G.dtl[d] = dtl;
+  G.sd[d] = sd;
+  G.pspec[d] = ps;
+  G.shocked[d] = sh;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) G.nbr[k * G.NC + d] = nb[k];
 }
 
-// phase 1: a ghost track takes the active cells and interfaces of the edge track
-GB_HD void ghosts_tracks(const Grid2 &G, int j, int tid, int nth, bool reset) {
-  const int jL = jL_of(G), jR = jR_of(G);
-  if (j > jL && j < jR) return;
-  const int src = j <= jL ? jL + 1 : jR - 1;
+// track holding the pooled cell id g (ids fit in int: NC < 2^31 is checked at creation)
+GB_HD int track_of(const Grid2 &G, long long g) { return (int)g / G.cap; }
+
+// phase 1: a ghost track takes the active cells and interfaces of the edge
+// track; slot i of ghost track number k (0..2 ngst-1, lower tracks first)
+GB_HD int ghost_track(const Grid2 &G, int k) { return k < G.ngst ? k : G.NJ - 2 * G.ngst + k; }
+
+GB_HD void ghosts_track_slot(const Grid2 &G, int k, int i, bool reset) {
+  const int j = ghost_track(G, k);
+  const int src = j <= jL_of(G) ? jL_of(G) + 1 : jR_of(G) - 1;
   const int n = G.ntrack[src];
   const int iL = iL_of(G), iR = n - G.ngst;
-  if (tid == 0) G.ntrack[j] = n;
+  if (i == 0) G.ntrack[j] = n;
   const long long o = (long long)j * G.cap, os = (long long)src * G.cap;
-  for (int i = iL + 1 + tid; i <= iR - 1; i += nth) copy_cell(G, o + i, os + i, reset);
-  for (int i = iL + tid; i <= iR - 1; i += nth) G.xI[o + i] = G.xI[os + i];
+  if (i >= iL + 1 && i <= iR - 1) copy_cell(G, o + i, os + i, reset);
+  if (i >= iL && i <= iR - 1) G.xI[o + i] = G.xI[os + i];
 }
 
 // phase 2: ghost cells and ghost interfaces of the track (after phase 1)
@@ -342,7 +351,7 @@ GB_HD void trans_grad(const Grid2 &G, int j, int i) {
       const int first = G.nbr[(2 * d) * G.NC + g0], cnt = G.nbr[(2 * d + 1) * G.NC + g0];
       for (int k = 0; k < cnt; ++k) {
         const long long gn = first + k;
-        const int jn = (int)(gn / G.cap);
+        const int jn = track_of(G, gn);
         double xm, w;
         overlap(G, g0, gn, &xm, &w);
         // theta of the interface: th - dth/2 below, th (unmoved) above
@@ -381,7 +390,7 @@ struct F1Result {
 };
 
 GB_HD void f1_interface(const Phys &ph, const Grid2 &G, int j, long long g0, long long gn, F1Result &out) {
-  const int jn = (int)(gn / G.cap);
+  const int jn = track_of(G, gn);
   const TrackGeo t0 = tgeo(G, j);
   const double jpos = t0.th + t0.dth / 2.;
   double xm, w;
@@ -456,7 +465,7 @@ GB_HD void stale_append(const Grid2 &G, int j) {
     const long long g = (long long)j * G.cap + cells[c];
     const int first = G.nbr[2 * G.NC + g], cnt = G.nbr[3 * G.NC + g];
     if (cnt <= 0) continue;
-    const int t = first / G.cap;
+    const int t = track_of(G, first);
     if (t == j + 1 || t < 0 || t >= G.NJ) continue;
 #ifdef __CUDA_ARCH__
     const int k = atomicAdd(&G.stale_n[t], 1);
@@ -523,7 +532,7 @@ GB_HD void f1_gather(const Phys &ph, const Grid2 &G, int t, int k) {
   // ... from tracks below t-1
   for (int s = 0; s < ns; ++s) {
     const long long g0 = sid[s];
-    const int j = (int)(g0 / G.cap);
+    const int j = track_of(G, g0);
     if (j < t - 1) add(j, g0);
   }
   if (t >= 1) {
@@ -558,7 +567,7 @@ GB_HD void f1_gather(const Phys &ph, const Grid2 &G, int t, int k) {
   // ... from track t and above
   for (int s = 0; s < ns; ++s) {
     const long long g0 = sid[s];
-    const int j = (int)(g0 / G.cap);
+    const int j = track_of(G, g0);
     if (j >= t) add(j, g0);
   }
 #pragma unroll
