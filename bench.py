@@ -67,6 +67,7 @@ class ClockSampler:
         self.index = index
         self.rows = []
         self.proc = None
+        self.n_before = 0
 
     def __enter__(self):
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -78,6 +79,10 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.perf_counter()  # the first sample marks the start of the timed region
+            while not self.rows and self.proc.poll() is None and time.perf_counter() - t0 < 5.:
+                time.sleep(0.01)
+            self.n_before = len(self.rows)
         except OSError:
             self.proc = None
         return self
@@ -90,6 +95,10 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc:
+            # a region shorter than the sampling period still gets the sample that follows it
+            t0 = time.perf_counter()
+            while len(self.rows) <= self.n_before and self.proc.poll() is None and time.perf_counter() - t0 < 1.:
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -222,43 +231,98 @@ def _jet2d_cpu_worker(args):
     return steps * 0.5 * (n0 + n1), dt
 
 
+def _jet2d_run(s, steps, warmup, guess_ptr=0, dev_index=None):
+    """Fresh 2D grid from the initial state: warm-up steps, one step with
+    statistics, then `steps` timed graph launches (statistics over them)."""
+    import torch
+
+    from gamma_b200 import gpu2d
+    th, dth = s.theta()
+    g = gpu2d.Grid2DGPU(s.ntheta, s.nmax, th, dth)
+    g.set_params(s.params())
+    g.set_guess(guess_ptr)
+    g.upload(s.initial_state(), run_ghosts=True)
+    for _ in range(max(warmup, 3)):
+        g.step(1, stats=False)
+    st0 = g.step(1)
+    assert st0["status"] == 0, st0
+    stream = torch.cuda.ExternalStream(g.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    clk = ClockSampler(dev_index) if dev_index is not None else None
+    if clk:
+        clk.__enter__()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        st = g.step(steps)  # K graph launches, then the statistics (one small copy)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__()
+    assert st["status"] == 0, st
+    out = g.download()
+    g.close()
+    return e0.elapsed_time(e1), st, out, (clk.summary() if clk else None)
+
+
+def _active_cells(out):
+    o = np.arange(out.NJ) * out.cap
+    return np.concatenate([np.arange(o[j] + 2, o[j] + int(out.ntrack[j]) - 2) for j in range(2, out.NJ - 2)])
+
+
 def jet2d_arm(args, dev_index):
     """2D (r, theta) blast wave with a jet-like cap: 512 theta tracks over
     [0, 0.2] rad, BM profile (Gamma_shock^2 = 2e4) inside 0.1 rad, cold ambient
     outside, the reference problem module's regrid ratios (tracks settle at a
-    few thousand cells), shock detection and synchrotron on."""
-    import torch
-
-    from gamma_b200 import gpu2d, problems
+    few thousand cells), shock detection and synchrotron on.  Plain, then with
+    the learned cons2prim start (trained on this run's states and drawn ones)
+    from the same initial state, compared after the same steps."""
+    from gamma_b200 import gpu, problems
     s = problems.Jet2dSetup(**dict(JET2D, ntheta=args.ntheta))
-    th, dth = s.theta()
-    g = gpu2d.Grid2DGPU(s.ntheta, s.nmax, th, dth)
-    g.set_params(s.params())
-    g.upload(s.initial_state(), run_ghosts=True)
-    for _ in range(max(args.warmup, 3)):
-        g.step(1, stats=False)
-    st = g.step(1)
-    assert st["status"] == 0, st
+    ms, st, out, clk = _jet2d_run(s, args.steps, args.warmup, 0, dev_index)
     zones = st["zone_updates"]
-    stream = torch.cuda.ExternalStream(g.stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    with ClockSampler(dev_index) as clk:
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-            g.step(args.steps, stats=False)
-            e1.record(stream)
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    out = g.download()
-    g.close()
     n = out.ntrack[2:-2]
     res = {"workload": f"{s.ntheta} theta tracks over [{s.th_min}, {s.th_max}] rad, BM cap below {s.th_jet} rad, "
                        f"{s.ncell} initial cells per track (reference regrid ratios), NUM_Q=10, regrid + shock "
                        "detection + synchrotron on",
-           "value": zones * args.steps / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / args.steps,
-           "zones_per_step": zones, "cells_per_track": [int(n.min()), int(n.max())],
-           "c2p_mean_newton_iters": st["c2p_iters"] / max(st["c2p_calls"], 1), "clocks": clk.summary()}
+           "value": zones / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / args.steps,
+           "zones_per_step": zones / args.steps, "cells_per_track": [int(n.min()), int(n.max())],
+           "c2p": {"mean_newton_iters": st["c2p_iters"] / max(st["c2p_calls"], 1),
+                   "max_newton_iters": st["c2p_max_iters"], "fallbacks": st["c2p_fallbacks"]},
+           "clocks": clk, "gpu_launches": 43 * args.steps}
+    peak, peak_kind = measured_peak_hbm()
+    achieved = B_ZU_NQ10 * zones / (ms / 1e3) / 1e9
+    res["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                       "peak_source": peak_kind, "bytes_per_zone_update": B_ZU_NQ10,
+                       "note": "whole step (43 launches); per-kernel shares in the ncu launch list"}
+    if not args.no_learned:
+        # training states: the run's active cells, as 1D states of the same |u| (cons2prim sees |S| only)
+        live = _active_cells(out)
+        prim = np.zeros((10, live.size))
+        prim[:, :] = out.prim[:, live]
+        prim[2] = np.hypot(out.prim[2, live], out.prim[3, live])
+        prim[3] = 0.
+        P, train = train_guess(gpu.config_sph(), prim, np.arange(live.size), SEED + 3)
+        ms_l, st_l, out_l, _ = _jet2d_run(s, args.steps, args.warmup, P.data_ptr())
+        same = bool(np.array_equal(out_l.ntrack, out.ntrack))
+        l1 = None
+        if same:
+            l1 = {}
+            for q, name in ((0, "rho"), (1, "p"), (2, "u_r"), (3, "u_theta"), (4, "tracer")):
+                a, b = out_l.prim[q, live], out.prim[q, live]
+                l1[name] = float(np.sum(np.abs(a - b)) / max(np.sum(np.abs(b)), 1e-300))
+        res["learned_guess"] = {
+            "value": st_l["zone_updates"] / (ms_l / 1e3), "unit": "zone-updates/s", "ms_per_step": ms_l / args.steps,
+            "mean_newton_iters": st_l["c2p_iters"] / max(st_l["c2p_calls"], 1),
+            "max_newton_iters": st_l["c2p_max_iters"], "fallbacks": st_l["c2p_fallbacks"],
+            "fallback_rate": st_l["c2p_fallbacks"] / max(st_l["c2p_calls"], 1),
+            "plain_mean_newton_iters": res["c2p"]["mean_newton_iters"],
+            "plain_max_newton_iters": res["c2p"]["max_newton_iters"],
+            "same_cell_counts": same, "l1_vs_plain": l1, "steps_compared": max(args.warmup, 3) + 1 + args.steps,
+            "training": train,
+            "note": "the network's pressure starts every cons2prim of the cell updates (regrid merges keep the "
+                    "warm start); Newton still converges to the reference tolerance"}
+        del P
     lib = os.path.join(ROOT, "oracle", "_ref", "libref_jet2d.so")
     if not args.no_cpu_baseline and os.path.exists(lib):
         import multiprocessing as mp

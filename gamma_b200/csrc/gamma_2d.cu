@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include "mlp.cuh"
 #include "step2d.cuh"
 
 using namespace gb;
@@ -216,9 +217,52 @@ __global__ void k_iface(Grid2 G, int stage) {
   FOR_LIVE_CELLS(G, j, i) iface_move(G, j, i, stage);
 }
 
-__global__ void __launch_bounds__(kThreads, GB2_MINB) k_update(Phys ph, Params2 P, Grid2 G, int stage, Stats2 *S) {
+// Learned cons2prim starting pressure for the 32 cells of a warp (BF16 tensor
+// cores, mlp.cuh).  The network sees |S| = sqrt(S_r^2 + (S_theta / r)^2), the
+// momentum magnitude cons2prim solves with; a non-finite or non-positive
+// guess keeps the warm start.
+struct LearnedStart {
+  const mlp::InferSmem *inf;
+  __device__ void operator()(const double *cons, double *prim, bool on, double r) const {
+    float f[3] = {0.f, 0.f, 0.f}, o[2] = {0.f, 0.f};
+    if (on) {
+      const double s1 = cons[SS1], s2 = cons[SS2] / r;
+      mlp::features(cons[DEN], cons[TAU], sqrt(s1 * s1 + s2 * s2), f);
+    }
+    __syncwarp();
+    mlp::infer_warp(*inf, f, o);
+    if (on) {
+      const double pg = mlp::guess_pressure(cons[DEN], o[0]);
+      if (isfinite(pg) && pg > 0.) prim[PPP] = pg;
+    }
+  }
+};
+
+// Grid::update + RK3 combines over the live cells.  With `guess` (device
+// parameters of the network), the loop runs warp-uniform so that every lane
+// takes part in the tensor-core inference; the weights are staged in shared
+// memory once per block.
+template <bool GUESS>
+__global__ void __launch_bounds__(kThreads, GB2_MINB)
+    k_update(Phys ph, Params2 P, Grid2 G, int stage, Stats2 *S, const float *guess) {
   unsigned long long c2p[4] = {0, 0, 0, 0};
-  FOR_LIVE_CELLS(G, j, i) update_cell(ph, P, G, j, i, stage, c2p);
+  if (!GUESS) {
+    FOR_LIVE_CELLS(G, j, i) update_cell(ph, P, G, j, i, stage, c2p, true, WarmStart{});
+  } else {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    mlp::InferSmem &inf = *reinterpret_cast<mlp::InferSmem *>(smem_raw);
+    mlp::load_infer_weights(guess, inf);
+    __syncthreads();
+    const LearnedStart ls{&inf};
+    const long long n = G.pref[G.NJ], stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+      const long long g = base + (threadIdx.x & 31);
+      int j = 0, i = 0;
+      const bool live = g < n;
+      if (live) cell_at(G, g, &j, &i);
+      update_cell(ph, P, G, j, i, stage, c2p, live, ls);
+    }
+  }
   add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3]);
 }
 
@@ -245,6 +289,7 @@ struct gamma_2d {
   std::vector<void *> allocs;
   Grid2 G{};
   Stats2 *d_stats = nullptr;
+  const float *guess = nullptr;  // learned cons2prim start (device parameters), or none
   int *d_flags = nullptr;  // [NJ] regrid flags
   std::vector<double> tg;  // host copy of the per-track factors
   std::string err;
@@ -359,7 +404,11 @@ int enqueue_step(gamma_2d *c) {
       k_dtfinal<<<1, kThreads, 0, s>>>(G, nb, c->cfg.cfl);
     }
     k_iface<<<nb, kThreads, 0, s>>>(G, stage);
-    k_update<<<nb, kThreads, 0, s>>>(ph, P, G, stage, c->d_stats);
+    if (c->guess) {
+      k_update<true><<<nb, kThreads, sizeof(mlp::InferSmem), s>>>(ph, P, G, stage, c->d_stats, c->guess);
+    } else {
+      k_update<false><<<nb, kThreads, 0, s>>>(ph, P, G, stage, c->d_stats, nullptr);
+    }
   }
   k_advance<<<1, 32, 0, s>>>(G, c->d_stats);
   G2_CUDA(c, cudaGetLastError());
@@ -504,15 +553,27 @@ GAMMA_API int gamma_2d_layout(const gamma_2d_t *ctx, int *ntracks, int *cap) {
   return GAMMA_OK;
 }
 
-GAMMA_API int gamma_2d_set_params(gamma_2d_t *ctx, const gamma_2d_params_t *params) {
-  if (!ctx || !params) return GAMMA_ERR_INVALID;
-  ctx->par = *params;
-  if (ctx->exec) {  // the graph holds the old values: capture again on the next step
+// the graph holds the launch arguments: capture again on the next step
+static void drop_graph(gamma_2d *ctx) {
+  if (ctx->exec) {
     cudaGraphExecDestroy(ctx->exec);
     cudaGraphDestroy(ctx->graph);
     ctx->exec = nullptr;
     ctx->graph = nullptr;
   }
+}
+
+GAMMA_API int gamma_2d_set_params(gamma_2d_t *ctx, const gamma_2d_params_t *params) {
+  if (!ctx || !params) return GAMMA_ERR_INVALID;
+  ctx->par = *params;
+  drop_graph(ctx);
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_2d_set_guess(gamma_2d_t *ctx, const float *params) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  ctx->guess = params;
+  drop_graph(ctx);
   return GAMMA_OK;
 }
 

@@ -55,9 +55,12 @@ constexpr double DT_INF = 1.e15;
 #endif
 
 // cartesian + rel_cart, ideal gas, no shock detection / synchrotron: NUM_Q = 6.
+#ifndef GB_CART_MIN_BLOCKS
+#define GB_CART_MIN_BLOCKS 5
+#endif
 struct CfgCart {
   static constexpr bool FAST = GB_FAST_ARITH;
-  static constexpr int MIN_BLOCKS = 4;  // 128-thread CTAs per SM: caps registers at 128
+  static constexpr int MIN_BLOCKS = GB_CART_MIN_BLOCKS;  // 128-thread CTAs per SM (5: 96 registers)
   static constexpr int NQ = 6;
   static constexpr bool SPH = false;    // rel_sph hydro and spherical1D geometry
   static constexpr bool SHOCK = false;  // SHOCK_DETECTION_
@@ -66,9 +69,12 @@ struct CfgCart {
 };
 
 // spherical1D + rel_sph + radiation_sph: NUM_Q = 10.
+#ifndef GB_SPH_MIN_BLOCKS
+#define GB_SPH_MIN_BLOCKS 3
+#endif
 struct CfgSph {
   static constexpr bool FAST = GB_FAST_ARITH;
-  static constexpr int MIN_BLOCKS = 1;
+  static constexpr int MIN_BLOCKS = GB_SPH_MIN_BLOCKS;
   static constexpr int NQ = 10;
   static constexpr bool SPH = true;
   static constexpr bool SHOCK = true;

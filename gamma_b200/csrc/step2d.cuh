@@ -617,77 +617,105 @@ GB_HD void iface_move(const Grid2 &G, int j, int i, int stage) {
 // cons2prim; at stage 3 the particle injection of every cell (run after
 // evolve by Simu::run).  Every cell copies this stage's grad_f1 into the
 // persistent one.
+// The starting pressure of cons2prim: the cell's previous pressure (the
+// reference's warm start).  A learned guess replaces it through `guess`, which
+// is called the same number of times (1 in stage 1, 2 after) by every lane of a
+// warp whether or not the lane's cell is updated (`upd`), so that it may work
+// across the warp; `r` is the radius cons2prim divides S_theta by.
+struct WarmStart {
+  GB_HD void operator()(const double *, double *, bool, double) const {}
+};
+
+// `live` = false: a lane without a cell (the learned guess' warp-uniform loop).
+template <class Guess>
 GB_HD void update_cell(const Phys &ph, const Params2 &P, const Grid2 &G, int j, int i, int stage,
-                       unsigned long long *c2p) {
-  const int n = G.ntrack[j];
-  if (i >= n) return;
+                       unsigned long long *c2p, bool live, const Guess &guess) {
+  const int n = live ? G.ntrack[j] : 0;
+  live = live && i < n;
   const long long g = (long long)j * G.cap + i;
   const int jL = jL_of(G), jR = jR_of(G);
   const int iL = iL_of(G), iR = n - G.ngst;
   const bool active_track = j > jL && j < jR;
-  double prim[NQ];
-  load_prim(G, g, prim);
-  if (active_track) {
-    const double dt = *G.dt;
-    if (i >= iL + 1 && i <= iR - 1) {
-      const Geom G0 = cell_geom(G, j, g);
-      double cons[NQ];
-      prim2cons(ph, prim, cons, G0.r);
-      if (stage == 1) {
+  const bool upd = live && active_track && i >= iL + 1 && i <= iR - 1;
+  double prim[NQ], cons[NQ];
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) G.cons0[q * G.NC + g] = cons[q];
-        G.dV0[g] = G0.dV;
-      }
+  for (int q = 0; q < NQ; ++q) prim[q] = cons[q] = 0.;
+  if (live) load_prim(G, g, prim);
+  double dt = 0., r1 = 1., r2 = 1., xn = 0., dxn = 0., dV1 = 0.;
+  TrackGeo tj{};
+  if (upd) {
+    dt = *G.dt;
+    const Geom G0 = cell_geom(G, j, g);
+    prim2cons(ph, prim, cons, G0.r);
+    if (stage == 1) {
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) cons[q] *= G0.dV;
+      for (int q = 0; q < NQ; ++q) G.cons0[q * G.NC + g] = cons[q];
+      G.dV0[g] = G0.dV;
+    }
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) cons[q] += (G.flx[q * G.NC + g - 1] - G.flx[q * G.NC + g]) * dt;
+    for (int q = 0; q < NQ; ++q) cons[q] *= G0.dV;
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) cons[q] += (G.f1lo[q * G.NC + g] - G.f1hi[q * G.NC + g]) * dt;
-      const TrackGeo tj = tgeo(G, j);
-      source_terms(ph, prim, G0, tj, dt, cons);
-      {  // Cell::radiativeSourceTerms
-        const SynchConst sc{P.Nalpha, P.Nmp, P.Nme};
-        const double dg = radiative_source<Cfg2>(ph, sc, prim, G0.dV, dt);
-        cons[GMX] += dg;
-        cons[GMN] += dg;
-      }
-      const double xL = G.xIm[g - 1], xR = G.xIm[g];
-      const Geom G1 = make_geom((xR + xL) / 2., (xR - xL), tj);
+    for (int q = 0; q < NQ; ++q) cons[q] += (G.flx[q * G.NC + g - 1] - G.flx[q * G.NC + g]) * dt;
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) cons[q] /= G1.dV;
-      C2PStats cs;
-      cons2prim(ph, cons, prim, G1.cen_r, &cs);
+    for (int q = 0; q < NQ; ++q) cons[q] += (G.f1lo[q * G.NC + g] - G.f1hi[q * G.NC + g]) * dt;
+    tj = tgeo(G, j);
+    source_terms(ph, prim, G0, tj, dt, cons);
+    {  // Cell::radiativeSourceTerms
+      const SynchConst sc{P.Nalpha, P.Nmp, P.Nme};
+      const double dg = radiative_source<Cfg2>(ph, sc, prim, G0.dV, dt);
+      cons[GMX] += dg;
+      cons[GMN] += dg;
+    }
+    const double xL = G.xIm[g - 1], xR = G.xIm[g];
+    const Geom G1 = make_geom((xR + xL) / 2., (xR - xL), tj);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) cons[q] /= G1.dV;
+    r1 = G1.cen_r;
+    dV1 = G1.dV;
+    xn = G1.r;
+    dxn = G1.dr;
+  }
+  guess(cons, prim, upd, r1);
+  C2PStats cs;
+  if (upd) {
+    cons2prim(ph, cons, prim, r1, &cs);
+    c2p[0] += 1;
+    c2p[1] += cs.iters;
+    c2p[2] += cs.fallback;
+    if ((unsigned long long)cs.iters > c2p[3]) c2p[3] = cs.iters;
+  }
+  if (stage > 1) {
+    if (upd) {
+      const double w0 = stage == 2 ? 3. / 4. : 1. / 3.;
+      const double w1 = stage == 2 ? 1. / 4. : 2. / 3.;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) cons[q] = w0 * G.cons0[q * G.NC + g] * G.dV0[g] + w1 * cons[q] * dV1;
+      const double cL = G.xI[g - 1], cR = G.xI[g];  // combined positions
+      const Geom G2 = make_geom((cR + cL) / 2., (cR - cL), tj);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) cons[q] /= G2.dV;
+      r2 = G2.r;
+      xn = G2.r;
+      dxn = G2.dr;
+    }
+    guess(cons, prim, upd, r2);
+    if (upd) {
+      cons2prim(ph, cons, prim, r2, &cs);
       c2p[0] += 1;
       c2p[1] += cs.iters;
       c2p[2] += cs.fallback;
       if ((unsigned long long)cs.iters > c2p[3]) c2p[3] = cs.iters;
-      double xn = G1.r, dxn = G1.dr;
-      if (stage > 1) {
-        const double w0 = stage == 2 ? 3. / 4. : 1. / 3.;
-        const double w1 = stage == 2 ? 1. / 4. : 2. / 3.;
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) cons[q] = w0 * G.cons0[q * G.NC + g] * G.dV0[g] + w1 * cons[q] * G1.dV;
-        const double cL = G.xI[g - 1], cR = G.xI[g];  // combined positions
-        const Geom G2 = make_geom((cR + cL) / 2., (cR - cL), tj);
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) cons[q] /= G2.dV;
-        cons2prim(ph, cons, prim, G2.r, &cs);
-        c2p[0] += 1;
-        c2p[1] += cs.iters;
-        c2p[2] += cs.fallback;
-        if ((unsigned long long)cs.iters > c2p[3]) c2p[3] = cs.iters;
-        xn = G2.r;
-        dxn = G2.dr;
-      }
-      G.x[g] = xn;
-      G.dx[g] = dxn;
-    } else if (stage > 1 && i >= 1 && i <= n - 2) {
-      // CellGeomFromInterfacePos also moves the ghost cells 1 and ntrack-2
-      const double cL = G.xI[g - 1], cR = G.xI[g];
-      G.x[g] = (cR + cL) / 2.;
-      G.dx[g] = (cR - cL);
     }
+  }
+  if (!live) return;
+  if (upd) {
+    G.x[g] = xn;
+    G.dx[g] = dxn;
+  } else if (active_track && stage > 1 && i >= 1 && i <= n - 2) {
+    // CellGeomFromInterfacePos also moves the ghost cells 1 and ntrack-2
+    const double cL = G.xI[g - 1], cR = G.xI[g];
+    G.x[g] = (cR + cL) / 2.;
+    G.dx[g] = (cR - cL);
   }
   if (stage == 3) {
     const SynchConst sc{P.Nalpha, P.Nmp, P.Nme};

@@ -75,6 +75,7 @@ def lib() -> ctypes.CDLL:
         L.gamma_2d_create.argtypes = [ctypes.POINTER(Config2D), v, v, ctypes.POINTER(ctypes.c_void_p)]
         L.gamma_2d_layout.argtypes = [v, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.gamma_2d_set_params.argtypes = [v, ctypes.POINTER(Params2D)]
+        L.gamma_2d_set_guess.argtypes = [v, v]
         L.gamma_2d_upload.argtypes = [v] + [v] * 9 + [ctypes.c_double, ctypes.c_longlong, ctypes.c_int]
         L.gamma_2d_step.argtypes = [v, ctypes.c_int, ctypes.POINTER(gpu.StepStats)]
         L.gamma_2d_download.argtypes = [v] * 17
@@ -85,8 +86,9 @@ def lib() -> ctypes.CDLL:
         L.gamma_2d_last_error.argtypes = [v]
         L.gamma_2d_last_error.restype = ctypes.c_char_p
         L.gamma_2d_destroy.argtypes = [v]
-        for name in ("gamma_2d_create", "gamma_2d_layout", "gamma_2d_set_params", "gamma_2d_upload", "gamma_2d_step",
-                     "gamma_2d_download", "gamma_2d_prepare", "gamma_2d_download_fluxes"):
+        for name in ("gamma_2d_create", "gamma_2d_layout", "gamma_2d_set_params", "gamma_2d_set_guess",
+                     "gamma_2d_upload", "gamma_2d_step", "gamma_2d_download", "gamma_2d_prepare",
+                     "gamma_2d_download_fluxes"):
             getattr(L, name).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -137,6 +139,11 @@ class Grid2DGPU:
     def set_params(self, p: Params2D):
         self._check(lib().gamma_2d_set_params(self.h, ctypes.byref(p)))
 
+    def set_guess(self, params_ptr: int):
+        """Learned cons2prim starting pressure in every cell update (device
+        parameter pointer), or 0 for the warm start of the reference."""
+        self._check(lib().gamma_2d_set_guess(self.h, ctypes.c_void_p(params_ptr) if params_ptr else None))
+
     def upload(self, s: State2D, run_ghosts: bool = False):
         assert s.NJ == self.NJ and s.cap == self.cap
         c = lambda a, dt: None if a is None else np.ascontiguousarray(a, dtype=dt)
@@ -184,6 +191,7 @@ class Grid2DGPU:
         return s
 
 
-EXPORTS = ("gamma_2d_create", "gamma_2d_layout", "gamma_2d_set_params", "gamma_2d_upload", "gamma_2d_step",
+EXPORTS = ("gamma_2d_create", "gamma_2d_layout", "gamma_2d_set_params", "gamma_2d_set_guess", "gamma_2d_upload",
+           "gamma_2d_step",
            "gamma_2d_download", "gamma_2d_prepare", "gamma_2d_download_fluxes", "gamma_2d_stream",
            "gamma_2d_last_error", "gamma_2d_destroy")

@@ -258,6 +258,15 @@ int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta, const dou
 int gamma_2d_layout(const gamma_2d_t *ctx, int *ntracks, int *cap);
 int gamma_2d_set_params(gamma_2d_t *ctx, const gamma_2d_params_t *params);
 
+/* Learned cons2prim starting pressure in every cell update of the step (device
+ * pointer to gamma_mlp_param_count() floats, trained with gamma_mlp_train), or
+ * NULL for the reference's warm start (the cell's previous pressure).  Replaces
+ * the starting point of FluidState::cons2prim (src/Hydro/rel_sph.cpp:213-320)
+ * called from Cell::update and the RK3 combines (src/Timestep/rk3.cpp); the
+ * root and its stopping rule are unchanged.  The pointer must stay valid while
+ * steps run. */
+int gamma_2d_set_guess(gamma_2d_t *ctx, const float *params);
+
 /* Host -> device state.  grad_mv, grad_f1, nbr and dt_loc may be NULL (a new
  * grid: zero gradients, empty lists, dt_loc = 1e15).  run_ghosts = 1 runs the
  * updateGhosts that precedes Simu::run's loop (simu.cpp:74). */
