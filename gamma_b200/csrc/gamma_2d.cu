@@ -14,6 +14,9 @@
 #include <string>
 #include <vector>
 
+#include <cstring>
+
+#include "io.h"
 #include "mlp.cuh"
 #include "step2d.cuh"
 
@@ -266,6 +269,13 @@ __global__ void __launch_bounds__(kThreads, GB2_MINB)
   add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3]);
 }
 
+// Grid::printCols' side effect with shock detection (text2d.cpp:147-153):
+// slot TR1+1 of every cell of every track takes Sd.
+__global__ void k_mark_sd(Grid2 G) {
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < G.NC; g += (long long)gridDim.x * blockDim.x)
+    if ((int)(g % G.cap) < G.ntrack[g / G.cap]) G.prim[(TR1 + 1) * G.NC + g] = G.sd[g];
+}
+
 __global__ void k_advance(Grid2 G, Stats2 *S) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   *G.t += *G.dt;
@@ -292,6 +302,7 @@ struct gamma_2d {
   const float *guess = nullptr;  // learned cons2prim start (device parameters), or none
   int *d_flags = nullptr;  // [NJ] regrid flags
   std::vector<double> tg;  // host copy of the per-track factors
+  std::vector<double> theta, dtheta;  // of the active tracks, as given at creation
   std::string err;
 };
 
@@ -439,6 +450,8 @@ GAMMA_API int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta,
   if ((long long)(cfg->ntheta + 2 * cfg->ngst) * (cfg->nmax + 2 * cfg->ngst) >= (1LL << 31)) return GAMMA_ERR_INVALID;
   gamma_2d *c = new gamma_2d();
   c->cfg = *cfg;
+  c->theta.assign(theta, theta + cfg->ntheta);
+  c->dtheta.assign(dtheta, dtheta + cfg->ntheta);
   const int ng = cfg->ngst;
   c->NJ = cfg->ntheta + 2 * ng;
   c->cap = cfg->nmax + 2 * ng;
@@ -725,6 +738,109 @@ GAMMA_API int gamma_2d_download_fluxes(gamma_2d_t *ctx, double *v, double *lL, d
 GAMMA_API void *gamma_2d_stream(gamma_2d_t *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 GAMMA_API const char *gamma_2d_last_error(const gamma_2d_t *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+GAMMA_API int gamma_2d_print_cols(gamma_2d_t *ctx, const char *dir) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  gamma_2d *c = ctx;
+  k_mark_sd<<<ghost_blocks(c, true), kThreads, 0, c->stream>>>(c->G);
+  G2_CUDA(c, cudaGetLastError());
+  const size_t NC = (size_t)c->NC;
+  std::vector<int> nt(c->NJ);
+  std::vector<double> prim(NQ * NC), x(NC), dx(NC);
+  double t = 0.;
+  long long it = 0;
+  int rc = gamma_2d_download(c, nt.data(), &t, nullptr, &it, nullptr, prim.data(), x.data(), dx.data(), nullptr,
+                             nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+  if (rc != GAMMA_OK) return rc;
+  const std::string path = gb::io::phys_name(dir, it);
+  return gb::io::write_text2d(path.c_str(), c->cfg, c->NJ, c->cap, nt.data(), c->theta.data(), c->dtheta.data(), it,
+                              t, prim.data(), x.data(), dx.data());
+}
+
+// Checkpoint: configuration, tracks, parameters, then every array that carries
+// state from one step to the next -- including the gradients and the
+// neighbour lists that the ghost cells keep from earlier stages.
+GAMMA_API int gamma_2d_save(gamma_2d_t *ctx, const char *path) {
+  if (!ctx || !path) return GAMMA_ERR_INVALID;
+  gamma_2d *c = ctx;
+  const size_t NC = (size_t)c->NC, d = sizeof(double);
+  std::vector<int> nt(c->NJ), nbr(4 * NC);
+  std::vector<double> prim(NQ * NC), x(NC), dx(NC), dtl(NC), xI(NC), gmv(NQ * NC), gf1(NQ * NC), sd(NC), ps(NC);
+  std::vector<unsigned char> sh(NC);
+  double sc[2] = {0., 0.};  // t, dt
+  long long it = 0;
+  int rc = gamma_2d_download(c, nt.data(), &sc[0], &sc[1], &it, nullptr, prim.data(), x.data(), dx.data(),
+                             dtl.data(), xI.data(), gmv.data(), gf1.data(), nbr.data(), sd.data(), ps.data(),
+                             sh.data());
+  if (rc != GAMMA_OK) return rc;
+  gb::io::CkptOut out(path);
+  if (!out.ok()) return GAMMA_ERR_IO;
+  const uint32_t kind = gb::io::kCkpt2D;
+  out.block("kind", &kind, sizeof(kind));
+  out.block("config", &c->cfg, sizeof(c->cfg));
+  out.block("theta", c->theta.data(), c->theta.size() * d);
+  out.block("dtheta", c->dtheta.data(), c->dtheta.size() * d);
+  out.block("params", &c->par, sizeof(c->par));
+  out.block("t_dt", sc, sizeof(sc));
+  out.block("it", &it, sizeof(it));
+  out.block("ntrack", nt.data(), nt.size() * sizeof(int));
+  out.block("prim", prim.data(), prim.size() * d);
+  out.block("x", x.data(), NC * d);
+  out.block("dx", dx.data(), NC * d);
+  out.block("dt_loc", dtl.data(), NC * d);
+  out.block("xI", xI.data(), NC * d);
+  out.block("grad_mv", gmv.data(), gmv.size() * d);
+  out.block("grad_f1", gf1.data(), gf1.size() * d);
+  out.block("nbr", nbr.data(), nbr.size() * sizeof(int));
+  out.block("sd", sd.data(), NC * d);
+  out.block("pspec", ps.data(), NC * d);
+  out.block("shocked", sh.data(), NC);
+  return out.close();
+}
+
+GAMMA_API int gamma_2d_load(gamma_2d_t *ctx, const char *path) {
+  if (!ctx || !path) return GAMMA_ERR_INVALID;
+  gamma_2d *c = ctx;
+  const size_t NC = (size_t)c->NC, d = sizeof(double);
+  gb::io::CkptIn in(path);
+  if (!in.ok()) return GAMMA_ERR_IO;
+  uint32_t kind = 0;
+  gamma_2d_config_t cfg;
+  if (!in.block("kind", &kind, sizeof(kind)) || kind != gb::io::kCkpt2D) return GAMMA_ERR_IO;
+  if (!in.block("config", &cfg, sizeof(cfg)) || std::memcmp(&cfg, &c->cfg, sizeof(cfg)) != 0)
+    return GAMMA_ERR_INVALID;
+  std::vector<double> th(c->theta.size()), dth(c->dtheta.size());
+  if (!in.block("theta", th.data(), th.size() * d) || !in.block("dtheta", dth.data(), dth.size() * d) ||
+      th != c->theta || dth != c->dtheta)
+    return GAMMA_ERR_INVALID;
+  gamma_2d_params_t par;
+  double sc[2];
+  long long it = 0;
+  std::vector<int> nt(c->NJ), nbr(4 * NC);
+  std::vector<double> prim(NQ * NC), x(NC), dx(NC), dtl(NC), xI(NC), gmv(NQ * NC), gf1(NQ * NC), sd(NC), ps(NC);
+  std::vector<unsigned char> sh(NC);
+  const bool ok = in.block("params", &par, sizeof(par)) && in.block("t_dt", sc, sizeof(sc)) &&
+                  in.block("it", &it, sizeof(it)) && in.block("ntrack", nt.data(), nt.size() * sizeof(int)) &&
+                  in.block("prim", prim.data(), prim.size() * d) && in.block("x", x.data(), NC * d) &&
+                  in.block("dx", dx.data(), NC * d) && in.block("dt_loc", dtl.data(), NC * d) &&
+                  in.block("xI", xI.data(), NC * d) && in.block("grad_mv", gmv.data(), gmv.size() * d) &&
+                  in.block("grad_f1", gf1.data(), gf1.size() * d) &&
+                  in.block("nbr", nbr.data(), nbr.size() * sizeof(int)) && in.block("sd", sd.data(), NC * d) &&
+                  in.block("pspec", ps.data(), NC * d) && in.block("shocked", sh.data(), NC);
+  if (!ok) return GAMMA_ERR_IO;
+  int rc = gamma_2d_set_params(c, &par);
+  if (rc == GAMMA_OK)
+    rc = gamma_2d_upload(c, nt.data(), prim.data(), x.data(), dx.data(), dtl.data(), xI.data(), gmv.data(),
+                         gf1.data(), nbr.data(), sc[0], it, 0);
+  if (rc != GAMMA_OK) return rc;
+  const Grid2 &G = c->G;
+  G2_CUDA(c, cudaMemcpyAsync(G.sd, sd.data(), NC * d, cudaMemcpyHostToDevice, c->stream));
+  G2_CUDA(c, cudaMemcpyAsync(G.pspec, ps.data(), NC * d, cudaMemcpyHostToDevice, c->stream));
+  G2_CUDA(c, cudaMemcpyAsync(G.shocked, sh.data(), NC, cudaMemcpyHostToDevice, c->stream));
+  G2_CUDA(c, cudaMemcpyAsync(G.dt, &sc[1], d, cudaMemcpyHostToDevice, c->stream));
+  G2_CUDA(c, cudaStreamSynchronize(c->stream));
+  return GAMMA_OK;
+}
 
 GAMMA_API void gamma_2d_destroy(gamma_2d_t *ctx) {
   if (!ctx) return;

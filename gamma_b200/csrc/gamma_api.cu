@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "io.h"
 #include "track_step.cuh"
 
 namespace {
@@ -139,6 +140,15 @@ __global__ void cons2prim_kernel(gb::Phys ph, double *cons, double *prim, int n,
     }
     if (iters) iters[k] = st.iters;
   }
+}
+
+// Grid::printCols' side effect with shock detection (text1d.cpp:135-141):
+// slot TR1+1 (stored row 4) of every cell of run r takes isShocked.
+__global__ void mark_shocked_kernel(gb::Tracks T, int r) {
+  const long long o = T.off[r];
+  const int n = T.run[r].ntrack;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    T.prim[(size_t)(gb::TR1 + 1 - 1) * T.N + o + i] = (double)T.shocked[o + i];
 }
 
 }  // namespace
@@ -442,6 +452,125 @@ GAMMA_API int gamma_gpu_cons2prim(const gamma_config_t *cfg, double *cons, doubl
   else
     cons2prim_kernel<gb::CfgCart><<<grid, bs, 0, s>>>(phys_of(*cfg), cons, prim, n, iters);
   if (cudaGetLastError() != cudaSuccess) return GAMMA_ERR_CUDA;
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_gpu_print_cols(gamma_ctx_t *ctx, int run, const char *dir) {
+  if (!ctx || run < 0 || run >= ctx->nruns) return GAMMA_ERR_INVALID;
+  const gb::Tracks &T = ctx->T;
+  if (ctx->cfg.shock_detection) {
+    mark_shocked_kernel<<<4, 256, 0, ctx->stream>>>(T, run);
+    GB_CUDA(ctx, cudaGetLastError());
+  }
+  gb::RunState rs;
+  GB_CUDA(ctx, cudaMemcpyAsync(&rs, T.run + run, sizeof(rs), cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const int n = rs.ntrack;
+  const long long o = ctx->off[run];
+  std::vector<double> prim((size_t)ctx->nq * n, 0.), x(n), dx(n);
+  for (int s = 0; s < ctx->nqs; ++s) {
+    const int q = s < 3 ? s : s + 1;
+    GB_CUDA(ctx, cudaMemcpyAsync(prim.data() + (size_t)q * n, T.prim + (size_t)s * ctx->N + o, n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  GB_CUDA(ctx, cudaMemcpyAsync(x.data(), T.x + o, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(ctx, cudaMemcpyAsync(dx.data(), T.dx + o, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const std::string path = gb::io::phys_name(dir, rs.it);
+  return gb::io::write_text1d(path.c_str(), ctx->cfg, n, rs.it, rs.t, prim.data(), n, x.data(), dx.data());
+}
+
+// Checkpoint blocks: config, layout, parameters, run scalars, then every array
+// that carries state from one step to the next (the shock fields too, which a
+// dump right after a load reads).
+GAMMA_API int gamma_gpu_save(gamma_ctx_t *ctx, const char *path) {
+  if (!ctx || !path) return GAMMA_ERR_INVALID;
+  const gb::Tracks &T = ctx->T;
+  const int R = ctx->nruns;
+  const size_t N = (size_t)ctx->N, d = sizeof(double);
+  std::vector<gb::RunState> rs(R);
+  std::vector<gb::RunParams> par(R);
+  std::vector<double> buf((size_t)ctx->nqs * N);
+  std::vector<unsigned char> sh(N);
+  gb::io::CkptOut out(path);
+  if (!out.ok()) return GAMMA_ERR_IO;
+  const uint32_t kind = gb::io::kCkpt1D;
+  out.block("kind", &kind, sizeof(kind));
+  out.block("config", &ctx->cfg, sizeof(ctx->cfg));
+  out.block("capacity", ctx->cap.data(), R * sizeof(int));
+  GB_CUDA(ctx, cudaMemcpyAsync(rs.data(), T.run, R * sizeof(gb::RunState), cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(ctx, cudaMemcpyAsync(par.data(), T.par, R * sizeof(gb::RunParams), cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  out.block("runs", rs.data(), R * sizeof(gb::RunState));
+  out.block("params", par.data(), R * sizeof(gb::RunParams));
+  auto arr = [&](const char *name, const void *src, size_t bytes) -> int {
+    GB_CUDA(ctx, cudaMemcpyAsync(buf.data(), src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    out.block(name, buf.data(), bytes);
+    return GAMMA_OK;
+  };
+  int rc;
+  if ((rc = arr("prim", T.prim, ctx->nqs * N * d)) != GAMMA_OK) return rc;
+  if ((rc = arr("x", T.x, N * d)) != GAMMA_OK) return rc;
+  if ((rc = arr("dx", T.dx, N * d)) != GAMMA_OK) return rc;
+  if ((rc = arr("dt_loc", T.dtl, N * d)) != GAMMA_OK) return rc;
+  if ((rc = arr("xI", T.xI, N * d)) != GAMMA_OK) return rc;
+  if (T.sd) {
+    if ((rc = arr("sd", T.sd, N * d)) != GAMMA_OK) return rc;
+    if ((rc = arr("pspec", T.pspec, N * d)) != GAMMA_OK) return rc;
+    GB_CUDA(ctx, cudaMemcpyAsync(sh.data(), T.shocked, N, cudaMemcpyDeviceToHost, ctx->stream));
+    GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    out.block("shocked", sh.data(), N);
+  }
+  return out.close();
+}
+
+GAMMA_API int gamma_gpu_load(gamma_ctx_t *ctx, const char *path) {
+  if (!ctx || !path) return GAMMA_ERR_INVALID;
+  const gb::Tracks &T = ctx->T;
+  const int R = ctx->nruns;
+  const size_t N = (size_t)ctx->N, d = sizeof(double);
+  gb::io::CkptIn in(path);
+  if (!in.ok()) return GAMMA_ERR_IO;
+  uint32_t kind = 0;
+  gamma_config_t cfg;
+  std::vector<int> cap(R);
+  if (!in.block("kind", &kind, sizeof(kind)) || kind != gb::io::kCkpt1D) return GAMMA_ERR_IO;
+  if (!in.block("config", &cfg, sizeof(cfg)) || std::memcmp(&cfg, &ctx->cfg, sizeof(cfg)) != 0)
+    return GAMMA_ERR_INVALID;
+  if (!in.block("capacity", cap.data(), R * sizeof(int)) || cap != ctx->cap) return GAMMA_ERR_INVALID;
+  std::vector<gb::RunState> rs(R);
+  std::vector<gb::RunParams> par(R);
+  if (!in.block("runs", rs.data(), R * sizeof(gb::RunState))) return GAMMA_ERR_IO;
+  if (!in.block("params", par.data(), R * sizeof(gb::RunParams))) return GAMMA_ERR_IO;
+  std::vector<double> buf((size_t)ctx->nqs * N);
+  std::vector<unsigned char> sh(N);
+  auto arr = [&](const char *name, void *dst, size_t bytes) -> int {
+    if (!in.block(name, buf.data(), bytes)) return GAMMA_ERR_IO;
+    GB_CUDA(ctx, cudaMemcpyAsync(dst, buf.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+    GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GAMMA_OK;
+  };
+  int rc;
+  if ((rc = arr("prim", T.prim, ctx->nqs * N * d)) != GAMMA_OK) return rc;
+  if ((rc = arr("x", T.x, N * d)) != GAMMA_OK) return rc;
+  if ((rc = arr("dx", T.dx, N * d)) != GAMMA_OK) return rc;
+  if ((rc = arr("dt_loc", T.dtl, N * d)) != GAMMA_OK) return rc;
+  if ((rc = arr("xI", T.xI, N * d)) != GAMMA_OK) return rc;
+  if (T.sd) {
+    if ((rc = arr("sd", T.sd, N * d)) != GAMMA_OK) return rc;
+    if ((rc = arr("pspec", T.pspec, N * d)) != GAMMA_OK) return rc;
+    if (!in.block("shocked", sh.data(), N)) return GAMMA_ERR_IO;
+    GB_CUDA(ctx, cudaMemcpyAsync(T.shocked, sh.data(), N, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  std::vector<int> order(R);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rs[a].ntrack > rs[b].ntrack; });
+  GB_CUDA(ctx, cudaMemcpyAsync(T.run, rs.data(), R * sizeof(gb::RunState), cudaMemcpyHostToDevice, ctx->stream));
+  GB_CUDA(ctx, cudaMemcpyAsync((void *)T.par, par.data(), R * sizeof(gb::RunParams), cudaMemcpyHostToDevice,
+                               ctx->stream));
+  GB_CUDA(ctx, cudaMemcpyAsync(ctx->d_order, order.data(), R * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return GAMMA_OK;
 }
 

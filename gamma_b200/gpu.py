@@ -35,6 +35,7 @@ EXPORTS = (
     "gamma_mlp_param_count", "gamma_mlp_init", "gamma_mlp_pairs", "gamma_mlp_train", "gamma_mlp_forward",
     "gamma_mlp_loss_grad",
     "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess",
+    "gamma_text1d_write", "gamma_text1d_read", "gamma_gpu_print_cols", "gamma_gpu_save", "gamma_gpu_load",
 )
 
 
@@ -131,10 +132,19 @@ def lib() -> ctypes.CDLL:
         L.gamma_mlp_loss_grad.argtypes = [v, v, v, ctypes.c_int, v, v, v]
         L.gamma_gpu_cons2prim_guess.argtypes = [ctypes.POINTER(Config), v, v, ctypes.c_int, v, v, v]
         L.gamma_gpu_set_guess.argtypes = [v, v]
+        L.gamma_text1d_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config), ctypes.c_int, ctypes.c_longlong,
+                                         ctypes.c_double, _dp, ctypes.c_longlong, _dp, _dp]
+        L.gamma_text1d_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config), ctypes.c_int, _ip, _lp, _dp,
+                                        _dp, _dp, _dp, _dp]
+        L.gamma_gpu_print_cols.argtypes = [v, ctypes.c_int, ctypes.c_char_p]
+        L.gamma_gpu_save.argtypes = [v, ctypes.c_char_p]
+        L.gamma_gpu_load.argtypes = [v, ctypes.c_char_p]
         for name in ("gamma_gpu_create", "gamma_gpu_layout", "gamma_gpu_set_params", "gamma_gpu_upload",
                      "gamma_gpu_step", "gamma_gpu_regrid", "gamma_gpu_download", "gamma_gpu_cons2prim",
                      "gamma_mlp_param_count", "gamma_mlp_init", "gamma_mlp_pairs", "gamma_mlp_train",
-                     "gamma_mlp_forward", "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess", "gamma_mlp_loss_grad"):
+                     "gamma_mlp_forward", "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess", "gamma_mlp_loss_grad",
+                     "gamma_text1d_write", "gamma_text1d_read", "gamma_gpu_print_cols", "gamma_gpu_save",
+                     "gamma_gpu_load"):
             getattr(L, name).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -232,6 +242,22 @@ class GammaGPU:
             _p(out["prim"]), _p(out["x"]), _p(out["dx"]), _p(out["dt_loc"]), _p(out["xI"])))
         return out
 
+    def print_cols(self, run: int, directory: str) -> str:
+        """Grid::printCols of one run: marks isShocked into slot TR1+1 on the
+        device (as the reference does), writes <directory>/phys%010d.out and
+        returns that path."""
+        self._check(lib().gamma_gpu_print_cols(self.h, int(run), directory.encode()))
+        it = int(self.download()["it"][run])
+        return os.path.join(directory, f"phys{it:010d}.out")
+
+    def save(self, path: str):
+        """Exact checkpoint of every run."""
+        self._check(lib().gamma_gpu_save(self.h, path.encode()))
+
+    def load(self, path: str):
+        """Restore a checkpoint made by a context of the same configuration and capacities."""
+        self._check(lib().gamma_gpu_load(self.h, path.encode()))
+
     def download_ptrs(self, prim_ptr, x_ptr=None, dx_ptr=None, dtl_ptr=None, xI_ptr=None):
         R = self.nruns
         nt = np.zeros(R, np.int32)
@@ -239,6 +265,30 @@ class GammaGPU:
         self._check(lib().gamma_gpu_download(self.h, _p(nt, _ip), None, None, None, None, c(prim_ptr), c(x_ptr),
                                              c(dx_ptr), c(dtl_ptr), c(xI_ptr)))
         return nt
+
+
+def text1d_write(path: str, cfg: Config, prim, x, dx, it: int, t: float):
+    """Grid::printCols columns of one run from host arrays: prim [nq][ntrack]
+    (slot TR1+1 already holding what the reference stores there), x, dx."""
+    prim = np.ascontiguousarray(prim, dtype=np.float64)
+    n = prim.shape[1]
+    _ok(lib().gamma_text1d_write(path.encode(), ctypes.byref(cfg), int(n), int(it), float(t), _p(prim), int(n),
+                                 _p(np.ascontiguousarray(x, dtype=np.float64)),
+                                 _p(np.ascontiguousarray(dx, dtype=np.float64))))
+
+
+def text1d_read(path: str, cfg: Config, cap: int) -> dict:
+    """Simu::reinitialise of the 1D build without the problem hooks: the state
+    reloadFromData + mpi_distribute + prepForRun leave ([nq][cap] arrays;
+    ghost cells still to be filled by the problem's updateGhosts)."""
+    prim = np.zeros((cfg.nq, cap))
+    x, dx, xI = np.zeros(cap), np.zeros(cap), np.zeros(cap)
+    n = ctypes.c_int()
+    it = ctypes.c_longlong()
+    t = ctypes.c_double()
+    _ok(lib().gamma_text1d_read(path.encode(), ctypes.byref(cfg), int(cap), ctypes.byref(n), ctypes.byref(it),
+                                ctypes.byref(t), _p(prim), _p(x), _p(dx), _p(xI)))
+    return dict(ntrack=int(n.value), it=int(it.value), t=float(t.value), prim=prim, x=x, dx=dx, xI=xI)
 
 
 def cons2prim_device(cfg: Config, cons_ptr: int, prim_ptr: int, n: int, iters_ptr: int = 0, stream: int = 0):

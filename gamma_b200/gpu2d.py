@@ -76,6 +76,12 @@ def lib() -> ctypes.CDLL:
         L.gamma_2d_layout.argtypes = [v, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.gamma_2d_set_params.argtypes = [v, ctypes.POINTER(Params2D)]
         L.gamma_2d_set_guess.argtypes = [v, v]
+        L.gamma_2d_print_cols.argtypes = [v, ctypes.c_char_p]
+        L.gamma_2d_save.argtypes = [v, ctypes.c_char_p]
+        L.gamma_2d_load.argtypes = [v, ctypes.c_char_p]
+        L.gamma_text2d_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config2D), v, v, v, ctypes.c_longlong,
+                                         ctypes.c_double, v, v, v]
+        L.gamma_text2d_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config2D), v, v, v, v, v, v, v, v, v]
         L.gamma_2d_upload.argtypes = [v] + [v] * 9 + [ctypes.c_double, ctypes.c_longlong, ctypes.c_int]
         L.gamma_2d_step.argtypes = [v, ctypes.c_int, ctypes.POINTER(gpu.StepStats)]
         L.gamma_2d_download.argtypes = [v] * 17
@@ -88,7 +94,8 @@ def lib() -> ctypes.CDLL:
         L.gamma_2d_destroy.argtypes = [v]
         for name in ("gamma_2d_create", "gamma_2d_layout", "gamma_2d_set_params", "gamma_2d_set_guess",
                      "gamma_2d_upload", "gamma_2d_step", "gamma_2d_download", "gamma_2d_prepare",
-                     "gamma_2d_download_fluxes"):
+                     "gamma_2d_download_fluxes", "gamma_2d_print_cols", "gamma_2d_save", "gamma_2d_load",
+                     "gamma_text2d_write", "gamma_text2d_read"):
             getattr(L, name).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -171,6 +178,23 @@ class Grid2DGPU:
                                                              ("v", "lL", "lR", "flux", "f1lo", "f1hi", "grad_f1")]))
         return out
 
+    def print_cols(self, directory: str) -> str:
+        """Grid::printCols of the 2D build: Sd into slot TR1+1 of every cell
+        on the device (as the reference does), then <directory>/phys%010d.out;
+        returns that path."""
+        self._check(lib().gamma_2d_print_cols(self.h, directory.encode()))
+        it = ctypes.c_longlong()
+        self._check(lib().gamma_2d_download(self.h, *([None] * 3), ctypes.byref(it), *([None] * 12)))
+        return f"{directory.rstrip('/')}/phys{it.value:010d}.out"
+
+    def save(self, path: str):
+        """Exact checkpoint (state, gradients, neighbour lists, dt_loc, t, it)."""
+        self._check(lib().gamma_2d_save(self.h, path.encode()))
+
+    def load(self, path: str):
+        """Restore a checkpoint made with the same configuration and tracks."""
+        self._check(lib().gamma_2d_load(self.h, path.encode()))
+
     def download(self) -> State2D:
         NC = self.NC
         nt = np.zeros(self.NJ, np.int32)
@@ -191,7 +215,39 @@ class Grid2DGPU:
         return s
 
 
+def _config(ntheta, nmax, gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=gpu.EOS_IDEAL) -> Config2D:
+    return Config2D(int(ntheta), int(nmax), 2, NQ, int(eos), float(gamma_ad), float(cfl), float(vi))
+
+
+def text2d_write(path: str, s: State2D, theta, dtheta, **cfg):
+    """Grid::printCols columns of the 2D build from a host state whose slot
+    TR1+1 already holds Sd; theta/dtheta of the active tracks."""
+    c = _config(s.NJ - 4, s.cap - 4, **cfg)
+    arr = lambda a, dt: np.ascontiguousarray(a, dtype=dt)
+    keep = [arr(s.ntrack, np.int32), arr(theta, np.float64), arr(dtheta, np.float64), arr(s.prim, np.float64),
+            arr(s.x, np.float64), arr(s.dx, np.float64)]
+    gpu._ok(lib().gamma_text2d_write(path.encode(), ctypes.byref(c), _ptr(keep[0]), _ptr(keep[1]), _ptr(keep[2]),
+                                     int(s.it), float(s.t), _ptr(keep[3]), _ptr(keep[4]), _ptr(keep[5])))
+
+
+def text2d_read(path: str, ntheta: int, nmax: int, **cfg):
+    """Simu::reinitialise of the 2D build: the state prepForRun leaves (ghost
+    tracks and cells for the ghost pass), and the tracks' theta/dtheta."""
+    c = _config(ntheta, nmax, **cfg)
+    NJ, cap = ntheta + 4, nmax + 4
+    NC = NJ * cap
+    nt = np.zeros(NJ, np.int32)
+    th, dth = np.zeros(ntheta), np.zeros(ntheta)
+    prim = np.zeros((NQ, NC))
+    x, dx, xI = np.zeros(NC), np.zeros(NC), np.zeros(NC)
+    it, t = ctypes.c_longlong(), ctypes.c_double()
+    gpu._ok(lib().gamma_text2d_read(path.encode(), ctypes.byref(c), _ptr(nt), ctypes.byref(it), ctypes.byref(t),
+                                    _ptr(th), _ptr(dth), _ptr(prim), _ptr(x), _ptr(dx), _ptr(xI)))
+    return State2D(NJ, cap, nt, prim, x, dx, xI, t=t.value, it=it.value), th, dth
+
+
 EXPORTS = ("gamma_2d_create", "gamma_2d_layout", "gamma_2d_set_params", "gamma_2d_set_guess", "gamma_2d_upload",
            "gamma_2d_step",
            "gamma_2d_download", "gamma_2d_prepare", "gamma_2d_download_fluxes", "gamma_2d_stream",
-           "gamma_2d_last_error", "gamma_2d_destroy")
+           "gamma_2d_last_error", "gamma_2d_destroy", "gamma_2d_print_cols", "gamma_2d_save", "gamma_2d_load",
+           "gamma_text2d_write", "gamma_text2d_read")

@@ -136,6 +136,11 @@ class TubeSetup:
         _update_ghosts(prim, x, dx, xI, g)
         return TrackState(nt, self.capacity, prim, x, dx, xI, np.full(nt, DT_INF), 0.0, 0)
 
+    def resume_state(self, path: str, cfg=None) -> TrackState:
+        """The -r start from a dump (Simu::reinitialise, then Simu::run's first
+        updateGhosts)."""
+        return _resume_1d(path, cfg or gpu.config_cart(), self.capacity, self.ngst)
+
     def run_params(self):
         return gpu.RunParams()
 
@@ -298,15 +303,37 @@ class Bm1dSetup:
                     prim[q, c] = lim / (lf * rho)
         _update_ghosts(prim, x, dx, xI, g)
         t = d["tstart"]
-        if t < self.t_bm_until:  # userBoundaries (BM1D.cpp:254-274)
-            for i in range(0, g):
+        self._user_boundaries(prim, x, t)
+        return TrackState(nt, self.capacity, prim, x, dx, xI, np.full(nt, DT_INF), t, 0)
+
+    def _user_boundaries(self, prim, x, t):
+        """userBoundaries (BM1D.cpp:254-274): the analytic BM state in the inner ghosts."""
+        if t < self.t_bm_until:
+            for i in range(0, self.ngst):
                 rho, u, p = self.calc_bm(x[i], t)
                 prim[RHO, i] = rho
                 prim[UU1, i] = u
                 prim[UU2, i] = 0.0
                 prim[PPP, i] = p
                 prim[TR1, i] = 2.0
-        return TrackState(nt, self.capacity, prim, x, dx, xI, np.full(nt, DT_INF), t, 0)
+
+    def resume_state(self, path: str, cfg=None) -> TrackState:
+        """The -r start from a dump (Simu::reinitialise, then Simu::run's first
+        updateGhosts with the BM inner boundary)."""
+        st = _resume_1d(path, cfg or gpu.config_sph(gamma_ad=self.gamma_ad), self.capacity, self.ngst)
+        self._user_boundaries(st.prim, st.x, st.t)
+        return st
+
+
+def _resume_1d(path, cfg, cap, ngst) -> TrackState:
+    """gamma_text1d_read, then updateGhosts without the user hook."""
+    r = gpu.text1d_read(path, cfg, cap)
+    n = r["ntrack"]
+    prim = np.ascontiguousarray(r["prim"][:, :n])
+    x, dx = r["x"][:n].copy(), r["dx"][:n].copy()
+    xI = r["xI"][:n - 1].copy()
+    _update_ghosts(prim, x, dx, xI, ngst)
+    return TrackState(n, cap, prim, x, dx, xI, np.full(n, DT_INF), r["t"], r["it"])
 
 
 def pack(states, offsets, total, nq):

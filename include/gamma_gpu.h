@@ -38,6 +38,7 @@ extern "C" {
 #define GAMMA_ERR_CUDA (-2)        /* a CUDA call failed; see gamma_gpu_last_error */
 #define GAMMA_ERR_CAPACITY (-3)    /* a track does not fit its capacity */
 #define GAMMA_ERR_NO_DEVICE (-4)   /* no usable sm_100 device */
+#define GAMMA_ERR_IO (-5)          /* a snapshot file could not be opened, written or parsed */
 #define GAMMA_ERR_NEG_DT (-30)     /* a CFL candidate was negative: the reference exit(30)s (cell.cpp:70-73) */
 
 enum { GAMMA_GEOM_SPHERICAL1D = 0, GAMMA_GEOM_CARTESIAN = 1 };
@@ -300,6 +301,71 @@ void gamma_2d_destroy(gamma_2d_t *ctx);
 
 /* The context's CUDA stream (a cudaStream_t). */
 void *gamma_gpu_stream(gamma_ctx_t *ctx);
+
+/* ---- Snapshots -------------------------------------------------------------
+ * Text: the reference's dump columns and its resume reader, so that files move
+ * between this library and the reference both ways.  The reference names a
+ * dump <dir>/phys%010d.out after the iteration.  Binary: this library's exact
+ * checkpoint (the text is lossy: 16 significant digits in 1D, 7 for most 2D
+ * columns). */
+
+/* Grid::printCols of the 1D build (src/IO/text1d.cpp:135-243) from host
+ * arrays: one line per active cell with t, nact, i, x, dx, dl, rho, v, p, D,
+ * S, tau, the first tracer, slot TR1+1 and, with local synchrotron, gamma_min
+ * and gamma_max.  prim holds nq rows of `stride` doubles starting at the run's
+ * cell 0 (ghosts included); slot TR1+1 must already hold what the reference
+ * stores there first (isShocked, with shock detection).  D, S and tau are
+ * prim2cons of each cell: what Cell::S.cons holds at a dump, since cons2prim
+ * ends with prim2cons (src/Hydro/rel_sph.cpp:318). */
+int gamma_text1d_write(const char *path, const gamma_config_t *cfg, int ntrack, long long it, double t,
+                       const double *prim, long long stride, const double *x, const double *dx);
+
+/* Simu::reinitialise of the 1D build (text1d.cpp:67-133, Grid::prepForRun)
+ * without the problem hooks: reads a dump into `cap` cells (nmax + 2 ngst) as
+ * reloadFromData, mpi_distribute and prepForRun leave them -- the file's cells
+ * at ngst.., the rest default states, 3-velocities turned into 4-velocities,
+ * interfaces from the cell positions.  prim is [nq][cap], xI [cap].  The
+ * ghost cells are the problem's updateGhosts to fill.  `it` comes from the
+ * file name, `t` from its first line. */
+int gamma_text1d_read(const char *path, const gamma_config_t *cfg, int cap, int *ntrack, long long *it, double *t,
+                      double *prim, double *x, double *dx, double *xI);
+
+/* A dump of run `run` as printCols makes it: with shock detection, stores
+ * isShocked in slot TR1+1 of every cell of the run on the device (the
+ * reference changes the state that way too), then writes <dir>/phys%010d.out
+ * from the run's state.  The directory must exist. */
+int gamma_gpu_print_cols(gamma_ctx_t *ctx, int run, const char *dir);
+
+/* Exact checkpoint of every run (the state the next step reads: primitives,
+ * cells, interfaces, dt_loc, t, it, the shock fields and the run parameters).
+ * Loading needs a context created with the same configuration and
+ * capacities. */
+int gamma_gpu_save(gamma_ctx_t *ctx, const char *path);
+int gamma_gpu_load(gamma_ctx_t *ctx, const char *path);
+
+/* Grid::printCols of the 2D build (src/IO/text2d.cpp:145-283) from host
+ * arrays in the 2D layout; theta/dtheta of the active tracks.  Slot TR1+1
+ * must already hold Sd (the reference's side effect). */
+int gamma_text2d_write(const char *path, const gamma_2d_config_t *cfg, const int *ntrack, const double *theta,
+                       const double *dtheta, long long it, double t, const double *prim, const double *x,
+                       const double *dx);
+
+/* Simu::reinitialise of the 2D build (text2d.cpp:75-143): the file's cells at
+ * (j + ngst, i + ngst), default states elsewhere, v2u and
+ * interfaceGeomFromCellPos on the active tracks; theta/dtheta (may be NULL)
+ * receive each active track's values.  Ghost tracks and cells are the ghost
+ * pass's to fill (gamma_2d_upload with run_ghosts). */
+int gamma_text2d_read(const char *path, const gamma_2d_config_t *cfg, int *ntrack, long long *it, double *t,
+                      double *theta, double *dtheta, double *prim, double *x, double *dx, double *xI);
+
+/* A 2D dump as printCols makes it (Sd stored in slot TR1+1 of every cell on
+ * the device first), written to <dir>/phys%010d.out. */
+int gamma_2d_print_cols(gamma_2d_t *ctx, const char *dir);
+
+/* Exact 2D checkpoint: state, gradients and neighbour lists (which the ghost
+ * cells carry between stages), dt_loc, t, dt, it, shock fields, parameters. */
+int gamma_2d_save(gamma_2d_t *ctx, const char *path);
+int gamma_2d_load(gamma_2d_t *ctx, const char *path);
 
 const char *gamma_gpu_strerror(int code);
 const char *gamma_gpu_last_error(const gamma_ctx_t *ctx);

@@ -40,6 +40,28 @@ REF_API int ref_init(void) {
   return 0;
 }
 
+/* Grid::printCols of the linked IO module (src/IO/text2d.cpp:145-283 in the *_io
+ * builds): writes ../results/Last/phys%010d.out relative to the working
+ * directory, which must exist.  io_none.cpp's printCols does nothing. */
+REF_API void ref_print_cols(void) { g_simu->grid.printCols(g_simu->it, g_simu->t); }
+
+/* The resume start of main.cpp (src/main.cpp:43-49 with -r): Simu::reinitialise
+ * from the last phys*.out under ../results/Last, then the pre-loop part of
+ * Simu::run (updateGhosts + printCols, src/simu.cpp:74-75).  *_io builds only. */
+REF_API int ref_resume(void) {
+  int argc = 0;
+  char **argv = nullptr;
+  mpi_init(&argc, &argv);
+  checkEnvironment();
+  DIR *dir = opendir("../results/Last");
+  if (!dir) return -1;
+  g_simu = new Simu();
+  g_simu->reinitialise(dir);
+  g_simu->grid.updateGhosts(g_simu->it, g_simu->t);
+  g_simu->grid.printCols(g_simu->it, g_simu->t);
+  return 0;
+}
+
 /* n iterations of the body of Simu::run's loop (src/simu.cpp:79-105). */
 REF_API int ref_step(int n) {
   Simu &s = *g_simu;

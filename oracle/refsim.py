@@ -52,7 +52,10 @@ class Snapshot:
 
 
 class RefSim:
-    """One reference build (``kind`` in {bm1d, bm1d_orig, tube})."""
+    """One reference build (``kind`` in {bm1d, bm1d_orig, tube, bm1d_synge}, or
+    bm1d_io / tube_io: the reference's own text IO module linked, so printCols
+    writes ../results/Last/phys*.out relative to the working directory and
+    resume() reads the last one back)."""
 
     def __init__(self, kind: str):
         path = os.path.join(REF_DIR, f"libref_{kind}.so")
@@ -76,6 +79,7 @@ class RefSim:
             lib.ref_set_param.restype = ctypes.c_int
         if hasattr(lib, "ref_set_c2p_epsrel"):
             lib.ref_set_c2p_epsrel.argtypes = [ctypes.c_double]
+        lib.ref_resume.restype = ctypes.c_int
         if hasattr(lib, "ref_bm1d_derived"):
             lib.ref_bm1d_derived.argtypes = [_dp]
         self.lib = lib
@@ -92,6 +96,15 @@ class RefSim:
 
     def init(self):
         self.lib.ref_init()
+
+    def print_cols(self):
+        """Grid::printCols at the current iteration (io builds write a file)."""
+        self.lib.ref_print_cols()
+
+    def resume(self):
+        """main.cpp's -r start from the last ../results/Last/phys*.out (io builds)."""
+        if self.lib.ref_resume() != 0:
+            raise FileNotFoundError("../results/Last missing")
 
     def set_c2p_epsrel(self, epsrel: float):
         """cons2prim's Brent stopping tolerance (1e-13 in the reference; 0 restores it)"""

@@ -59,10 +59,15 @@ class Grid2D:
 
 
 class RefJet2D:
-    def __init__(self):
-        if not os.path.exists(LIB):
-            raise FileNotFoundError(f"{LIB} missing: run `make -C oracle ref`")
-        lib = ctypes.CDLL(LIB, mode=os.RTLD_LOCAL)
+    """io=True loads the build with the reference's own text IO module
+    (libref_jet2d_io.so): printCols then writes ../results/Last/phys*.out
+    relative to the working directory, and resume() reads it back."""
+
+    def __init__(self, io: bool = False):
+        path = LIB.replace("libref_jet2d.so", "libref_jet2d_io.so") if io else LIB
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
+        lib = ctypes.CDLL(path, mode=os.RTLD_LOCAL)
         lib.ref_nq.restype = ctypes.c_int
         lib.ref_init.restype = ctypes.c_int
         lib.ref_step.argtypes = [ctypes.c_int]
@@ -77,6 +82,7 @@ class RefJet2D:
         lib.ref_set_c2p_epsrel.argtypes = [ctypes.c_double]
         lib.ref_fluxes.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int]
         lib.ref_fluxes.restype = ctypes.c_int
+        lib.ref_resume.restype = ctypes.c_int
         self.lib = lib
         self.nq = lib.ref_nq()
 
@@ -84,6 +90,15 @@ class RefJet2D:
         for k, v in params.items():
             if self.lib.ref_set_param(k.encode(), float(v)) != 0:
                 raise KeyError(f"unknown parameter {k}")
+
+    def print_cols(self):
+        """Grid::printCols at the current iteration (io builds write a file)."""
+        self.lib.ref_print_cols()
+
+    def resume(self):
+        """main.cpp's -r start from the last ../results/Last/phys*.out (io builds)."""
+        if self.lib.ref_resume() != 0:
+            raise FileNotFoundError("../results/Last missing")
 
     def derived(self) -> dict:
         out = np.zeros(8)
