@@ -231,9 +231,10 @@ def _jet2d_cpu_worker(args):
     return steps * 0.5 * (n0 + n1), dt
 
 
-def _jet2d_run(s, steps, warmup, guess_ptr=0, dev_index=None):
+def _jet2d_run(s, steps, warmup, guess_ptr=0, dev_index=None, after=None):
     """Fresh 2D grid from the initial state: warm-up steps, one step with
-    statistics, then `steps` timed graph launches (statistics over them)."""
+    statistics, then `steps` timed graph launches (statistics over them);
+    after(grid) runs before the grid is released."""
     import torch
 
     from gamma_b200 import gpu2d
@@ -261,8 +262,58 @@ def _jet2d_run(s, steps, warmup, guess_ptr=0, dev_index=None):
         clk.__exit__()
     assert st["status"] == 0, st
     out = g.download()
+    if after:
+        after(g)
     g.close()
     return e0.elapsed_time(e1), st, out, (clk.summary() if clk else None)
+
+
+def _dump_timing(g, s):
+    """Grid::printCols of the whole grid (device mark, download, parallel
+    formatting, write) and the resume reader on that file, timed on the host."""
+    import shutil
+    import tempfile
+
+    from gamma_b200 import gpu2d
+    d = tempfile.mkdtemp(prefix="gamma_dump_")
+    try:
+        t0 = time.perf_counter()
+        path = g.print_cols(d)
+        t1 = time.perf_counter()
+        nbytes = os.path.getsize(path)
+        st, _, _ = gpu2d.text2d_read(path, s.ntheta, s.nmax)
+        t2 = time.perf_counter()
+        cells = int(sum(max(0, int(n) - 4) for n in st.ntrack[2:-2]))
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return {"cells": cells, "bytes": nbytes, "write_s": t1 - t0, "read_s": t2 - t1,
+            "write_cells_per_s": cells / (t1 - t0), "read_cells_per_s": cells / (t2 - t1),
+            "host_threads": os.cpu_count()}
+
+
+def _jet2d_ref_dump_worker(args):
+    """The reference's own printCols and resume (libref_jet2d_io.so) on its 2D
+    state after a few steps, timed."""
+    params, warmup, root = args
+    sys.path.insert(0, ROOT)
+    os.makedirs(os.path.join(root, "results", "Last"), exist_ok=True)
+    os.makedirs(os.path.join(root, "bin"), exist_ok=True)
+    os.chdir(os.path.join(root, "bin"))
+    from oracle.refsim2d import RefJet2D
+    s = RefJet2D(io=True)
+    s.set_params(**params)
+    s.init()
+    s.step(warmup)
+    cells = sum(t.ntrack - 4 for t in s.snapshot().tracks[2:-2])
+    t0 = time.perf_counter()
+    s.print_cols()
+    t1 = time.perf_counter()
+    r = RefJet2D(io=True)
+    r.set_params(**params)
+    t2 = time.perf_counter()
+    r.resume()  # reinitialise, updateGhosts and one more printCols
+    t3 = time.perf_counter()
+    return cells, t1 - t0, (t3 - t2) - (t1 - t0)
 
 
 def _active_cells(out):
@@ -279,7 +330,9 @@ def jet2d_arm(args, dev_index):
     from the same initial state, compared after the same steps."""
     from gamma_b200 import gpu, problems
     s = problems.Jet2dSetup(**dict(JET2D, ntheta=args.ntheta))
-    ms, st, out, clk = _jet2d_run(s, args.steps, args.warmup, 0, dev_index)
+    dump = {}
+    ms, st, out, clk = _jet2d_run(s, args.steps, args.warmup, 0, dev_index,
+                                  after=lambda g: dump.update(_dump_timing(g, s)))
     zones = st["zone_updates"]
     n = out.ntrack[2:-2]
     res = {"workload": f"{s.ntheta} theta tracks over [{s.th_min}, {s.th_max}] rad, BM cap below {s.th_jet} rad, "
@@ -336,6 +389,21 @@ def jet2d_arm(args, dev_index):
         res["cpu_baseline"] = {"value": z / t, "unit": "zone-updates/s", "cores": 1, "kind": "reference",
                                "sample": "the same wedge with 16 tracks of 1,200 initial cells, 10 steps after 3 "
                                          "warm-up steps, one thread"}
+    if not args.no_cpu_baseline and os.path.exists(lib.replace("jet2d.so", "jet2d_io.so")):
+        import multiprocessing as mp
+        import shutil
+        import tempfile
+        root = tempfile.mkdtemp(prefix="gamma_refdump_")
+        try:
+            with mp.get_context("spawn").Pool(1) as pool:
+                cells, tw, tr = pool.apply(_jet2d_ref_dump_worker, ((dict(ncell=1200, ntrack=16, nmax=1200), 3,
+                                                                     root),))
+        finally:
+            shutil.rmtree(root, ignore_errors=True)
+        dump["reference"] = {"cells": cells, "write_cells_per_s": cells / tw, "read_cells_per_s": cells / max(tr, 1e-9),
+                             "note": "the reference's printCols / reinitialise on the 16-track wedge, one thread; "
+                                     "its read time is the resume minus one printCols"}
+    res["dump"] = dump
     return res
 
 

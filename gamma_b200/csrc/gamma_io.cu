@@ -7,8 +7,10 @@
 //
 // Binary checkpoint: this library's own exact format (every array that carries
 // state from one step to the next, raw), written as tagged blocks.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 // The state conversions are the step's own (physics.cuh, physics2d.cuh),
 // compiled here for the host.
@@ -62,6 +64,38 @@ double trac2gammae(double trac, double lfac, double rho) {
   return 0;
 }
 
+// Formats rows 0 .. n-1 with fmt(row, buf, size) -> characters written and
+// writes them in order.  Large dumps are formatted by several host threads,
+// each into its own buffer; the bytes are those of one thread's loop.
+template <class Fmt>
+bool write_rows(FILE *f, long long n, Fmt fmt) {
+  constexpr int kLine = 640;
+  const long long per = 16384;
+  unsigned hw = std::thread::hardware_concurrency();
+  const int nt = (int)std::max<long long>(1, std::min<long long>({(long long)(hw ? hw : 1), 32, (n + per - 1) / per}));
+  std::vector<std::string> out(nt);
+  auto work = [&](int k) {
+    const long long a = n * k / nt, b = n * (k + 1) / nt;
+    std::string &o = out[k];
+    o.reserve((size_t)(b - a) * 256);
+    char line[kLine];
+    for (long long r = a; r < b; ++r) {
+      const int len = fmt(r, line, kLine);
+      o.append(line, (size_t)std::min(len, kLine - 1));
+    }
+  };
+  if (nt == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int k = 0; k < nt; ++k) th.emplace_back(work, k);
+    for (auto &t : th) t.join();
+  }
+  for (auto &o : out)
+    if (!o.empty() && std::fwrite(o.data(), 1, o.size(), f) != o.size()) return false;
+  return true;
+}
+
 }  // namespace
 
 int write_text1d(const char *path, const gamma_config_t &cfg, int ntrack, long long it, double t,
@@ -74,32 +108,32 @@ int write_text1d(const char *path, const gamma_config_t &cfg, int ntrack, long l
   const bool synch = cfg.local_synchrotron != 0;
   if (synch) std::fprintf(f, "t nact i x dx dlx rho vx p D sx tau trac Sd gmin gmax\n");
   else std::fprintf(f, "t nact i x dx dlx rho vx p D sx tau trac Sd\n");
-  double p[10] = {0}, c[10] = {0};
-  for (int i = ng; i < ntrack - ng; ++i) {
+  const int nactd = ntrack - 2 * ng;
+  const bool ok = write_rows(f, nactd, [&](long long r, char *line, int size) {
+    const int i = ng + (int)r;
+    double p[10] = {0}, c[10] = {0};
     for (int q = 0; q < nq; ++q) p[q] = prim[q * stride + i];
     // Cell::S.cons at a dump: cons2prim ends with prim2cons (rel_sph.cpp:318)
     if (is_sph(cfg)) prim2cons<CfgSph>(ph, p, c);
     else prim2cons<CfgCart>(ph, p, c);
     const double lfac = lfac_of(p[UU1]);
-    const int nactd = ntrack - 2 * ng;
     // spherical1D and cartesian: dl = dx (spherical1D.cpp:23-33, cartesian.cpp:20-26)
     if (synch) {
       const double gmin = trac2gammae(p[GMN], lfac, p[RHO]);
       const double gmax = trac2gammae(p[GMX], lfac, p[RHO]);
-      std::fprintf(f,
-                   "%1.15le %d %d %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le "
-                   "%1.15le %1.15le %1.15le\n",
-                   t, nactd, i - ng, x[i], dx[i], dx[i], p[RHO], p[UU1] / lfac, p[PPP], c[DEN], c[SS1], c[TAU],
-                   p[TR1], p[TR1 + 1], gmin, gmax);
-    } else {
-      std::fprintf(f,
-                   "%1.15le %d %d %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le "
-                   "%1.15le\n",
-                   t, nactd, i - ng, x[i], dx[i], dx[i], p[RHO], p[UU1] / lfac, p[PPP], c[DEN], c[SS1], c[TAU],
-                   p[TR1], p[TR1 + 1]);
+      return std::snprintf(line, size,
+                           "%1.15le %d %d %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le "
+                           "%1.15le %1.15le %1.15le %1.15le\n",
+                           t, nactd, i - ng, x[i], dx[i], dx[i], p[RHO], p[UU1] / lfac, p[PPP], c[DEN], c[SS1],
+                           c[TAU], p[TR1], p[TR1 + 1], gmin, gmax);
     }
-  }
-  return std::fclose(f) == 0 ? GAMMA_OK : GAMMA_ERR_IO;
+    return std::snprintf(line, size,
+                         "%1.15le %d %d %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le %1.15le "
+                         "%1.15le %1.15le\n",
+                         t, nactd, i - ng, x[i], dx[i], dx[i], p[RHO], p[UU1] / lfac, p[PPP], c[DEN], c[SS1], c[TAU],
+                         p[TR1], p[TR1 + 1]);
+  });
+  return (std::fclose(f) == 0 && ok) ? GAMMA_OK : GAMMA_ERR_IO;
 }
 
 int write_text2d(const char *path, const gamma_2d_config_t &cfg, int NJ, int cap, const int *ntrack,
@@ -113,28 +147,31 @@ int write_text2d(const char *path, const gamma_2d_config_t &cfg, int NJ, int cap
   const int ng = cfg.ngst;
   const long long NC = (long long)NJ * cap;
   std::fprintf(f, "t nact j i x y dx dy dlx dly rho vx vy p D sx sy tau trac Sd gmin gmax gmid psyn\n");
-  double p[d2::NQ], c[d2::NQ];
-  for (int j = ng; j < NJ - ng; ++j) {
-    const int n = ntrack[j];
+  // rows in (j, i) order: start[k] = first row of active track ng + k
+  std::vector<long long> start(NJ - 2 * ng + 1, 0);
+  for (int j = ng; j < NJ - ng; ++j) start[j - ng + 1] = start[j - ng] + std::max(0, ntrack[j] - 2 * ng);
+  const bool ok = write_rows(f, start.back(), [&](long long r, char *line, int size) {
+    const int k = (int)(std::upper_bound(start.begin(), start.end(), r) - start.begin()) - 1;
+    const int j = ng + k, n = ntrack[j], i = ng + (int)(r - start[k]);
     const double th = theta[j - ng], dth = dtheta[j - ng];
-    for (int i = ng; i < n - ng; ++i) {
-      const long long g = (long long)j * cap + i;
-      for (int q = 0; q < d2::NQ; ++q) p[q] = prim[q * NC + g];
-      const double r = x[g];
-      d2::prim2cons(ph, p, c, r);  // cons2prim(G.x[r_]) ends every update (rk3.cpp:183-191)
-      const double lf = d2::lfac(p);
-      const double gmin = trac2gammae(p[GMN], lf, p[RHO]);
-      const double gmax = trac2gammae(p[GMX], lf, p[RHO]);
-      const double gmid = trac2gammae(p[GMD], lf, p[RHO]);
-      // spherical: dl = (dr, r dtheta) (spherical.cpp:36-47)
-      std::fprintf(f,
-                   "%1.15le %d %d %d %1.15le %1.15le %1.15le %1.15le %1.15le %le %le %le %le %le %le %le %le %le %le "
-                   "%le %le %le %le %le\n",
-                   t, n - 2 * ng, j - ng, i - ng, r, th, dx[g], dth, dx[g], r * dth, p[RHO], p[UU1] / lf, p[UU2] / lf,
-                   p[PPP], c[DEN], c[SS1], c[SS2], c[TAU], p[TR1], p[TR1 + 1], gmin, gmax, gmid, p[PSN]);
-    }
-  }
-  return std::fclose(f) == 0 ? GAMMA_OK : GAMMA_ERR_IO;
+    const long long g = (long long)j * cap + i;
+    double p[d2::NQ], c[d2::NQ];
+    for (int q = 0; q < d2::NQ; ++q) p[q] = prim[q * NC + g];
+    const double rr = x[g];
+    d2::prim2cons(ph, p, c, rr);  // cons2prim(G.x[r_]) ends every update (rk3.cpp:183-191)
+    const double lf = d2::lfac(p);
+    const double gmin = trac2gammae(p[GMN], lf, p[RHO]);
+    const double gmax = trac2gammae(p[GMX], lf, p[RHO]);
+    const double gmid = trac2gammae(p[GMD], lf, p[RHO]);
+    // spherical: dl = (dr, r dtheta) (spherical.cpp:36-47)
+    return std::snprintf(line, size,
+                         "%1.15le %d %d %d %1.15le %1.15le %1.15le %1.15le %1.15le %le %le %le %le %le %le %le %le "
+                         "%le %le %le %le %le %le %le\n",
+                         t, n - 2 * ng, j - ng, i - ng, rr, th, dx[g], dth, dx[g], rr * dth, p[RHO], p[UU1] / lf,
+                         p[UU2] / lf, p[PPP], c[DEN], c[SS1], c[SS2], c[TAU], p[TR1], p[TR1 + 1], gmin, gmax, gmid,
+                         p[PSN]);
+  });
+  return (std::fclose(f) == 0 && ok) ? GAMMA_OK : GAMMA_ERR_IO;
 }
 
 // ---------------------------------------------------------------------------

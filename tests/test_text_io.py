@@ -155,3 +155,17 @@ def test_text_reader_rejects_bad_files(tmp_path):
     big.write_text("header\n" + line + "\n")
     with pytest.raises(gpu.GammaError):  # more cells than the capacity
         gpu.text1d_read(str(big), gpu.config_sph(), 100)
+
+
+def test_text1d_large_dump_matches_reference(tmp_path):
+    """50,000 cells: the writer formats in several host threads; the bytes are
+    still the reference's (its initial dump, iteration 0)."""
+    if not ref_available("bm1d_io"):
+        pytest.skip("oracle/_ref/libref_bm1d_io.so not built")
+    from gamma_b200 import gpu
+    params = dict(BM, ncell=50000, nmax=60000)
+    snap, sc = _in_ref_process(_ref_dump_1d, "bm1d_io", params, 0, str(tmp_path))
+    ref_file = os.path.join(tmp_path, "results", "Last", "phys0000000000.out")
+    mine = str(tmp_path / "mine.out")
+    gpu.text1d_write(mine, gpu.config_sph(), snap.prim, snap.x, snap.dx, 0, snap.t)
+    assert open(mine, "rb").read() == open(ref_file, "rb").read()
