@@ -261,6 +261,67 @@ long long it_of_name(const char *path) {
   return it;
 }
 
+// The data lines of a dump (the header skipped).  The reference reads lines
+// with fgets into 512 bytes; a longer line is refused here.
+bool split_lines(const char *path, std::string &text, std::vector<size_t> &start) {
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return false;
+  char chunk[1 << 16];
+  size_t got;
+  while ((got = std::fread(chunk, 1, sizeof(chunk), f)) > 0) text.append(chunk, got);
+  std::fclose(f);
+  size_t pos = text.find('\n');
+  if (pos == std::string::npos) return false;  // no header line
+  ++pos;
+  while (pos < text.size()) {
+    size_t e = text.find('\n', pos);
+    if (e == std::string::npos) e = text.size();
+    if (e - pos + 1 > 511) return false;
+    if (e > pos) start.push_back(pos);
+    pos = e + 1;
+  }
+  start.push_back(text.size() + 1);  // sentinel: the end of the last line + 1
+  return true;
+}
+
+// Parses line k of `text` with parse(buf, row) -> ok on several host threads;
+// rows keeps the file's order.
+template <class Row, class Parse>
+bool parse_rows(const std::string &text, const std::vector<size_t> &start, std::vector<Row> &rows, Parse parse) {
+  const long long n = (long long)start.size() - 1;
+  rows.resize((size_t)std::max<long long>(n, 0));
+  unsigned hw = std::thread::hardware_concurrency();
+  const int nt = (int)std::max<long long>(1, std::min<long long>({(long long)(hw ? hw : 1), 32, (n + 16383) / 16384}));
+  std::vector<char> ok(nt, 1);
+  auto work = [&](int k) {
+    char buf[512];
+    for (long long r = n * k / nt; r < n * (k + 1) / nt; ++r) {
+      const size_t a = start[r], len = std::min(start[r + 1] - 1 - a, sizeof(buf) - 1);
+      std::memcpy(buf, text.data() + a, len);
+      buf[len] = '\0';
+      if (!parse(buf, rows[r])) ok[k] = 0;
+    }
+  };
+  if (nt == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int k = 0; k < nt; ++k) th.emplace_back(work, k);
+    for (auto &t : th) t.join();
+  }
+  return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
+}
+
+struct Row1 {
+  double t, x, dx, rho, vx, p, trac, gmn, gmx;
+  int nact, i;
+};
+
+struct Row2 {
+  double t, x, y, dx, dy, rho, vx, vy, p, trac, gmn, gmx, gmd, psyn;
+  int nact, j, i;
+};
+
 }  // namespace
 
 GAMMA_API int gamma_text1d_read(const char *path, const gamma_config_t *cfg, int cap, int *ntrack, long long *it,
@@ -268,51 +329,47 @@ GAMMA_API int gamma_text1d_read(const char *path, const gamma_config_t *cfg, int
   if (!path || !cfg || !ntrack || !prim || !x || !dx || !xI || cfg->nq < 6 || cfg->nq > 10) return GAMMA_ERR_INVALID;
   const int ng = cfg->ngst, nq = cfg->nq;
   if (cap < 2 * ng + 1) return GAMMA_ERR_INVALID;
-  FILE *f = std::fopen(path, "r");
-  if (!f) return GAMMA_ERR_IO;
+  std::string text;
+  std::vector<size_t> start;
+  if (!split_lines(path, text, start)) return GAMMA_ERR_IO;
+  const bool synch = cfg->local_synchrotron != 0;
+  std::vector<Row1> rows;
+  // Data::Data and the values Data::toCell stores (text1d.cpp:17-63)
+  const bool parsed = parse_rows(text, start, rows, [&](const char *line, Row1 &r) {
+    double dlx, D, sx, tau, Sd, gmin = 0., gmax = 0.;
+    const int got =
+        synch ? std::sscanf(line, "%le %d %d %le %le %le %le %le %le %le %le %le %le %le %le %le\n", &r.t, &r.nact,
+                            &r.i, &r.x, &r.dx, &dlx, &r.rho, &r.vx, &r.p, &D, &sx, &tau, &r.trac, &Sd, &gmin, &gmax)
+              : std::sscanf(line, "%le %d %d %le %le %le %le %le %le %le %le %le %le\n", &r.t, &r.nact, &r.i, &r.x,
+                            &r.dx, &dlx, &r.rho, &r.vx, &r.p, &D, &sx, &tau, &r.trac);
+    if (synch) {
+      r.gmn = pow(r.rho, 1. / 3.) / gmin;
+      r.gmx = pow(r.rho, 1. / 3.) / gmax;
+    }
+    return got == (synch ? 16 : 13);
+  });
+  if (!parsed || rows.empty()) return GAMMA_ERR_IO;
   // Grid::initialise + Cell defaults (FluidState: rho = p = 1, the rest 0)
   for (int q = 0; q < nq; ++q)
     for (int i = 0; i < cap; ++i) prim[(size_t)q * cap + i] = (q == RHO || q == PPP) ? 1. : 0.;
   for (int i = 0; i < cap; ++i) x[i] = dx[i] = 0.;
-  const bool synch = cfg->local_synchrotron != 0;
-  char line[512];
-  int nact = -1, rows = 0, rc = GAMMA_OK;
-  double t0 = 0.;
-  if (!std::fgets(line, sizeof(line), f)) rc = GAMMA_ERR_IO;  // header
-  while (rc == GAMMA_OK && std::fgets(line, sizeof(line), f)) {
-    // Data::Data and Data::toCell (text1d.cpp:17-63); Cinit[i] lands in Ctot[ngst + i]
-    double tt, xx, ddx, dlx, rho, vx, p, D, sx, tau, trac, Sd = 0., gmin = 0., gmax = 0.;
-    int na, i;
-    int got = synch ? std::sscanf(line, "%le %d %d %le %le %le %le %le %le %le %le %le %le %le %le %le\n", &tt, &na,
-                                  &i, &xx, &ddx, &dlx, &rho, &vx, &p, &D, &sx, &tau, &trac, &Sd, &gmin, &gmax)
-                    : std::sscanf(line, "%le %d %d %le %le %le %le %le %le %le %le %le %le\n", &tt, &na, &i, &xx,
-                                  &ddx, &dlx, &rho, &vx, &p, &D, &sx, &tau, &trac);
-    if (got != (synch ? 16 : 13)) {
-      rc = GAMMA_ERR_IO;
-      break;
-    }
-    if (i < 0 || i + 2 * ng > cap - 0 || na + 2 * ng > cap) {
-      rc = GAMMA_ERR_CAPACITY;
-      break;
-    }
-    if (rows == 0) t0 = tt;
-    const int c = ng + i;
-    x[c] = xx;
-    dx[c] = ddx;
-    prim[(size_t)RHO * cap + c] = rho;
-    prim[(size_t)UU1 * cap + c] = vx;  // VV1: a 3-velocity until prepForRun's v2u
-    prim[(size_t)PPP * cap + c] = p;
-    prim[(size_t)TR1 * cap + c] = trac;
+  int nact = -1;
+  for (const Row1 &r : rows) {  // file order; Cinit[i] lands in Ctot[ngst + i]
+    if (r.i < 0 || r.i + 2 * ng > cap || r.nact + 2 * ng > cap) return GAMMA_ERR_CAPACITY;
+    const int c = ng + r.i;
+    x[c] = r.x;
+    dx[c] = r.dx;
+    prim[(size_t)RHO * cap + c] = r.rho;
+    prim[(size_t)UU1 * cap + c] = r.vx;  // VV1: a 3-velocity until prepForRun's v2u
+    prim[(size_t)PPP * cap + c] = r.p;
+    prim[(size_t)TR1 * cap + c] = r.trac;
     if (synch) {
-      prim[(size_t)GMN * cap + c] = pow(rho, 1. / 3.) / gmin;
-      prim[(size_t)GMX * cap + c] = pow(rho, 1. / 3.) / gmax;
+      prim[(size_t)GMN * cap + c] = r.gmn;
+      prim[(size_t)GMX * cap + c] = r.gmx;
     }
-    nact = na;
-    ++rows;
+    nact = r.nact;
   }
-  std::fclose(f);
-  if (rc != GAMMA_OK) return rc;
-  if (rows == 0 || nact < 0) return GAMMA_ERR_IO;
+  if (nact < 0) return GAMMA_ERR_IO;
   const int n = nact + 2 * ng;
   // Grid::prepForRun: v2u (1d.cpp:934-951) and interfaceGeomFromCellPos (:844-856)
   for (int i = 0; i < n; ++i) {
@@ -327,7 +384,7 @@ GAMMA_API int gamma_text1d_read(const char *path, const gamma_config_t *cfg, int
   for (int i = 0; i < n - 1; ++i) xI[i] = (i != iL) ? x[i] + dx[i] / 2. : x[i + 1] - dx[i + 1] / 2.;
   *ntrack = n;
   if (it) *it = it_of_name(path);
-  if (t) *t = t0;
+  if (t) *t = rows.front().t;
   return GAMMA_OK;
 }
 
@@ -337,54 +394,46 @@ GAMMA_API int gamma_text2d_read(const char *path, const gamma_2d_config_t *cfg, 
   if (!path || !cfg || !ntrack || !prim || !x || !dx || !xI || cfg->nq != 10) return GAMMA_ERR_INVALID;
   const int ng = cfg->ngst, NJ = cfg->ntheta + 2 * ng, cap = cfg->nmax + 2 * ng;
   const long long NC = (long long)NJ * cap;
-  FILE *f = std::fopen(path, "r");
-  if (!f) return GAMMA_ERR_IO;
+  std::string text;
+  std::vector<size_t> start;
+  if (!split_lines(path, text, start)) return GAMMA_ERR_IO;
+  std::vector<Row2> rows;
+  // Data::Data and the values Data::toCell stores (text2d.cpp:17-67)
+  const bool parsed = parse_rows(text, start, rows, [&](const char *line, Row2 &r) {
+    double dlx, dly, D, sx, sy, tau, Sd, gmin, gmax, gmid;
+    const int got = std::sscanf(
+        line, "%le %d %d %d %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le\n", &r.t,
+        &r.nact, &r.j, &r.i, &r.x, &r.y, &r.dx, &r.dy, &dlx, &dly, &r.rho, &r.vx, &r.vy, &r.p, &D, &sx, &sy, &tau,
+        &r.trac, &Sd, &gmin, &gmax, &gmid, &r.psyn);
+    r.gmn = pow(r.rho, 1. / 3.) / gmin;
+    r.gmx = pow(r.rho, 1. / 3.) / gmax;
+    r.gmd = pow(r.rho, 1. / 3.) / gmid;
+    return got == 24;
+  });
+  if (!parsed || rows.empty()) return GAMMA_ERR_IO;
   for (int q = 0; q < d2::NQ; ++q)
     for (long long g = 0; g < NC; ++g) prim[q * NC + g] = (q == RHO || q == PPP) ? 1. : 0.;
   for (long long g = 0; g < NC; ++g) x[g] = dx[g] = xI[g] = 0.;
   for (int j = 0; j < NJ; ++j) ntrack[j] = 0;
-  char line[512];
-  int rows = 0, rc = GAMMA_OK;
-  double t0 = 0.;
-  if (!std::fgets(line, sizeof(line), f)) rc = GAMMA_ERR_IO;
-  while (rc == GAMMA_OK && std::fgets(line, sizeof(line), f)) {
-    // Data::Data and Data::toCell (text2d.cpp:17-67); Cinit[j][i] lands in Ctot[j+ngst][i+ngst]
-    double tt, xx, yy, ddx, ddy, dlx, dly, rho, vx, vy, p, D, sx, sy, tau, trac, Sd, gmin, gmax, gmid, psyn;
-    int na, j, i;
-    const int got = std::sscanf(
-        line, "%le %d %d %d %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le %le\n", &tt,
-        &na, &j, &i, &xx, &yy, &ddx, &ddy, &dlx, &dly, &rho, &vx, &vy, &p, &D, &sx, &sy, &tau, &trac, &Sd, &gmin,
-        &gmax, &gmid, &psyn);
-    if (got != 24) {
-      rc = GAMMA_ERR_IO;
-      break;
-    }
-    if (j < 0 || j >= cfg->ntheta || i < 0 || i >= cfg->nmax || na > cfg->nmax) {
-      rc = GAMMA_ERR_CAPACITY;
-      break;
-    }
-    if (rows == 0) t0 = tt;
-    const int jj = j + ng;
-    const long long g = (long long)jj * cap + ng + i;
-    x[g] = xx;
-    dx[g] = ddx;
-    if (theta) theta[j] = yy;
-    if (dtheta) dtheta[j] = ddy;
-    prim[RHO * NC + g] = rho;
-    prim[UU1 * NC + g] = vx;  // VV1, VV2: 3-velocities until v2u
-    prim[UU2 * NC + g] = vy;
-    prim[PPP * NC + g] = p;
-    prim[TR1 * NC + g] = trac;
-    prim[GMN * NC + g] = pow(rho, 1. / 3.) / gmin;
-    prim[GMX * NC + g] = pow(rho, 1. / 3.) / gmax;
-    prim[GMD * NC + g] = pow(rho, 1. / 3.) / gmid;
-    prim[PSN * NC + g] = psyn;
-    ntrack[jj] = na + 2 * ng;  // reloadFromData (text2d.cpp:127-143)
-    ++rows;
+  for (const Row2 &r : rows) {  // file order; Cinit[j][i] lands in Ctot[j+ngst][i+ngst]
+    if (r.j < 0 || r.j >= cfg->ntheta || r.i < 0 || r.i >= cfg->nmax || r.nact > cfg->nmax) return GAMMA_ERR_CAPACITY;
+    const int jj = r.j + ng;
+    const long long g = (long long)jj * cap + ng + r.i;
+    x[g] = r.x;
+    dx[g] = r.dx;
+    if (theta) theta[r.j] = r.y;
+    if (dtheta) dtheta[r.j] = r.dy;
+    prim[RHO * NC + g] = r.rho;
+    prim[UU1 * NC + g] = r.vx;  // VV1, VV2: 3-velocities until v2u
+    prim[UU2 * NC + g] = r.vy;
+    prim[PPP * NC + g] = r.p;
+    prim[TR1 * NC + g] = r.trac;
+    prim[GMN * NC + g] = r.gmn;
+    prim[GMX * NC + g] = r.gmx;
+    prim[GMD * NC + g] = r.gmd;
+    prim[PSN * NC + g] = r.psyn;
+    ntrack[jj] = r.nact + 2 * ng;  // reloadFromData (text2d.cpp:127-143)
   }
-  std::fclose(f);
-  if (rc != GAMMA_OK) return rc;
-  if (rows == 0) return GAMMA_ERR_IO;
   // the ghost tracks take the edge tracks' lengths (updateGhosts copies the
   // edge tracks into them, text2d.cpp leaves them as initialise made them)
   for (int j = 0; j < ng; ++j) {
@@ -411,6 +460,6 @@ GAMMA_API int gamma_text2d_read(const char *path, const gamma_2d_config_t *cfg, 
       xI[o + i] = (i != iL) ? x[o + i] + dx[o + i] / 2. : x[o + i + 1] - dx[o + i + 1] / 2.;
   }
   if (it) *it = it_of_name(path);
-  if (t) *t = t0;
+  if (t) *t = rows.front().t;
   return GAMMA_OK;
 }

@@ -158,8 +158,9 @@ def test_text_reader_rejects_bad_files(tmp_path):
 
 
 def test_text1d_large_dump_matches_reference(tmp_path):
-    """50,000 cells: the writer formats in several host threads; the bytes are
-    still the reference's (its initial dump, iteration 0)."""
+    """50,000 cells: the writer formats and the reader parses in several host
+    threads; the bytes and the resumed state are still the reference's (its
+    initial dump, iteration 0)."""
     if not ref_available("bm1d_io"):
         pytest.skip("oracle/_ref/libref_bm1d_io.so not built")
     from gamma_b200 import gpu
@@ -169,3 +170,10 @@ def test_text1d_large_dump_matches_reference(tmp_path):
     mine = str(tmp_path / "mine.out")
     gpu.text1d_write(mine, gpu.config_sph(), snap.prim, snap.x, snap.dx, 0, snap.t)
     assert open(mine, "rb").read() == open(ref_file, "rb").read()
+    # the reader parses in several threads too
+    from gamma_b200 import problems
+    st = problems.Bm1dSetup(**params).resume_state(ref_file)
+    ref_snap, _ = _in_ref_process(_ref_resume_1d, "bm1d_io", params, str(tmp_path))
+    n = st.ntrack
+    assert n == ref_snap.ntrack
+    assert np.array_equal(st.prim, ref_snap.prim[:, :n]) and np.array_equal(st.xI, ref_snap.xI[:n - 1])
