@@ -177,7 +177,7 @@ __global__ void k_stale(Grid2 G) {
   if (j <= G.NJ - 2) stale_append(G, j);
 }
 
-__global__ void k_tgrad(Grid2 G) {
+__global__ void __launch_bounds__(kThreads, GB2_MINB) k_tgrad(Grid2 G) {
   FOR_LIVE_CELLS(G, j, i) trans_grad(G, j, i);
 }
 

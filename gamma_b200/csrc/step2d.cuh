@@ -329,6 +329,26 @@ GB_HD void overlap(const Grid2 &G, long long g0, long long gn, double *xm, doubl
   *w = fmax(0., fmin(xR0, xRn) - fmax(xL0, xLn));
 }
 
+// The gradient towards neighbour gn, (qR - qL) / dcen, of every slot.
+GB_HD void neighbour_grad(const Grid2 &G, long long gn, double xm, double cr0, double ct0, const double *p0,
+                          const double *m0, double *grad) {
+  const int jn = track_of(G, gn);
+  const double dxmL = xm - cr0;
+  const double dxmR = xm - cen_r(G.x[gn], G.dx[gn]);
+  const double dcen = tgeo(G, jn).cen_t - ct0;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const double qL = p0[q] + m0[q] * dxmL;
+    const double qR = G.prim[q * G.NC + gn] + G.gmv[q * G.NC + gn] * dxmR;
+    grad[q] = (qR - qL) / dcen;
+  }
+}
+
+// Pass 1 forms the dA-weighted average; pass 2 folds in minmod with each
+// neighbour's gradient in the reference's order (an order-dependent chain:
+// minmod(x, x) = 0).  The first KGRAD gradients of pass 1 are kept for pass 2.
+constexpr int KGRAD = 4;
+
 GB_HD void trans_grad(const Grid2 &G, int j, int i) {
   const int n = G.ntrack[j];
   if (i >= n) return;
@@ -341,38 +361,52 @@ GB_HD void trans_grad(const Grid2 &G, int j, int i) {
   const double cr0 = cen_r(G.x[g0], G.dx[g0]);
   const TrackGeo t0 = tgeo(G, j);
   const double ct0 = t0.cen_t;
-  double avg[NQ];
+  double p0[NQ], m0[NQ], avg[NQ], grad[NQ], kept[KGRAD][NQ];
 #pragma unroll
-  for (int q = 0; q < NQ; ++q) avg[q] = 0.;
+  for (int q = 0; q < NQ; ++q) {
+    p0[q] = G.prim[q * G.NC + g0];
+    m0[q] = G.gmv[q * G.NC + g0];
+    avg[q] = 0.;
+  }
+  const int f0 = G.nbr[0 * G.NC + g0], c0 = G.nbr[1 * G.NC + g0];
+  const int f1 = G.nbr[2 * G.NC + g0], c1 = G.nbr[3 * G.NC + g0];
   double dAtot = 0.;
-  // pass 1: dA-weighted average; pass 2: minmod with each neighbour's gradient
-  for (int pass = 0; pass < 2; ++pass) {
-    for (int d = 0; d < 2; ++d) {
-      const int first = G.nbr[(2 * d) * G.NC + g0], cnt = G.nbr[(2 * d + 1) * G.NC + g0];
-      for (int k = 0; k < cnt; ++k) {
-        const long long gn = first + k;
-        const int jn = track_of(G, gn);
-        double xm, w;
-        overlap(G, g0, gn, &xm, &w);
-        // theta of the interface: th - dth/2 below, th (unmoved) above
-        const double dA = dA_t(xm, w, d == 0 ? t0.s_lo : t0.s_mid);
-        if (pass == 0) dAtot += dA;
-        const double dxmL = xm - cr0;
-        const double dxmR = xm - cen_r(G.x[gn], G.dx[gn]);
-        const double dcen = tgeo(G, jn).cen_t - ct0;
+  int kn = 0;
+  for (int d = 0; d < 2; ++d) {
+    const int first = d == 0 ? f0 : f1, cnt = d == 0 ? c0 : c1;
+    for (int k = 0; k < cnt; ++k, ++kn) {
+      const long long gn = first + k;
+      double xm, w;
+      overlap(G, g0, gn, &xm, &w);
+      // theta of the interface: th - dth/2 below, th (unmoved) above
+      const double dA = dA_t(xm, w, d == 0 ? t0.s_lo : t0.s_mid);
+      dAtot += dA;
+      neighbour_grad(G, gn, xm, cr0, ct0, p0, m0, grad);
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-          const double qL = G.prim[q * G.NC + g0] + G.gmv[q * G.NC + g0] * dxmL;
-          const double qR = G.prim[q * G.NC + gn] + G.gmv[q * G.NC + gn] * dxmR;
-          const double grad = (qR - qL) / dcen;
-          if (pass == 0) avg[q] += grad * dA;
-          else avg[q] = minmod(avg[q], grad);
-        }
+      for (int q = 0; q < NQ; ++q) avg[q] += grad[q] * dA;
+      if (kn < KGRAD) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) kept[kn][q] = grad[q];
       }
     }
-    if (pass == 0) {
+  }
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) avg[q] /= dAtot;
+  for (int q = 0; q < NQ; ++q) avg[q] /= dAtot;
+  kn = 0;
+  for (int d = 0; d < 2; ++d) {
+    const int first = d == 0 ? f0 : f1, cnt = d == 0 ? c0 : c1;
+    for (int k = 0; k < cnt; ++k, ++kn) {
+      if (kn < KGRAD) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) avg[q] = minmod(avg[q], kept[kn][q]);
+      } else {
+        const long long gn = first + k;
+        double xm, w;
+        overlap(G, g0, gn, &xm, &w);
+        neighbour_grad(G, gn, xm, cr0, ct0, p0, m0, grad);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) avg[q] = minmod(avg[q], grad[q]);
+      }
     }
   }
 #pragma unroll
