@@ -332,7 +332,7 @@ def jet2d_arm(args, dev_index):
     s = problems.Jet2dSetup(**dict(JET2D, ntheta=args.ntheta))
     dump = {}
     ms, st, out, clk = _jet2d_run(s, args.steps, args.warmup, 0, dev_index,
-                                  after=lambda g: dump.update(_dump_timing(g, s)))
+                                  after=None if args.no_dump else (lambda g: dump.update(_dump_timing(g, s))))
     zones = st["zone_updates"]
     n = out.ntrack[2:-2]
     res = {"workload": f"{s.ntheta} theta tracks over [{s.th_min}, {s.th_max}] rad, BM cap below {s.th_jet} rad, "
@@ -403,7 +403,8 @@ def jet2d_arm(args, dev_index):
         dump["reference"] = {"cells": cells, "write_cells_per_s": cells / tw, "read_cells_per_s": cells / max(tr, 1e-9),
                              "note": "the reference's printCols / reinitialise on the 16-track wedge, one thread; "
                                      "its read time is the resume minus one printCols"}
-    res["dump"] = dump
+    if dump:
+        res["dump"] = dump
     return res
 
 
@@ -786,6 +787,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned cons2prim guess arm")
     ap.add_argument("--no-2d", action="store_true", help="skip the 2D (r, theta) workload")
     ap.add_argument("--no-sweep", action="store_true", help="skip the BM1D parameter sweep")
+    ap.add_argument("--no-dump", action="store_true", help="skip the 2D text dump and resume timing")
     ap.add_argument("--workload", default="all", choices=["all", "tubes", "jet2d", "sweep"],
                     help="one workload alone (profiling captures); 'all' prints the tube line with the others nested")
     ap.add_argument("--ntubes", type=int, default=NTUBES, help="smaller batches for profiling captures")

@@ -326,6 +326,7 @@ Phys phys_of(const gamma_2d_config_t &c) {
   p.vi = c.vi;
   p.eos = c.eos;
   p.ngst = c.ngst;
+  p.eos_ws = c.eos_wavespeeds;
   return p;
 }
 
@@ -807,7 +808,7 @@ GAMMA_API int gamma_2d_load(gamma_2d_t *ctx, const char *path) {
   uint32_t kind = 0;
   gamma_2d_config_t cfg;
   if (!in.block("kind", &kind, sizeof(kind)) || kind != gb::io::kCkpt2D) return GAMMA_ERR_IO;
-  if (!in.block("config", &cfg, sizeof(cfg)) || std::memcmp(&cfg, &c->cfg, sizeof(cfg)) != 0)
+  if (!in.block("config", &cfg, sizeof(cfg)) || !gb::io::same_config(cfg, c->cfg))
     return GAMMA_ERR_INVALID;
   std::vector<double> th(c->theta.size()), dth(c->dtheta.size());
   if (!in.block("theta", th.data(), th.size() * d) || !in.block("dtheta", dth.data(), dth.size() * d) ||

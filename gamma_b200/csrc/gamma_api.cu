@@ -83,6 +83,7 @@ gb::Phys phys_of(const gamma_config_t &c) {
   p.vi = c.vi;
   p.eos = c.eos;
   p.ngst = c.ngst;
+  p.eos_ws = c.eos_wavespeeds;
   return p;
 }
 
@@ -536,7 +537,7 @@ GAMMA_API int gamma_gpu_load(gamma_ctx_t *ctx, const char *path) {
   gamma_config_t cfg;
   std::vector<int> cap(R);
   if (!in.block("kind", &kind, sizeof(kind)) || kind != gb::io::kCkpt1D) return GAMMA_ERR_IO;
-  if (!in.block("config", &cfg, sizeof(cfg)) || std::memcmp(&cfg, &ctx->cfg, sizeof(cfg)) != 0)
+  if (!in.block("config", &cfg, sizeof(cfg)) || !gb::io::same_config(cfg, ctx->cfg))
     return GAMMA_ERR_INVALID;
   if (!in.block("capacity", cap.data(), R * sizeof(int)) || cap != ctx->cap) return GAMMA_ERR_INVALID;
   std::vector<gb::RunState> rs(R);

@@ -42,6 +42,7 @@ Phys phys_1d(const gamma_config_t &c) {
   p.vi = c.vi;
   p.eos = c.eos;
   p.ngst = c.ngst;
+  p.eos_ws = c.eos_wavespeeds;
   return p;
 }
 
@@ -53,6 +54,7 @@ Phys phys_2d(const gamma_2d_config_t &c) {
   p.vi = c.vi;
   p.eos = c.eos;
   p.ngst = c.ngst;
+  p.eos_ws = c.eos_wavespeeds;
   return p;
 }
 

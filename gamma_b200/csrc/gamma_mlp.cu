@@ -39,6 +39,7 @@ gb::Phys phys_of(const gamma_config_t &c) {
   p.vi = c.vi;
   p.eos = c.eos;
   p.ngst = c.ngst;
+  p.eos_ws = c.eos_wavespeeds;
   return p;
 }
 

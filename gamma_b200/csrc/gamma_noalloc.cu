@@ -121,7 +121,7 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
   T.run = reinterpret_cast<gb::RunState *>(runs);
   T.par = reinterpret_cast<const gb::RunParams *>(ws + off_par);
 
-  gb::Phys ph;
+  gb::Phys ph{};
   ph.gamma_ad = cfg->gamma_ad;
   ph.kgam = cfg->gamma_ad / (cfg->gamma_ad - 1.);
   ph.cfl = cfg->cfl;

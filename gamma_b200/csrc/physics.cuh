@@ -90,6 +90,8 @@ struct Phys {
   double vi;        // VI
   int eos;          // 0 ideal, 1 Synge / Taub-Mathews (rel_sph.cpp:37-52)
   int ngst;
+  int eos_ws;       // 1: each state's Gamma_eff in the wave speeds and the shock
+                    // detector too (the reference uses GAMMA_ there)
 };
 
 template <class Cfg>
@@ -430,14 +432,16 @@ struct Waves {
 // rel_cart.cpp:260-302 switches to the linear root when |FhllE| < 1e-15).
 template <class Cfg>
 GB_HD Waves compute_lambda_ref(const Phys &ph, const FState<Cfg> &L, const FState<Cfg> &R) {
-  const double G = ph.gamma_ad;
+  const bool ws = Cfg::SPH && ph.eos_ws;
+  const double GL = ws ? eos_gamma(ph, L.prim[RHO], L.prim[PPP]) : ph.gamma_ad;
+  const double GR = ws ? eos_gamma(ph, R.prim[RHO], R.prim[PPP]) : ph.gamma_ad;
   Waves w;
   double lfacL = L.lfac;
   double lfacR = R.lfac;
   double vL = L.v;
   double vR = R.v;
-  double cSL = sqrt(G * L.prim[PPP] / (L.prim[RHO] + L.prim[PPP] * G / (G - 1.)));
-  double cSR = sqrt(G * R.prim[PPP] / (R.prim[RHO] + R.prim[PPP] * G / (G - 1.)));
+  double cSL = sqrt(GL * L.prim[PPP] / (L.prim[RHO] + L.prim[PPP] * GL / (GL - 1.)));
+  double cSR = sqrt(GR * R.prim[PPP] / (R.prim[RHO] + R.prim[PPP] * GR / (GR - 1.)));
   double sgSL = cSL * cSL / (lfacL * lfacL * (1. - cSL * cSL));
   double sgSR = cSR * cSR / (lfacR * lfacR * (1. - cSR * cSR));
   double l1, l2;
@@ -477,7 +481,7 @@ GB_HD Waves compute_lambda_ref(const Phys &ph, const FState<Cfg> &L, const FStat
 
 template <class Cfg>
 GB_HD Waves compute_lambda(const Phys &ph, const FState<Cfg> &L, const FState<Cfg> &R) {
-  if (!Cfg::FAST) return compute_lambda_ref<Cfg>(ph, L, R);
+  if (!Cfg::FAST || ph.eos_ws) return compute_lambda_ref<Cfg>(ph, L, R);
   const double G = ph.gamma_ad;
   const double kg = ph.kgam;
   Waves w;
@@ -580,7 +584,8 @@ GB_HD void hllc_flux(const FState<Cfg> &L, const FState<Cfg> &R, const Waves &w,
 template <class Cfg>
 GB_HD bool compute_Sd(const Phys &ph, const FState<Cfg> &S1, const FState<Cfg> &S2, double *Sd,
                       double *pspec) {
-  const double G = ph.gamma_ad;
+  // with eos_ws, the upstream state's Gamma_eff throughout
+  const double G = (Cfg::SPH && ph.eos_ws) ? eos_gamma(ph, S1.prim[RHO], S1.prim[PPP]) : ph.gamma_ad;
   const int n_evals = 10;
   const double chi = 0.5;
   double p1 = S1.prim[PPP];

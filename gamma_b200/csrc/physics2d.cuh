@@ -108,14 +108,15 @@ struct Waves {
 // Interface::wavespeedEstimates + computeLambda (rel_sph.cpp:322-394) along
 // dim; d = r for the theta direction (the momentum is stored times r)
 GB_HD Waves compute_lambda(const Phys &ph, const St &L, const St &R, int dim, double xr) {
-  const double G = ph.gamma_ad;
+  const double GL = ph.eos_ws ? eos_gamma(ph, L.prim[RHO], L.prim[PPP]) : ph.gamma_ad;
+  const double GR = ph.eos_ws ? eos_gamma(ph, R.prim[RHO], R.prim[PPP]) : ph.gamma_ad;
   const int u = UU1 + dim, s = SS1 + dim;
   Waves w;
   double lfacL = L.lfac, lfacR = R.lfac;
   double vL = L.prim[u] / lfacL;
   double vR = R.prim[u] / lfacR;
-  double cSL = sqrt(G * L.prim[PPP] / (L.prim[RHO] + L.prim[PPP] * G / (G - 1.)));
-  double cSR = sqrt(G * R.prim[PPP] / (R.prim[RHO] + R.prim[PPP] * G / (G - 1.)));
+  double cSL = sqrt(GL * L.prim[PPP] / (L.prim[RHO] + L.prim[PPP] * GL / (GL - 1.)));
+  double cSR = sqrt(GR * R.prim[PPP] / (R.prim[RHO] + R.prim[PPP] * GR / (GR - 1.)));
   double sgSL = cSL * cSL / (lfacL * lfacL * (1. - cSL * cSL));
   double sgSR = cSR * cSR / (lfacR * lfacR * (1. - cSR * cSR));
   double l1, l2;
@@ -208,7 +209,8 @@ GB_HD void hllc_flux(const St &L, const St &R, const Waves &w, double v, double 
 // compute_Sd (radiation_sph.cpp:41-158) along dim, S1 upstream.  Returns false
 // where the reference returns -1 before reaching the spectral index.
 GB_HD bool compute_Sd(const Phys &ph, const St &S1, const St &S2, int dim, bool reverse, double *Sd) {
-  const double G = ph.gamma_ad;
+  // with eos_ws, the upstream state's Gamma_eff throughout
+  const double G = ph.eos_ws ? eos_gamma(ph, S1.prim[RHO], S1.prim[PPP]) : ph.gamma_ad;
   const int uux = UU1 + dim, uut = UU2 - dim;
   const int n_evals = 10;
   const double chi = 0.5;

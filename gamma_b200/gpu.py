@@ -50,7 +50,8 @@ class Config(ctypes.Structure):
 
     _fields_ = [(n, ctypes.c_int) for n in ("geometry", "hydro", "eos", "nq", "shock_detection",
                                              "local_synchrotron", "problem", "ngst")] + \
-               [(n, ctypes.c_double) for n in ("gamma_ad", "cfl", "vi")]
+               [(n, ctypes.c_double) for n in ("gamma_ad", "cfl", "vi")] + \
+               [("eos_wavespeeds", ctypes.c_int)]
 
 
 class RunParams(ctypes.Structure):
@@ -79,9 +80,12 @@ class MlpTrain(ctypes.Structure):
                 ("lr_final", ctypes.c_float), ("seed", ctypes.c_ulonglong)]
 
 
-def config_sph(gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=EOS_IDEAL) -> Config:
-    """spherical1D + rel_sph + radiation_sph, shock detection and local synchrotron (NUM_Q = 10)."""
-    return Config(GEOM_SPHERICAL1D, HYDRO_REL_SPH, eos, 10, 1, 1, PROBLEM_BM1D, 2, gamma_ad, cfl, vi)
+def config_sph(gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=EOS_IDEAL, eos_wavespeeds=0) -> Config:
+    """spherical1D + rel_sph + radiation_sph, shock detection and local synchrotron (NUM_Q = 10).
+    eos_wavespeeds=1 puts each state's Gamma_eff into the wave speeds and the
+    shock detector too (the reference uses GAMMA_ there)."""
+    return Config(GEOM_SPHERICAL1D, HYDRO_REL_SPH, eos, 10, 1, 1, PROBLEM_BM1D, 2, gamma_ad, cfl, vi,
+                  int(eos_wavespeeds))
 
 
 def config_cart(gamma_ad=5. / 3., cfl=0.2, vi=1.0) -> Config:

@@ -22,7 +22,7 @@ class Config2D(ctypes.Structure):
 
     _fields_ = [("ntheta", ctypes.c_int), ("nmax", ctypes.c_int), ("ngst", ctypes.c_int), ("nq", ctypes.c_int),
                 ("eos", ctypes.c_int), ("gamma_ad", ctypes.c_double), ("cfl", ctypes.c_double),
-                ("vi", ctypes.c_double)]
+                ("vi", ctypes.c_double), ("eos_wavespeeds", ctypes.c_int)]
 
 
 class Params2D(ctypes.Structure):
@@ -112,8 +112,9 @@ class Grid2DGPU:
     """One 2D run on the current CUDA device."""
 
     def __init__(self, ntheta: int, nmax: int, theta, dtheta, gamma_ad=4. / 3., cfl=0.2, vi=1.0,
-                 eos=gpu.EOS_IDEAL):
-        self.cfg = Config2D(int(ntheta), int(nmax), 2, NQ, int(eos), float(gamma_ad), float(cfl), float(vi))
+                 eos=gpu.EOS_IDEAL, eos_wavespeeds=0):
+        self.cfg = Config2D(int(ntheta), int(nmax), 2, NQ, int(eos), float(gamma_ad), float(cfl), float(vi),
+                            int(eos_wavespeeds))
         th = np.ascontiguousarray(theta, dtype=np.float64)
         dth = np.ascontiguousarray(dtheta, dtype=np.float64)
         assert th.size == ntheta and dth.size == ntheta
@@ -215,8 +216,9 @@ class Grid2DGPU:
         return s
 
 
-def _config(ntheta, nmax, gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=gpu.EOS_IDEAL) -> Config2D:
-    return Config2D(int(ntheta), int(nmax), 2, NQ, int(eos), float(gamma_ad), float(cfl), float(vi))
+def _config(ntheta, nmax, gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=gpu.EOS_IDEAL, eos_wavespeeds=0) -> Config2D:
+    return Config2D(int(ntheta), int(nmax), 2, NQ, int(eos), float(gamma_ad), float(cfl), float(vi),
+                    int(eos_wavespeeds))
 
 
 def text2d_write(path: str, s: State2D, theta, dtheta, **cfg):

@@ -63,6 +63,11 @@ typedef struct {
   double gamma_ad;
   double cfl;
   double vi;
+  /* 0: GAMMA_ in the wave speeds and the shock detector whatever the EOS, as
+   * the reference does (src/Hydro/rel_sph.cpp:331-334, radiation_sph.cpp:37-39);
+   * 1: each state's Gamma_eff there too (rel_sph.cpp:37-52), the Synge EOS end
+   * to end -- no counterpart in the reference.  No effect with the ideal EOS. */
+  int eos_wavespeeds;
 } gamma_config_t;
 
 /* Per-run parameters of the Blandford-McKee problem hooks
@@ -240,6 +245,7 @@ typedef struct {
   int nq;       /* 10 */
   int eos;      /* GAMMA_EOS_* */
   double gamma_ad, cfl, vi;
+  int eos_wavespeeds;  /* as in gamma_config_t */
 } gamma_2d_config_t;
 
 /* the problem module's constants (BM.cpp userKinematics, checkCellForRegrid)

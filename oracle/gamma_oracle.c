@@ -266,13 +266,15 @@ static int cons2prim(const oc_sim *s, fstate *St, double r, double pin) {
 
 /* Interface::wavespeedEstimates (rel_sph.cpp:322-350, identical in rel_cart) */
 static void wavespeeds(const oc_sim *s, iface *I) {
-  const double G = s->c.gamma_ad;
+  const int ws = s->c.eos_wavespeeds && s->sph;
+  const double GL = ws ? eos_gamma(s, I->SL.prim[RHO], I->SL.prim[PPP]) : s->c.gamma_ad;
+  const double GR = ws ? eos_gamma(s, I->SR.prim[RHO], I->SR.prim[PPP]) : s->c.gamma_ad;
   double lfacL = st_lfac(&I->SL);
   double lfacR = st_lfac(&I->SR);
   double vL = I->SL.prim[UU1] / lfacL;
   double vR = I->SR.prim[UU1] / lfacR;
-  double cSL = sqrt(G * I->SL.prim[PPP] / (I->SL.prim[RHO] + I->SL.prim[PPP] * G / (G - 1.)));
-  double cSR = sqrt(G * I->SR.prim[PPP] / (I->SR.prim[RHO] + I->SR.prim[PPP] * G / (G - 1.)));
+  double cSL = sqrt(GL * I->SL.prim[PPP] / (I->SL.prim[RHO] + I->SL.prim[PPP] * GL / (GL - 1.)));
+  double cSR = sqrt(GR * I->SR.prim[PPP] / (I->SR.prim[RHO] + I->SR.prim[PPP] * GR / (GR - 1.)));
   double sgSL = cSL * cSL / (lfacL * lfacL * (1. - cSL * cSL));
   double sgSR = cSR * cSR / (lfacR * lfacR * (1. - cSR * cSR));
   double l1, l2;
@@ -372,7 +374,8 @@ static void compute_flux(const oc_sim *s, iface *I) {
  * then an uninitialised local). */
 static int compute_Sd(const oc_sim *s, const fstate *S1, const fstate *S2, double *Sd_out,
                       double *pspec) {
-  const double G = s->c.gamma_ad;
+  /* with eos_wavespeeds, the upstream state's Gamma_eff throughout */
+  const double G = (s->c.eos_wavespeeds && s->sph) ? eos_gamma(s, S1->prim[RHO], S1->prim[PPP]) : s->c.gamma_ad;
   const int n_evals = 10;
   const double chi = 0.5;
   double p1 = S1->prim[PPP];

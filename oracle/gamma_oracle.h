@@ -50,6 +50,9 @@ typedef struct {
   /* relative bracket width at which the pressure root search stops: 1e-13 in
    * the reference (rel_sph.cpp:281); smaller values give a tighter oracle */
   double c2p_epsrel;
+  /* 1: Gamma_eff of each state in the wave speeds and the shock detector too
+   * (the reference uses GAMMA_ there whatever the EOS; 0 restates it) */
+  int eos_wavespeeds;
 } oc_config;
 
 typedef struct oc_sim oc_sim;
