@@ -492,6 +492,118 @@ def learned_arm(args, g, cfg, upload, stream, plain_out, rows, max_over_ranks, b
     }
 
 
+C2P_STATES = 1 << 24
+
+
+def c2p_states(n, seed=SEED):
+    """Seeded spherical-hydro states (NUM_Q = 10) over the learned guess's
+    training range: Lorentz factor log-uniform in [1, 1e3], p/rho in
+    [1e-10, 1e3], rho in [1e-6, 1e6]; their conserved variables (the
+    FluidState::prim2cons formulas, ideal gas, Gamma = 4/3, written out here)."""
+    rng = np.random.default_rng(seed + 5)
+    lfac = np.exp(rng.uniform(0., np.log(1e3), n))
+    rho = 10. ** rng.uniform(-6., 6., n)
+    p = rho * 10. ** rng.uniform(-10., 3., n)
+    u = np.sqrt(lfac * lfac - 1.) * rng.choice([-1., 1.], n)
+    prim = np.zeros((10, n))
+    prim[0], prim[1], prim[2], prim[4] = rho, p, u, 1.
+    G = 4. / 3.
+    h = 1. + p * G / (G - 1.) / rho
+    D = lfac * rho
+    cons = np.zeros((10, n))
+    cons[0], cons[1], cons[2], cons[4] = D, D * h * lfac - p - D, D * h * u, D
+    return prim, cons
+
+
+def _c2p_cpu_worker(args):
+    """The reference's own FluidState::cons2prim (GSL Brent through the shim) on
+    a slice of the states, from the same cold start."""
+    cons, prim0 = args
+    sys.path.insert(0, ROOT)
+    from oracle.refsim import RefSim
+    s = RefSim("bm1d")
+    t0 = time.perf_counter()
+    s.cons2prim(cons, prim0)
+    return cons.shape[1], time.perf_counter() - t0
+
+
+def c2p_arm(args, dev_index):
+    """FluidState::cons2prim on a batch of 16.8 M independent states with no
+    previous pressure (the start is p = 1): the plain Newton from that start,
+    and Newton from the learned guess (BF16 tensor-core inference fused into
+    the kernel), against each other and the reference's CPU routine."""
+    import torch
+
+    from gamma_b200 import gpu
+    n = args.c2p_states
+    prim, cons = c2p_states(n)
+    cold = prim.copy()
+    cold[1] = 1.
+    cfg = gpu.config_sph()
+    dev = torch.device("cuda", dev_index)
+    dcons0 = torch.tensor(cons, device=dev)
+    dcold = torch.tensor(cold, device=dev)
+    it = torch.zeros(n, dtype=torch.int32, device=dev)
+    # the network, trained on drawn states of the same range
+    nu = 2_000_000
+    x = torch.zeros((nu, 3), dtype=torch.float32, device=dev)
+    y = torch.zeros((nu, 2), dtype=torch.float32, device=dev)
+    gpu.mlp_pairs(cfg, 0, 0, nu, SEED + 6, x.data_ptr(), y.data_ptr())
+    P = torch.zeros(gpu.mlp_param_count(), dtype=torch.float32, device=dev)
+    gpu.mlp_init(P.data_ptr(), SEED)
+    t0 = time.perf_counter()
+    loss = gpu.mlp_train(P.data_ptr(), x.data_ptr(), y.data_ptr(), nu, epochs=6, batch=8192)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    res = {"workload": f"{n} independent spherical-hydro states (NUM_Q=10, Gamma=4/3), Lorentz factor log-uniform "
+                       "in [1,1e3], p/rho in [1e-10,1e3], rho in [1e-6,1e6]; cons2prim from p = 1",
+           "states": n, "unit": "states/s"}
+    out = {}
+    for name in ("plain", "learned"):
+        times = []
+        for k in range(max(args.warmup, 3) + args.steps):
+            dcons = dcons0.clone()
+            dprim = dcold.clone()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            if name == "plain":
+                gpu.cons2prim_device(cfg, dcons.data_ptr(), dprim.data_ptr(), n, it.data_ptr())
+            else:
+                gpu.cons2prim_guess_device(cfg, dcons.data_ptr(), dprim.data_ptr(), n, P.data_ptr(), it.data_ptr())
+            e1.record()
+            torch.cuda.synchronize()
+            if k >= max(args.warmup, 3):
+                times.append(e0.elapsed_time(e1))
+        iters = it.cpu().numpy()
+        out[name] = dprim.cpu().numpy()
+        ms = statistics.mean(times)
+        res[name] = {"value": n / (ms / 1e3), "ms": ms, "mean_newton_iters": float(iters.mean()),
+                     "max_newton_iters": int(iters.max()), "fallback_rate": float(np.mean(iters > 100))}
+        # per state: cons and the prim guess read, prim and the rewritten cons written
+        achieved = 4 * 10 * 8 * n / (ms / 1e3) / 1e9
+        peak, kind = measured_peak_hbm()
+        res[name]["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                 "frac": achieved / peak, "peak_source": kind, "bytes_per_state": 320}
+    for q, nm in ((0, "rho"), (1, "p"), (2, "u")):
+        a, b = out["learned"][q], out["plain"][q]
+        res.setdefault("l1_learned_vs_plain", {})[nm] = float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
+    res["speedup_learned"] = res["learned"]["value"] / res["plain"]["value"]
+    res["training"] = {"pairs": nu, "epochs": len(loss), "final_loss": float(loss[-1]), "seconds": train_s}
+    if not args.no_cpu_baseline and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_bm1d.so")):
+        import multiprocessing as mp
+        cores = os.cpu_count() or 1
+        m = 40_000 * cores
+        chunks = [(np.ascontiguousarray(cons[:, k:m:cores]), np.ascontiguousarray(cold[:, k:m:cores]))
+                  for k in range(cores)]
+        with mp.get_context("spawn").Pool(cores) as pool:
+            r = pool.map(_c2p_cpu_worker, chunks)
+        res["cpu_baseline"] = {"value": sum(a for a, _ in r) / max(t for _, t in r), "unit": "states/s",
+                               "cores": cores, "kind": "reference",
+                               "sample": f"the first {m} states, one process per core, from the same start"}
+    return res
+
+
 SWEEP_RUNS = 1024
 
 
@@ -667,6 +779,8 @@ def run_gpu_arm(args):
             res = jet2d_arm(args, local)
         elif args.workload == "sweep":
             res = sweep_arm(args, local, max_over_ranks, barrier, ws)
+        elif args.workload == "c2p":
+            res = c2p_arm(args, local)
         if args.workload != "tubes":
             if rank == 0:
                 print(json.dumps(dict({"metric": METRIC, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -765,6 +879,8 @@ def run_gpu_arm(args):
         line["jet2d"] = jet2d_arm(args, local)
     if not args.no_sweep and args.workload == "all":
         line["sweep"] = sweep_arm(args, local, max_over_ranks, barrier, ws)
+    if not args.no_c2p and args.workload == "all" and rank == 0:
+        line["c2p"] = c2p_arm(args, local)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         setups_cpu = setups
         cores = os.cpu_count() or 1
@@ -788,11 +904,13 @@ def main():
     ap.add_argument("--no-2d", action="store_true", help="skip the 2D (r, theta) workload")
     ap.add_argument("--no-sweep", action="store_true", help="skip the BM1D parameter sweep")
     ap.add_argument("--no-dump", action="store_true", help="skip the 2D text dump and resume timing")
-    ap.add_argument("--workload", default="all", choices=["all", "tubes", "jet2d", "sweep"],
+    ap.add_argument("--workload", default="all", choices=["all", "tubes", "jet2d", "sweep", "c2p"],
                     help="one workload alone (profiling captures); 'all' prints the tube line with the others nested")
     ap.add_argument("--ntubes", type=int, default=NTUBES, help="smaller batches for profiling captures")
     ap.add_argument("--ntheta", type=int, default=JET2D["ntheta"], help="theta tracks of the 2D workload")
     ap.add_argument("--sweep-runs", type=int, default=SWEEP_RUNS, help="runs of the BM1D sweep")
+    ap.add_argument("--c2p-states", type=int, default=C2P_STATES, help="states of the cons2prim batch")
+    ap.add_argument("--no-c2p", action="store_true", help="skip the cons2prim batch")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
