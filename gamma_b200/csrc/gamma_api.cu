@@ -12,6 +12,7 @@
 
 #include "io.h"
 #include "track_step.cuh"
+#include "tune.h"
 
 namespace {
 
@@ -41,6 +42,9 @@ struct gamma_ctx {
   size_t smem = 0;
   int grid_guess = 0;  // launch shape of the kernel with the learned guess
   size_t smem_guess = 0;
+  int variant = 0;     // step-kernel launch shape (tune.h); 0 = the default kernel
+  int vgrid[gb::tune::kVariants] = {};
+  size_t vsmem[gb::tune::kVariants] = {};
   std::string err;
 };
 
@@ -359,12 +363,25 @@ int run_steps(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats, int regri
   GB_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
   const bool guess = ctx->T.mlp != nullptr && !regrid_only;
   int rc;
-  if (ctx->kind == KIND_SPH)
+  if (!guess && ctx->variant > 0) {  // a tuned launch shape of the plain kernel
+    const int v = ctx->variant;
+    const cudaError_t e =
+        ctx->kind == KIND_SPH
+            ? gb::tune::launch_sph(v, ctx->vgrid[v], ctx->vsmem[v], ctx->stream, ctx->T, phys_of(ctx->cfg), nsteps,
+                                   ctx->d_order, ctx->nruns, ctx->d_queue, ctx->d_stats, regrid_only,
+                                   words_bytes(ctx->max_cap))
+            : gb::tune::launch_cart(v, ctx->vgrid[v], ctx->vsmem[v], ctx->stream, ctx->T, phys_of(ctx->cfg),
+                                    nsteps, ctx->d_order, ctx->nruns, ctx->d_queue, ctx->d_stats, regrid_only,
+                                    words_bytes(ctx->max_cap));
+    if (e != cudaSuccess) return fail_cuda(ctx, e, "variant launch");
+    rc = GAMMA_OK;
+  } else if (ctx->kind == KIND_SPH) {
     rc = guess ? launch_step<gb::CfgSph, true>(ctx, nsteps, regrid_only)
                : launch_step<gb::CfgSph, false>(ctx, nsteps, regrid_only);
-  else
+  } else {
     rc = guess ? launch_step<gb::CfgCart, true>(ctx, nsteps, regrid_only)
                : launch_step<gb::CfgCart, false>(ctx, nsteps, regrid_only);
+  }
   if (rc != GAMMA_OK) return rc;
   GB_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
   if (stats) {
@@ -573,6 +590,96 @@ GAMMA_API int gamma_gpu_load(gamma_ctx_t *ctx, const char *path) {
   GB_CUDA(ctx, cudaMemcpyAsync(ctx->d_order, order.data(), R * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return GAMMA_OK;
+}
+
+GAMMA_API int gamma_gpu_variant_info(int variant, int *threads, int *cells_per_thread) {
+  if (variant < 0 || variant >= gb::tune::kVariants) return GAMMA_ERR_INVALID;
+  if (threads) *threads = gb::tune::kShapes[variant].threads;
+  if (cells_per_thread) *cells_per_thread = gb::tune::kShapes[variant].cells_per_thread;
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_gpu_set_variant(gamma_ctx_t *ctx, int variant) {
+  if (!ctx || variant < 0 || variant >= gb::tune::kVariants) return GAMMA_ERR_INVALID;
+  if (variant > 0 && ctx->vgrid[variant] == 0) {
+    const cudaError_t e =
+        ctx->kind == KIND_SPH
+            ? gb::tune::configure_sph(variant, ctx->nruns, ctx->max_cap, &ctx->vgrid[variant], &ctx->vsmem[variant])
+            : gb::tune::configure_cart(variant, ctx->nruns, ctx->max_cap, &ctx->vgrid[variant],
+                                       &ctx->vsmem[variant]);
+    if (e != cudaSuccess) return fail_cuda(ctx, e, "variant set-up");
+  }
+  ctx->variant = variant;
+  return GAMMA_OK;
+}
+
+GAMMA_API int gamma_gpu_get_variant(const gamma_ctx_t *ctx) { return ctx ? ctx->variant : -1; }
+
+// Times nsteps steps of every launch shape from the current state, puts the
+// state back after each, and keeps the fastest.
+GAMMA_API int gamma_gpu_autotune(gamma_ctx_t *ctx, int nsteps, float *ms, int *chosen) {
+  if (!ctx || nsteps < 1) return GAMMA_ERR_INVALID;
+  if (ctx->T.mlp) return GAMMA_ERR_INVALID;  // the learned-guess kernel has one shape
+  const gb::Tracks &T = ctx->T;
+  const size_t N = (size_t)ctx->N, d = sizeof(double), R = (size_t)ctx->nruns;
+  struct Arr {
+    void *dev;
+    size_t bytes;
+  };
+  std::vector<Arr> arrs = {{T.prim, ctx->nqs * N * d}, {T.x, N * d},   {T.dx, N * d},
+                           {T.dtl, N * d},             {T.xI, N * d},  {T.run, R * sizeof(gb::RunState)}};
+  if (T.sd) {
+    arrs.push_back({T.sd, N * d});
+    arrs.push_back({T.pspec, N * d});
+    arrs.push_back({T.shocked, N});
+  }
+  std::vector<void *> saved(arrs.size(), nullptr);
+  auto release = [&]() {
+    for (void *p : saved)
+      if (p) cudaFree(p);
+  };
+  auto copy_all = [&](bool restore) -> cudaError_t {
+    for (size_t k = 0; k < arrs.size(); ++k) {
+      cudaError_t e = restore ? cudaMemcpyAsync(arrs[k].dev, saved[k], arrs[k].bytes, cudaMemcpyDeviceToDevice, ctx->stream)
+                              : cudaMemcpyAsync(saved[k], arrs[k].dev, arrs[k].bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
+  for (size_t k = 0; k < arrs.size(); ++k) {
+    const cudaError_t e = cudaMalloc(&saved[k], arrs[k].bytes);
+    if (e != cudaSuccess) {
+      release();
+      return fail_cuda(ctx, e, "autotune backup");
+    }
+  }
+  cudaError_t e = copy_all(false);
+  const int keep = ctx->variant;
+  int best = keep, rc = GAMMA_OK;
+  float best_ms = 0.f;
+  for (int v = 0; v < gb::tune::kVariants && rc == GAMMA_OK && e == cudaSuccess; ++v) {
+    if ((rc = gamma_gpu_set_variant(ctx, v)) != GAMMA_OK) break;
+    if ((rc = run_steps(ctx, nsteps, nullptr, 0)) != GAMMA_OK) break;
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) break;
+    float t = 0.f;
+    if ((e = cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1)) != cudaSuccess) break;
+    if (ms) ms[v] = t;
+    if (v == 0 || t < best_ms) {
+      best_ms = t;
+      best = v;
+    }
+    e = copy_all(true);
+  }
+  if (e == cudaSuccess) e = copy_all(true);  // the state the call found, whatever stopped the loop
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  release();
+  if (e != cudaSuccess) return fail_cuda(ctx, e, "autotune");
+  if (rc != GAMMA_OK) {
+    ctx->variant = keep;
+    return rc;
+  }
+  if (chosen) *chosen = best;
+  return gamma_gpu_set_variant(ctx, best);
 }
 
 GAMMA_API void gamma_gpu_destroy(gamma_ctx_t *ctx) {

@@ -88,18 +88,21 @@ __device__ __forceinline__ void calc_bm(const Phys &ph, const RunParams &P, doub
   *u = C_LIGHT * sqrt(1. - 1. / (lfac * lfac)) * lfac / P.vNorm;
 }
 
-template <class Cfg, int BS, bool GUESS = false>
+// BS threads advance one run; each sweep chunk holds CPT cells per thread
+// (CH = BS * CPT), which a thread takes in turn.
+template <class Cfg, int BS, bool GUESS = false, int CPT = 1>
 struct TrackStep {
   static constexpr int NQ = Cfg::NQ;
   static constexpr int NQS = Cfg::NQ - 1;
-  static constexpr int NC = BS + 3;  // staged cells per chunk: a-1 .. a+BS+1
+  static constexpr int CH = BS * CPT;  // cells and interfaces per chunk
+  static constexpr int NC = CH + 3;    // staged cells per chunk: a-1 .. a+CH+1
 
   struct Smem {
     double cp[NQS][NC];  // staged primitives
     double cx[NC], cdx[NC], cen[NC];
-    double fl[NQS][BS + 1];  // interface fluxes; slot 0 = carry (interface a-1)
-    double lL[BS + 1], lR[BS + 1], v[BS + 1];
-    double xold[BS + 1], xnew[BS + 1], xcmb[BS + 1];
+    double fl[NQS][CH + 1];  // interface fluxes; slot 0 = carry (interface a-1)
+    double lL[CH + 1], lR[CH + 1], v[CH + 1];
+    double xold[CH + 1], xnew[CH + 1], xcmb[CH + 1];
     double red[BS / 32];
     double edge[4];  // x, dx of the left and right edge cells this stage
     int ints[4];
@@ -283,8 +286,8 @@ struct TrackStep {
     const double w1 = stage == 2 ? 1. / 4. : 2. / 3.;
     double run_min = DT_INF;
 
-    for (int a = 0; a < n; a += BS) {
-      // ---- stage cells a-1 .. a+BS+1 (slot k <-> cell a-1+k); slot 0 is carried
+    for (int a = 0; a < n; a += CH) {
+      // ---- stage cells a-1 .. a+CH+1 (slot k <-> cell a-1+k); slot 0 is carried
       for (int k = tid + 1; k < NC; k += BS) {
         const int i = a - 1 + k;
         if (i < n) {
@@ -301,10 +304,13 @@ struct TrackStep {
       }
       __syncthreads();
 
-      // ---- interface i = a + tid
-      const int i = a + tid;
+      // ---- interfaces i = a + tid + u BS
+#pragma unroll 1
+      for (int u = 0; u < CPT; ++u) {
+      const int tt = tid + u * BS;
+      const int i = a + tt;
       const bool has_if = i <= n - 2;
-      const int c = tid + 1;  // slot of cell i
+      const int c = tt + 1;  // slot of cell i
       double myflux[NQ];
 #pragma unroll
       for (int q = 0; q < NQ; ++q) myflux[q] = 0.;
@@ -361,24 +367,30 @@ struct TrackStep {
       }
       // cell n-1 has no interface of its own; as for every cell, the shock
       // detector result of the last real interface is already in place.
-      sm.lL[tid + 1] = my_lL;
-      sm.lR[tid + 1] = my_lR;
-      sm.v[tid + 1] = my_v;
+      sm.lL[tt + 1] = my_lL;
+      sm.lR[tt + 1] = my_lR;
+      sm.v[tt + 1] = my_v;
       if (mode == 1) {
-        sm.xold[tid + 1] = my_xold;
-        sm.xnew[tid + 1] = my_xnew;
-        sm.xcmb[tid + 1] = my_xcmb;
+        sm.xold[tt + 1] = my_xold;
+        sm.xnew[tt + 1] = my_xnew;
+        sm.xcmb[tt + 1] = my_xcmb;
 #pragma unroll
-        for (int s = 0; s < NQS; ++s) sm.fl[s][tid + 1] = myflux[Slots<Cfg>::q_of(s)];
+        for (int s = 0; s < NQS; ++s) sm.fl[s][tt + 1] = myflux[Slots<Cfg>::q_of(s)];
+      }
       }
       __syncthreads();
 
-      // ---- cell i = a + tid
+      // ---- cells i = a + tid + u BS
+#pragma unroll 1
+      for (int u = 0; u < CPT; ++u) {
+      const int tt = tid + u * BS;
+      const int i = a + tt;
+      const int c = tt + 1;
       if (i < n) {
         const long long g = off + i;
         if (i >= 1 && i <= n - 2 && (mode == 0 || stage > 1)) {
           double cand;
-          if (!dt_candidate(sm.cdx[c], sm.lR[tid], sm.v[tid + 1], sm.lL[tid + 1], sm.v[tid], &cand)) {
+          if (!dt_candidate(sm.cdx[c], sm.lR[tt], sm.v[tt + 1], sm.lL[tt + 1], sm.v[tt], &cand)) {
             st.status = 30;
             cand = DT_INF;
           }
@@ -419,7 +431,7 @@ struct TrackStep {
 #pragma unroll
           for (int s = 0; s < NQS; ++s) {
             const int q = Slots<Cfg>::q_of(s);
-            cons[q] += (sm.fl[s][tid] - sm.fl[s][tid + 1]) * dt;
+            cons[q] += (sm.fl[s][tt] - sm.fl[s][tt + 1]) * dt;
           }
           if (Cfg::SPH) {  // Cell::sourceTerms, 1D (rel_sph.cpp:452-466)
             double p = prim[PPP];
@@ -433,7 +445,7 @@ struct TrackStep {
             cons[GMX] += dg;
             cons[GMN] += dg;
           }
-          G1 = geom_between<Cfg>(sm.xnew[tid], sm.xnew[tid + 1]);
+          G1 = geom_between<Cfg>(sm.xnew[tt], sm.xnew[tt + 1]);
           if (Cfg::FAST) {
             const double rdV1 = 1. / G1.dV;
 #pragma unroll
@@ -455,7 +467,7 @@ struct TrackStep {
               const int q = Slots<Cfg>::q_of(s);
               cons[q] = w0 * T.u0[s * T.N + g] + w1 * cons[q] * G1.dV;
             }
-            const Geom G2 = geom_between<Cfg>(sm.xcmb[tid], sm.xcmb[tid + 1]);
+            const Geom G2 = geom_between<Cfg>(sm.xcmb[tt], sm.xcmb[tt + 1]);
             if (Cfg::FAST) {
               const double rdV2 = 1. / G2.dV;
 #pragma unroll
@@ -478,22 +490,23 @@ struct TrackStep {
           store_prim(T, g, prim);
         }
       }
+      }
       __syncthreads();
-      // ---- carry cell a+BS-1 and interface a+BS-1 to the next chunk
+      // ---- carry cell a+CH-1 and interface a+CH-1 to the next chunk
       if (tid == 0) {
-        sm.lL[0] = sm.lL[BS];
-        sm.lR[0] = sm.lR[BS];
-        sm.v[0] = sm.v[BS];
-        sm.xold[0] = sm.xold[BS];
-        sm.xnew[0] = sm.xnew[BS];
-        sm.xcmb[0] = sm.xcmb[BS];
-        sm.cx[0] = sm.cx[BS];
-        sm.cdx[0] = sm.cdx[BS];
-        sm.cen[0] = sm.cen[BS];
+        sm.lL[0] = sm.lL[CH];
+        sm.lR[0] = sm.lR[CH];
+        sm.v[0] = sm.v[CH];
+        sm.xold[0] = sm.xold[CH];
+        sm.xnew[0] = sm.xnew[CH];
+        sm.xcmb[0] = sm.xcmb[CH];
+        sm.cx[0] = sm.cx[CH];
+        sm.cdx[0] = sm.cdx[CH];
+        sm.cen[0] = sm.cen[CH];
       }
       if (tid < NQS) {
-        sm.fl[tid][0] = sm.fl[tid][BS];
-        sm.cp[tid][0] = sm.cp[tid][BS];
+        sm.fl[tid][0] = sm.fl[tid][CH];
+        sm.cp[tid][0] = sm.cp[tid][CH];
       }
       __syncthreads();
     }
@@ -617,11 +630,11 @@ struct TrackStep {
 
 // Dynamic shared memory: TrackStep::Smem, the regrid bit words (words_bytes),
 // then, with GUESS, the tensor-core weights of the learned guess.
-template <class Cfg, int BS, bool GUESS = false>
-__global__ void __launch_bounds__(BS, Cfg::MIN_BLOCKS)
+template <class Cfg, int BS, bool GUESS = false, int CPT = 1, int MINB = Cfg::MIN_BLOCKS>
+__global__ void __launch_bounds__(BS, MINB)
     track_step_kernel(Tracks T, Phys ph, int nsteps, const int *order, int nruns, int *queue, StepStats *stats,
                       int regrid_only, unsigned words_bytes) {
-  using TS = TrackStep<Cfg, BS, GUESS>;
+  using TS = TrackStep<Cfg, BS, GUESS, CPT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typename TS::Smem &sm = *reinterpret_cast<typename TS::Smem *>(smem_raw);
   uint32_t *words = reinterpret_cast<uint32_t *>(smem_raw + sizeof(typename TS::Smem));

@@ -36,6 +36,7 @@ EXPORTS = (
     "gamma_mlp_loss_grad",
     "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess",
     "gamma_text1d_write", "gamma_text1d_read", "gamma_gpu_print_cols", "gamma_gpu_save", "gamma_gpu_load",
+    "gamma_gpu_variant_info", "gamma_gpu_set_variant", "gamma_gpu_get_variant", "gamma_gpu_autotune",
 )
 
 
@@ -141,6 +142,10 @@ def lib() -> ctypes.CDLL:
         L.gamma_text1d_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config), ctypes.c_int, _ip, _lp, _dp,
                                         _dp, _dp, _dp, _dp]
         L.gamma_gpu_print_cols.argtypes = [v, ctypes.c_int, ctypes.c_char_p]
+        L.gamma_gpu_variant_info.argtypes = [ctypes.c_int, _ip, _ip]
+        L.gamma_gpu_set_variant.argtypes = [v, ctypes.c_int]
+        L.gamma_gpu_get_variant.argtypes = [v]
+        L.gamma_gpu_autotune.argtypes = [v, ctypes.c_int, ctypes.POINTER(ctypes.c_float), _ip]
         L.gamma_gpu_save.argtypes = [v, ctypes.c_char_p]
         L.gamma_gpu_load.argtypes = [v, ctypes.c_char_p]
         for name in ("gamma_gpu_create", "gamma_gpu_layout", "gamma_gpu_set_params", "gamma_gpu_upload",
@@ -148,7 +153,8 @@ def lib() -> ctypes.CDLL:
                      "gamma_mlp_param_count", "gamma_mlp_init", "gamma_mlp_pairs", "gamma_mlp_train",
                      "gamma_mlp_forward", "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess", "gamma_mlp_loss_grad",
                      "gamma_text1d_write", "gamma_text1d_read", "gamma_gpu_print_cols", "gamma_gpu_save",
-                     "gamma_gpu_load"):
+                     "gamma_gpu_load", "gamma_gpu_variant_info", "gamma_gpu_set_variant", "gamma_gpu_get_variant",
+                     "gamma_gpu_autotune"):
             getattr(L, name).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -254,6 +260,22 @@ class GammaGPU:
         it = int(self.download()["it"][run])
         return os.path.join(directory, f"phys{it:010d}.out")
 
+    def set_variant(self, variant: int):
+        """Launch shape of the step kernel (variant_info); results do not change."""
+        self._check(lib().gamma_gpu_set_variant(self.h, int(variant)))
+
+    @property
+    def variant(self) -> int:
+        return int(lib().gamma_gpu_get_variant(self.h))
+
+    def autotune(self, nsteps: int = 3):
+        """Times nsteps steps of every launch shape on the current state (which
+        it restores) and keeps the fastest; returns (ms per variant, chosen)."""
+        ms = (ctypes.c_float * N_VARIANTS)()
+        ch = ctypes.c_int()
+        self._check(lib().gamma_gpu_autotune(self.h, int(nsteps), ms, ctypes.byref(ch)))
+        return [float(x) for x in ms], int(ch.value)
+
     def save(self, path: str):
         """Exact checkpoint of every run."""
         self._check(lib().gamma_gpu_save(self.h, path.encode()))
@@ -269,6 +291,16 @@ class GammaGPU:
         self._check(lib().gamma_gpu_download(self.h, _p(nt, _ip), None, None, None, None, c(prim_ptr), c(x_ptr),
                                              c(dx_ptr), c(dtl_ptr), c(xI_ptr)))
         return nt
+
+
+N_VARIANTS = 6
+
+
+def variant_info(variant: int):
+    """(threads per run, cells per thread per sweep chunk) of a launch shape."""
+    a, b = ctypes.c_int(), ctypes.c_int()
+    _ok(lib().gamma_gpu_variant_info(int(variant), ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value
 
 
 def text1d_write(path: str, cfg: Config, prim, x, dx, it: int, t: float):

@@ -308,6 +308,22 @@ void gamma_2d_destroy(gamma_2d_t *ctx);
 /* The context's CUDA stream (a cudaStream_t). */
 void *gamma_gpu_stream(gamma_ctx_t *ctx);
 
+/* ---- Launch shapes of the step kernel, and their autotuner ------------------
+ * No counterpart in the reference (its 1D step is one thread's loop).  A
+ * variant fixes the threads that advance one run (the CTA size) and the cells
+ * each thread takes per sweep chunk; variant 0 is the default (128 threads,
+ * one cell).  Every variant computes every cell the same way, so results are
+ * identical; only the speed depends on the batch (track lengths, run count).
+ * The learned-guess step always uses variant 0. */
+int gamma_gpu_variant_info(int variant, int *threads, int *cells_per_thread);
+int gamma_gpu_set_variant(gamma_ctx_t *ctx, int variant);
+int gamma_gpu_get_variant(const gamma_ctx_t *ctx);
+
+/* Times nsteps steps of every variant on the context's current state (ms[v],
+ * may be NULL), restores that state after each, and keeps the fastest
+ * (*chosen).  Allocates a copy of the state for the duration of the call. */
+int gamma_gpu_autotune(gamma_ctx_t *ctx, int nsteps, float *ms, int *chosen);
+
 /* ---- Snapshots -------------------------------------------------------------
  * Text: the reference's dump columns and its resume reader, so that files move
  * between this library and the reference both ways.  The reference names a

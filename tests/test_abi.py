@@ -36,3 +36,12 @@ def test_strerror_and_invalid_config_without_device():
     caps = (ctypes.c_int * 1)(64)
     rc = gpu.lib().gamma_gpu_create(ctypes.byref(bad), 1, caps, ctypes.byref(h))
     assert rc in (gpu.GAMMA_ERR_INVALID, gpu.GAMMA_ERR_NO_DEVICE)
+
+
+def test_variant_table_matches_binding():
+    """the launch-shape table of the library has the binding's size"""
+    from gamma_b200 import gpu
+    assert gpu.variant_info(0) == (128, 1)
+    assert gpu.variant_info(gpu.N_VARIANTS - 1)[0] > 0
+    with pytest.raises(gpu.GammaError):
+        gpu.variant_info(gpu.N_VARIANTS)
