@@ -408,6 +408,19 @@ def jet2d_arm(args, dev_index):
     return res
 
 
+def autotune(g, args):
+    """The step kernel's launch shape picked on the live state (gamma_gpu_autotune:
+    3 one-step launches per shape, state restored), outside the timed region."""
+    from gamma_b200 import gpu
+    if args.no_tune:
+        return {"threads": 128, "cells_per_thread": 1, "tuned": False}
+    ms, v = g.autotune(3)
+    th, cpt = gpu.variant_info(v)
+    return {"threads": th, "cells_per_thread": cpt, "tuned": True,
+            "ms_per_3_steps": {f"{a}x{b}": round(m, 3) for m, (a, b) in
+                               zip(ms, (gpu.variant_info(k) for k in range(gpu.N_VARIANTS)))}}
+
+
 def train_guess(cfg, prim, rows_live, seed):
     """Train the learned cons2prim starting pressure on device.
 
@@ -692,6 +705,7 @@ def sweep_arm(args, dev_index, max_over_ranks, barrier, ws):
     upload()
     for _ in range(max(args.warmup, 3)):
         g.step(1, stats=False)
+    tune = autotune(g, args)
     stats0 = g.step(1)
     assert stats0["status"] == 0, stats0
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
@@ -740,7 +754,7 @@ def sweep_arm(args, dev_index, max_over_ranks, barrier, ws):
            "c2p": {"mean_newton_iters": stats0["c2p_iters"] / max(stats0["c2p_calls"], 1),
                    "max_newton_iters": stats0["c2p_max_iters"], "fallbacks": stats0["c2p_fallbacks"]},
            "regrid_per_step": {"splits": stats0["splits"], "merges": stats0["merges"]},
-           "clocks": clk.summary(), "gpu_launches": args.steps}
+           "clocks": clk.summary(), "gpu_launches": args.steps, "launch_shape": tune}
     if not args.no_learned:
         res["learned_guess"] = learned_arm(args, g, cfg, upload, stream, plain_out, (0, 1, 2, 4, 5, 6, 7, 8, 9),
                                            max_over_ranks, barrier, ws, stats0)
@@ -810,6 +824,7 @@ def run_gpu_arm(args):
     upload()
     for _ in range(args.warmup):
         g.step(1, stats=False)
+    tune = autotune(g, args)
     torch.cuda.synchronize()
     stats0 = g.step(1)  # one step with statistics, outside the timed region
     assert stats0["status"] == 0, stats0
@@ -867,6 +882,7 @@ def run_gpu_arm(args):
                      "traffic": None if tz is None else tz * zones_per_step},
         "clocks": clk.summary(),
         "gpu_launches": args.steps,
+        "launch_shape": tune,
         "c2p": {"mean_newton_iters": stats0["c2p_iters"] / max(stats0["c2p_calls"], 1),
                 "max_newton_iters": stats0["c2p_max_iters"], "fallbacks": stats0["c2p_fallbacks"]},
     }
@@ -904,6 +920,7 @@ def main():
     ap.add_argument("--no-2d", action="store_true", help="skip the 2D (r, theta) workload")
     ap.add_argument("--no-sweep", action="store_true", help="skip the BM1D parameter sweep")
     ap.add_argument("--no-dump", action="store_true", help="skip the 2D text dump and resume timing")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape of the 1D step")
     ap.add_argument("--workload", default="all", choices=["all", "tubes", "jet2d", "sweep", "c2p"],
                     help="one workload alone (profiling captures); 'all' prints the tube line with the others nested")
     ap.add_argument("--ntubes", type=int, default=NTUBES, help="smaller batches for profiling captures")

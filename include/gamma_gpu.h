@@ -319,9 +319,10 @@ int gamma_gpu_variant_info(int variant, int *threads, int *cells_per_thread);
 int gamma_gpu_set_variant(gamma_ctx_t *ctx, int variant);
 int gamma_gpu_get_variant(const gamma_ctx_t *ctx);
 
-/* Times nsteps steps of every variant on the context's current state (ms[v],
- * may be NULL), restores that state after each, and keeps the fastest
- * (*chosen).  Allocates a copy of the state for the duration of the call. */
+/* Times nsteps launches of one step each with every variant on the context's
+ * current state (ms[v], may be NULL), restores that state after each, and
+ * keeps the fastest (*chosen); another variant must beat variant 0 by 3%.
+ * Allocates a copy of the state for the duration of the call. */
 int gamma_gpu_autotune(gamma_ctx_t *ctx, int nsteps, float *ms, int *chosen);
 
 /* ---- Snapshots -------------------------------------------------------------

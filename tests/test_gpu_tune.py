@@ -64,7 +64,8 @@ def test_autotune_restores_the_state_and_keeps_the_fastest(gpu_available):
     before = g.download()
     ms, chosen = g.autotune(4)
     assert len(ms) == gpu.N_VARIANTS and all(t > 0 for t in ms)
-    assert chosen == int(np.argmin(ms)) and g.variant == chosen
+    assert g.variant == chosen and ms[chosen] <= ms[0]
+    assert chosen == 0 or ms[chosen] < 0.97 * ms[0]
     _same(before, g.download(), g.offsets)  # the state it timed is put back
     g.step(10)
     a = g.download()
