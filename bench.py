@@ -412,6 +412,10 @@ def autotune(g, args):
     """The step kernel's launch shape picked on the live state (gamma_gpu_autotune:
     3 one-step launches per shape, state restored), outside the timed region."""
     from gamma_b200 import gpu
+    if args.variant is not None:
+        g.set_variant(args.variant)
+        th, cpt = gpu.variant_info(args.variant)
+        return {"threads": th, "cells_per_thread": cpt, "tuned": False}
     if args.no_tune:
         return {"threads": 128, "cells_per_thread": 1, "tuned": False}
     ms, v = g.autotune(3)
@@ -921,6 +925,7 @@ def main():
     ap.add_argument("--no-sweep", action="store_true", help="skip the BM1D parameter sweep")
     ap.add_argument("--no-dump", action="store_true", help="skip the 2D text dump and resume timing")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape of the 1D step")
+    ap.add_argument("--variant", type=int, default=None, help="a fixed launch shape of the 1D step (no tuning)")
     ap.add_argument("--workload", default="all", choices=["all", "tubes", "jet2d", "sweep", "c2p"],
                     help="one workload alone (profiling captures); 'all' prints the tube line with the others nested")
     ap.add_argument("--ntubes", type=int, default=NTUBES, help="smaller batches for profiling captures")
