@@ -13,14 +13,14 @@
 namespace gb {
 namespace tune {
 
-constexpr int kVariants = 6;  // variant 0 included
+constexpr int kVariants = 8;  // variant 0 included
 
 struct Shape {
   int threads, cells_per_thread;
 };
 
 // threads per run and cells per thread of each variant
-constexpr Shape kShapes[kVariants] = {{128, 1}, {64, 1}, {256, 1}, {128, 2}, {64, 2}, {128, 4}};
+constexpr Shape kShapes[kVariants] = {{128, 1}, {64, 1}, {256, 1}, {128, 2}, {64, 2}, {128, 4}, {512, 1}, {256, 2}};
 
 // the register cap of each variant keeps the default's resident warps per SM
 constexpr int min_blocks(int default_blocks, int threads) {

@@ -54,6 +54,8 @@ cudaError_t GB_TUNE_CONFIGURE(int v, int nruns, int max_cap, int *grid, size_t *
     case 3: return configure_v<3>(nruns, max_cap, grid, smem);
     case 4: return configure_v<4>(nruns, max_cap, grid, smem);
     case 5: return configure_v<5>(nruns, max_cap, grid, smem);
+    case 6: return configure_v<6>(nruns, max_cap, grid, smem);
+    case 7: return configure_v<7>(nruns, max_cap, grid, smem);
   }
   return cudaErrorInvalidValue;
 }
@@ -66,6 +68,8 @@ cudaError_t GB_TUNE_LAUNCH(int v, int grid, size_t smem, cudaStream_t s, const T
     case 3: return launch_v<3>(grid, smem, s, T, ph, nsteps, order, nruns, queue, stats, regrid_only, wb);
     case 4: return launch_v<4>(grid, smem, s, T, ph, nsteps, order, nruns, queue, stats, regrid_only, wb);
     case 5: return launch_v<5>(grid, smem, s, T, ph, nsteps, order, nruns, queue, stats, regrid_only, wb);
+    case 6: return launch_v<6>(grid, smem, s, T, ph, nsteps, order, nruns, queue, stats, regrid_only, wb);
+    case 7: return launch_v<7>(grid, smem, s, T, ph, nsteps, order, nruns, queue, stats, regrid_only, wb);
   }
   return cudaErrorInvalidValue;
 }

@@ -293,7 +293,7 @@ class GammaGPU:
         return nt
 
 
-N_VARIANTS = 6
+N_VARIANTS = 8
 
 
 def variant_info(variant: int):
