@@ -321,7 +321,7 @@ def _active_cells(out):
     return np.concatenate([np.arange(o[j] + 2, o[j] + int(out.ntrack[j]) - 2) for j in range(2, out.NJ - 2)])
 
 
-def jet2d_arm(args, dev_index):
+def jet2d_arm(args, dev_index, host_work=True):
     """2D (r, theta) blast wave with a jet-like cap: 512 theta tracks over
     [0, 0.2] rad, BM profile (Gamma_shock^2 = 2e4) inside 0.1 rad, cold ambient
     outside, the reference problem module's regrid ratios (tracks settle at a
@@ -331,8 +331,11 @@ def jet2d_arm(args, dev_index):
     from gamma_b200 import gpu, problems
     s = problems.Jet2dSetup(**dict(JET2D, ntheta=args.ntheta))
     dump = {}
+    # host-side measurements (dump timing, CPU baselines) on one rank of one GPU only
+    host_work = host_work and not args.no_cpu_baseline
     ms, st, out, clk = _jet2d_run(s, args.steps, args.warmup, 0, dev_index,
-                                  after=None if args.no_dump else (lambda g: dump.update(_dump_timing(g, s))))
+                                  after=None if (args.no_dump or not host_work)
+                                  else (lambda g: dump.update(_dump_timing(g, s))))
     zones = st["zone_updates"]
     n = out.ntrack[2:-2]
     res = {"workload": f"{s.ntheta} theta tracks over [{s.th_min}, {s.th_max}] rad, BM cap below {s.th_jet} rad, "
@@ -377,7 +380,7 @@ def jet2d_arm(args, dev_index):
                     "warm start); Newton still converges to the reference tolerance"}
         del P
     lib = os.path.join(ROOT, "oracle", "_ref", "libref_jet2d.so")
-    if not args.no_cpu_baseline and os.path.exists(lib):
+    if host_work and os.path.exists(lib):
         import multiprocessing as mp
         # a 16-track wedge with 1,200 initial cells per track (the reference moves
         # whole Cell records for every merge, so its first regrid grows with the
@@ -389,7 +392,7 @@ def jet2d_arm(args, dev_index):
         res["cpu_baseline"] = {"value": z / t, "unit": "zone-updates/s", "cores": 1, "kind": "reference",
                                "sample": "the same wedge with 16 tracks of 1,200 initial cells, 10 steps after 3 "
                                          "warm-up steps, one thread"}
-    if not args.no_cpu_baseline and os.path.exists(lib.replace("jet2d.so", "jet2d_io.so")):
+    if host_work and os.path.exists(lib.replace("jet2d.so", "jet2d_io.so")):
         import multiprocessing as mp
         import shutil
         import tempfile
@@ -544,7 +547,7 @@ def _c2p_cpu_worker(args):
     return cons.shape[1], time.perf_counter() - t0
 
 
-def c2p_arm(args, dev_index):
+def c2p_arm(args, dev_index, host_work=True):
     """FluidState::cons2prim on a batch of 16.8 M independent states with no
     previous pressure (the start is p = 1): the plain Newton from that start,
     and Newton from the learned guess (BF16 tensor-core inference fused into
@@ -607,7 +610,8 @@ def c2p_arm(args, dev_index):
         res.setdefault("l1_learned_vs_plain", {})[nm] = float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
     res["speedup_learned"] = res["learned"]["value"] / res["plain"]["value"]
     res["training"] = {"pairs": nu, "epochs": len(loss), "final_loss": float(loss[-1]), "seconds": train_s}
-    if not args.no_cpu_baseline and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_bm1d.so")):
+    if host_work and not args.no_cpu_baseline and os.path.exists(os.path.join(ROOT, "oracle", "_ref",
+                                                                              "libref_bm1d.so")):
         import multiprocessing as mp
         cores = os.cpu_count() or 1
         m = 40_000 * cores
@@ -902,11 +906,11 @@ def run_gpu_arm(args):
                                             max_over_ranks, barrier, ws, stats0)
     g.close()
     if not args.no_2d and args.workload == "all":
-        line["jet2d"] = jet2d_arm(args, local)
+        line["jet2d"] = jet2d_arm(args, local, host_work=(ws == 1 and rank == 0))
     if not args.no_sweep and args.workload == "all":
         line["sweep"] = sweep_arm(args, local, max_over_ranks, barrier, ws)
     if not args.no_c2p and args.workload == "all" and rank == 0:
-        line["c2p"] = c2p_arm(args, local)
+        line["c2p"] = c2p_arm(args, local, host_work=(ws == 1))
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         setups_cpu = setups
         cores = os.cpu_count() or 1
