@@ -779,6 +779,24 @@ def sweep_arm(args, dev_index, max_over_ranks, barrier, ws):
     return res
 
 
+def rank_sync(ws, device):
+    """Replicas only: the ranks share no data, only a barrier around each timed
+    region and the slowest rank's time (all-reduce MAX)."""
+    import torch
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], device=device, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+    return barrier, max_over_ranks
+
+
 def run_gpu_arm(args):
     import torch
 
@@ -791,16 +809,7 @@ def run_gpu_arm(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
 
-    def barrier():
-        if ws > 1:
-            torch.distributed.barrier()
-
-    def max_over_ranks(x):
-        if ws == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = rank_sync(ws, "cuda")
 
     if args.workload != "all":  # one workload alone, as its own line (profiling captures)
         if args.workload == "jet2d":
