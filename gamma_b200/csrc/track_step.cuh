@@ -103,6 +103,7 @@ struct TrackStep {
     double fl[NQS][CH + 1];  // interface fluxes; slot 0 = carry (interface a-1)
     double lL[CH + 1], lR[CH + 1], v[CH + 1];
     double xold[CH + 1], xnew[CH + 1], xcmb[CH + 1];
+    double gp[Cfg::FAST ? 1 : NQS][Cfg::FAST ? 1 : NC];  // gradient between slots k and k+1 (grad())
     double red[BS / 32];
     double edge[4];  // x, dx of the left and right edge cells this stage
     int ints[4];
@@ -223,10 +224,10 @@ struct TrackStep {
           gN = (qR - qL) * r2;
           gL = (qL - qLL) * r1;
           gR = (qRR - qR) * r3;
-        } else {  // grad() of 1d.cpp:262-274
-          gN = (qR - qL) / d2;
-          gL = (qL - qLL) / d1;
-          gR = (qRR - qR) / d3;
+        } else {  // grad() of 1d.cpp:262-274, formed once per cell pair (pair_gradients)
+          gN = sm.gp[s][c];
+          gL = sm.gp[s][c - 1];
+          gR = sm.gp[s][c + 1];
         }
         gL = minmod(gL, gN);
         gR = minmod(gR, gN);
@@ -303,6 +304,18 @@ struct TrackStep {
         }
       }
       __syncthreads();
+      if (!Cfg::FAST && !(mode == 1 && stage == 1)) {
+        // grad() between staged cells k and k+1: (q[k+1] - q[k]) / (cen[k+1] - cen[k]),
+        // each used by the three interfaces around it (slots past the track end unused)
+        for (int k = tid; k < NC - 1; k += BS) {
+          if ((a > 0 || k > 0) && a + k < n) {  // slots k and k+1 both hold cells
+            const double d = sm.cen[k + 1] - sm.cen[k];
+#pragma unroll
+            for (int s = 0; s < NQS; ++s) sm.gp[s][k] = (sm.cp[s][k + 1] - sm.cp[s][k]) / d;
+          }
+        }
+        __syncthreads();
+      }
 
       // ---- interfaces i = a + tid + u BS
 #pragma unroll 1
