@@ -26,10 +26,27 @@ using namespace gb::d2;
 namespace {
 
 constexpr int kThreads = 256;
-// resident blocks per SM asked of the heavy per-cell passes (interface solves,
-// cell update): their FP64 latency needs warps more than registers
+// resident blocks per SM asked of the heavy per-cell passes: their FP64 and
+// load latency needs warps more than registers (measured per pass at 512
+// tracks: 3 for the r interfaces and the transverse gradients, 4 for the
+// theta gather and the cell update, 2 for the theta interfaces)
 #ifndef GB2_MINB
 #define GB2_MINB 2
+#endif
+#ifndef GB2_MINB_MV
+#define GB2_MINB_MV 3
+#endif
+#ifndef GB2_MINB_TG
+#define GB2_MINB_TG 3
+#endif
+#ifndef GB2_MINB_F1
+#define GB2_MINB_F1 GB2_MINB
+#endif
+#ifndef GB2_MINB_GA
+#define GB2_MINB_GA 4
+#endif
+#ifndef GB2_MINB_UP
+#define GB2_MINB_UP 4
 #endif
 
 struct Stats2 {
@@ -159,7 +176,7 @@ __device__ __forceinline__ void cell_at(const Grid2 &G, long long g, int *j, int
        g_ += (long long)gridDim.x * blockDim.x)                                                     \
     if (int j = 0, i = 0; cell_at((G), g_, &j, &i), true)
 
-__global__ void __launch_bounds__(kThreads, GB2_MINB) k_mv(Phys ph, Params2 P, Grid2 G) {
+__global__ void __launch_bounds__(kThreads, GB2_MINB_MV) k_mv(Phys ph, Params2 P, Grid2 G) {
   const long long it = *G.it;
   FOR_LIVE_CELLS(G, j, i) mv_interface(ph, P, G, j, i, it);
 }
@@ -177,15 +194,15 @@ __global__ void k_stale(Grid2 G) {
   if (j <= G.NJ - 2) stale_append(G, j);
 }
 
-__global__ void __launch_bounds__(kThreads, GB2_MINB) k_tgrad(Grid2 G) {
+__global__ void __launch_bounds__(kThreads, GB2_MINB_TG) k_tgrad(Grid2 G) {
   FOR_LIVE_CELLS(G, j, i) trans_grad(G, j, i);
 }
 
-__global__ void __launch_bounds__(kThreads, GB2_MINB) k_f1own(Phys ph, Grid2 G) {
+__global__ void __launch_bounds__(kThreads, GB2_MINB_F1) k_f1own(Phys ph, Grid2 G) {
   FOR_LIVE_CELLS(G, j, i) f1_own(ph, G, j, i);
 }
 
-__global__ void __launch_bounds__(kThreads, GB2_MINB) k_f1gather(Phys ph, Grid2 G) {
+__global__ void __launch_bounds__(kThreads, GB2_MINB_GA) k_f1gather(Phys ph, Grid2 G) {
   FOR_LIVE_CELLS(G, j, i) f1_gather(ph, G, j, i);
 }
 
@@ -246,7 +263,7 @@ struct LearnedStart {
 // takes part in the tensor-core inference; the weights are staged in shared
 // memory once per block.
 template <bool GUESS>
-__global__ void __launch_bounds__(kThreads, GB2_MINB)
+__global__ void __launch_bounds__(kThreads, GB2_MINB_UP)
     k_update(Phys ph, Params2 P, Grid2 G, int stage, Stats2 *S, const float *guess) {
   unsigned long long c2p[4] = {0, 0, 0, 0};
   if (!GUESS) {
