@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -42,6 +43,10 @@ struct gamma_ctx {
   size_t smem = 0;
   int grid_guess = 0;  // launch shape of the kernel with the learned guess
   size_t smem_guess = 0;
+  bool graphs = true;  // steps replayed from a captured CUDA graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  long long gkey[4] = {-1, -1, -1, -1};  // nsteps, variant, guess pointer, regrid_only of the graph
   int variant = 0;     // step-kernel launch shape (tune.h); 0 = the default kernel
   int vgrid[gb::tune::kVariants] = {};
   size_t vsmem[gb::tune::kVariants] = {};
@@ -356,11 +361,18 @@ GAMMA_API int gamma_gpu_upload(gamma_ctx_t *ctx, const int *ntrack, const double
 }
 
 namespace {
-int run_steps(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats, int regrid_only) {
-  if (!ctx || nsteps < 0) return GAMMA_ERR_INVALID;
+void drop_graph(gamma_ctx_t *ctx) {
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  ctx->gexec = nullptr;
+  ctx->graph = nullptr;
+  ctx->gkey[0] = -1;
+}
+
+// The launches of one call: queue and statistics reset, then the step kernel.
+int enqueue_steps(gamma_ctx_t *ctx, int nsteps, int regrid_only) {
   GB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(int), ctx->stream));
   GB_CUDA(ctx, cudaMemsetAsync(ctx->d_stats, 0, sizeof(gb::StepStats), ctx->stream));
-  GB_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
   const bool guess = ctx->T.mlp != nullptr && !regrid_only;
   int rc;
   if (!guess && ctx->variant > 0) {  // a tuned launch shape of the plain kernel
@@ -382,7 +394,36 @@ int run_steps(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats, int regri
     rc = guess ? launch_step<gb::CfgCart, true>(ctx, nsteps, regrid_only)
                : launch_step<gb::CfgCart, false>(ctx, nsteps, regrid_only);
   }
-  if (rc != GAMMA_OK) return rc;
+  return rc;
+}
+
+int run_steps(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats, int regrid_only) {
+  if (!ctx || nsteps < 0) return GAMMA_ERR_INVALID;
+  if (ctx->graphs) {
+    // the call's launches as one graph, captured again when what they bake in changes
+    const long long key[4] = {nsteps, ctx->variant, (long long)(uintptr_t)ctx->T.mlp, regrid_only};
+    if (!ctx->gexec || std::memcmp(key, ctx->gkey, sizeof(key)) != 0) {
+      drop_graph(ctx);
+      GB_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      const int rc = enqueue_steps(ctx, nsteps, regrid_only);
+      cudaGraph_t g = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+      if (rc != GAMMA_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (e != cudaSuccess) return fail_cuda(ctx, e, "step graph capture");
+      ctx->graph = g;
+      GB_CUDA(ctx, cudaGraphInstantiate(&ctx->gexec, ctx->graph, 0));
+      std::memcpy(ctx->gkey, key, sizeof(key));
+    }
+    GB_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    GB_CUDA(ctx, cudaGraphLaunch(ctx->gexec, ctx->stream));
+  } else {
+    GB_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    const int rc = enqueue_steps(ctx, nsteps, regrid_only);
+    if (rc != GAMMA_OK) return rc;
+  }
   GB_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
   if (stats) {
     gb::StepStats h;
@@ -693,9 +734,17 @@ GAMMA_API int gamma_gpu_autotune(gamma_ctx_t *ctx, int nsteps, float *ms, int *c
   return gamma_gpu_set_variant(ctx, best);
 }
 
+GAMMA_API int gamma_gpu_use_graphs(gamma_ctx_t *ctx, int on) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  ctx->graphs = on != 0;
+  if (!ctx->graphs) drop_graph(ctx);
+  return GAMMA_OK;
+}
+
 GAMMA_API void gamma_gpu_destroy(gamma_ctx_t *ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_graph(ctx);
   for (void *p : ctx->allocs) cudaFree(p);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);

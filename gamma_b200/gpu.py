@@ -37,6 +37,7 @@ EXPORTS = (
     "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess",
     "gamma_text1d_write", "gamma_text1d_read", "gamma_gpu_print_cols", "gamma_gpu_save", "gamma_gpu_load",
     "gamma_gpu_variant_info", "gamma_gpu_set_variant", "gamma_gpu_get_variant", "gamma_gpu_autotune",
+    "gamma_gpu_use_graphs",
 )
 
 
@@ -146,6 +147,7 @@ def lib() -> ctypes.CDLL:
         L.gamma_gpu_set_variant.argtypes = [v, ctypes.c_int]
         L.gamma_gpu_get_variant.argtypes = [v]
         L.gamma_gpu_autotune.argtypes = [v, ctypes.c_int, ctypes.POINTER(ctypes.c_float), _ip]
+        L.gamma_gpu_use_graphs.argtypes = [v, ctypes.c_int]
         L.gamma_gpu_save.argtypes = [v, ctypes.c_char_p]
         L.gamma_gpu_load.argtypes = [v, ctypes.c_char_p]
         for name in ("gamma_gpu_create", "gamma_gpu_layout", "gamma_gpu_set_params", "gamma_gpu_upload",
@@ -154,7 +156,7 @@ def lib() -> ctypes.CDLL:
                      "gamma_mlp_forward", "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess", "gamma_mlp_loss_grad",
                      "gamma_text1d_write", "gamma_text1d_read", "gamma_gpu_print_cols", "gamma_gpu_save",
                      "gamma_gpu_load", "gamma_gpu_variant_info", "gamma_gpu_set_variant", "gamma_gpu_get_variant",
-                     "gamma_gpu_autotune"):
+                     "gamma_gpu_autotune", "gamma_gpu_use_graphs"):
             getattr(L, name).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -259,6 +261,10 @@ class GammaGPU:
         self._check(lib().gamma_gpu_print_cols(self.h, int(run), directory.encode()))
         it = int(self.download()["it"][run])
         return os.path.join(directory, f"phys{it:010d}.out")
+
+    def use_graphs(self, on: bool):
+        """Replay step calls from a captured CUDA graph (default) or launch directly."""
+        self._check(lib().gamma_gpu_use_graphs(self.h, 1 if on else 0))
 
     def set_variant(self, variant: int):
         """Launch shape of the step kernel (variant_info); results do not change."""

@@ -325,6 +325,12 @@ int gamma_gpu_get_variant(const gamma_ctx_t *ctx);
  * Allocates a copy of the state for the duration of the call. */
 int gamma_gpu_autotune(gamma_ctx_t *ctx, int nsteps, float *ms, int *chosen);
 
+/* Step calls are replayed from a captured CUDA graph (the queue and statistics
+ * resets and the step kernel), captured again when the step count, launch
+ * shape or learned guess changes; on by default.  0 launches them directly.
+ * No counterpart in the reference. */
+int gamma_gpu_use_graphs(gamma_ctx_t *ctx, int on);
+
 /* ---- Snapshots -------------------------------------------------------------
  * Text: the reference's dump columns and its resume reader, so that files move
  * between this library and the reference both ways.  The reference names a

@@ -75,3 +75,20 @@ def test_autotune_restores_the_state_and_keeps_the_fastest(gpu_available):
     h.step(13)
     _same(a, h.download(), offsets)
     h.close()
+
+
+def test_graph_replay_gives_the_same_bits(gpu_available):
+    """Step calls replayed from the captured graph (the default), recaptured
+    when the step count or the shape changes, against direct launches."""
+    setups = _setups("sph")
+    outs = []
+    for graphs in (True, False):
+        g = _context("sph", setups)
+        g.use_graphs(graphs)
+        for k, v in ((3, 0), (1, 0), (1, 0), (4, 2), (2, 0)):
+            g.set_variant(v)
+            assert g.step(k)["status"] == 0
+        outs.append(g.download())
+        offsets = g.offsets
+        g.close()
+    _same(outs[0], outs[1], offsets)
