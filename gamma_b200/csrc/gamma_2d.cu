@@ -344,6 +344,7 @@ Phys phys_of(const gamma_2d_config_t &c) {
   p.eos = c.eos;
   p.ngst = c.ngst;
   p.eos_ws = c.eos_wavespeeds;
+  p.euler = c.timestep == GAMMA_TS_EULER;
   return p;
 }
 
@@ -417,7 +418,8 @@ int enqueue_step(gamma_2d *c) {
     k_regrid_check<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst + 1);
     k_regrid<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst + 1, 0);
   }
-  for (int stage = 1; stage <= 3; ++stage) {
+  const int nstage = c->cfg.timestep == GAMMA_TS_EULER ? 1 : 3;  // Timestep/euler.cpp or rk3.cpp
+  for (int stage = 1; stage <= nstage; ++stage) {
     k_ghosts_copy<<<ghost_blocks(c, stage == 1), kThreads, 0, s>>>(G, stage == 1);
     k_ghost_cells<<<c->NJ, 32, 0, s>>>(G);
     k_prefix<<<1, 1024, 0, s>>>(G);
@@ -455,7 +457,7 @@ GAMMA_API int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta,
   if (!cfg || !out || !theta || !dtheta) return GAMMA_ERR_INVALID;
   *out = nullptr;
   if (cfg->ngst != 2 || cfg->ntheta < 1 || cfg->nmax < 8 || !(cfg->gamma_ad > 1.) || !(cfg->cfl > 0.) ||
-      cfg->nq != 10)
+      cfg->nq != 10 || (cfg->timestep != GAMMA_TS_RK3 && cfg->timestep != GAMMA_TS_EULER))
     return GAMMA_ERR_INVALID;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GAMMA_ERR_NO_DEVICE;

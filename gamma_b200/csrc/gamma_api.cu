@@ -70,6 +70,7 @@ int check_cfg(const gamma_config_t *cfg, int *kind) {
   if (!cfg) return GAMMA_ERR_INVALID;
   if (cfg->ngst != 2) return GAMMA_ERR_INVALID;
   if (!(cfg->gamma_ad > 1.) || !(cfg->cfl > 0.)) return GAMMA_ERR_INVALID;
+  if (cfg->timestep != GAMMA_TS_RK3 && cfg->timestep != GAMMA_TS_EULER) return GAMMA_ERR_INVALID;
   if (cfg->geometry == GAMMA_GEOM_SPHERICAL1D && cfg->hydro == GAMMA_HYDRO_REL_SPH && cfg->nq == 10 &&
       cfg->shock_detection && cfg->local_synchrotron && cfg->problem == GAMMA_PROBLEM_BM1D) {
     *kind = KIND_SPH;
@@ -93,6 +94,7 @@ gb::Phys phys_of(const gamma_config_t &c) {
   p.eos = c.eos;
   p.ngst = c.ngst;
   p.eos_ws = c.eos_wavespeeds;
+  p.euler = c.timestep == GAMMA_TS_EULER;
   return p;
 }
 

@@ -43,6 +43,7 @@ Phys phys_1d(const gamma_config_t &c) {
   p.eos = c.eos;
   p.ngst = c.ngst;
   p.eos_ws = c.eos_wavespeeds;
+  p.euler = c.timestep == GAMMA_TS_EULER;
   return p;
 }
 
@@ -55,6 +56,7 @@ Phys phys_2d(const gamma_2d_config_t &c) {
   p.eos = c.eos;
   p.ngst = c.ngst;
   p.eos_ws = c.eos_wavespeeds;
+  p.euler = c.timestep == GAMMA_TS_EULER;
   return p;
 }
 

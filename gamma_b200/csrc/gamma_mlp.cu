@@ -40,6 +40,7 @@ gb::Phys phys_of(const gamma_config_t &c) {
   p.eos = c.eos;
   p.ngst = c.ngst;
   p.eos_ws = c.eos_wavespeeds;
+  p.euler = c.timestep == GAMMA_TS_EULER;
   return p;
 }
 

@@ -76,7 +76,8 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
   if (!cfg || nruns <= 0 || total <= 0 || nsteps < 0) return GAMMA_ERR_INVALID;
   if (!(cfg->geometry == GAMMA_GEOM_CARTESIAN && cfg->hydro == GAMMA_HYDRO_REL_CART && cfg->nq == 6 &&
         !cfg->shock_detection && !cfg->local_synchrotron && cfg->problem == GAMMA_PROBLEM_TUBE &&
-        cfg->eos == GAMMA_EOS_IDEAL && cfg->ngst == 2 && cfg->gamma_ad > 1. && cfg->cfl > 0.))
+        cfg->eos == GAMMA_EOS_IDEAL && cfg->ngst == 2 && cfg->gamma_ad > 1. && cfg->cfl > 0. &&
+        (cfg->timestep == GAMMA_TS_RK3 || cfg->timestep == GAMMA_TS_EULER)))
     return GAMMA_ERR_INVALID;
   if (!offsets || !capacity || !runs || !prim || !x || !dx || !dt_loc || !xI) return GAMMA_ERR_INVALID;
 
@@ -128,6 +129,8 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
   ph.vi = cfg->vi;
   ph.eos = cfg->eos;
   ph.ngst = cfg->ngst;
+  ph.eos_ws = cfg->eos_wavespeeds;
+  ph.euler = cfg->timestep == GAMMA_TS_EULER;
 
   auto kern = gb::track_step_kernel<gb::CfgCart, kBlock>;
   const size_t smem = sizeof(gb::TrackStep<gb::CfgCart, kBlock>::Smem) + 4u * 4u * (size_t)gb::regrid_words(32);

@@ -61,11 +61,12 @@ inline bool same_config(const gamma_config_t &a, const gamma_config_t &b) {
   return a.geometry == b.geometry && a.hydro == b.hydro && a.eos == b.eos && a.nq == b.nq &&
          a.shock_detection == b.shock_detection && a.local_synchrotron == b.local_synchrotron &&
          a.problem == b.problem && a.ngst == b.ngst && a.gamma_ad == b.gamma_ad && a.cfl == b.cfl && a.vi == b.vi &&
-         a.eos_wavespeeds == b.eos_wavespeeds;
+         a.eos_wavespeeds == b.eos_wavespeeds && a.timestep == b.timestep;
 }
 inline bool same_config(const gamma_2d_config_t &a, const gamma_2d_config_t &b) {
   return a.ntheta == b.ntheta && a.nmax == b.nmax && a.ngst == b.ngst && a.nq == b.nq && a.eos == b.eos &&
-         a.gamma_ad == b.gamma_ad && a.cfl == b.cfl && a.vi == b.vi && a.eos_wavespeeds == b.eos_wavespeeds;
+         a.gamma_ad == b.gamma_ad && a.cfl == b.cfl && a.vi == b.vi && a.eos_wavespeeds == b.eos_wavespeeds &&
+         a.timestep == b.timestep;
 }
 
 }  // namespace io

@@ -92,6 +92,8 @@ struct Phys {
   int ngst;
   int eos_ws;       // 1: each state's Gamma_eff in the wave speeds and the shock
                     // detector too (the reference uses GAMMA_ there)
+  int euler;        // 1: Grid::evolve of Timestep/euler.cpp (one Grid::update),
+                    // 0: the three SSP-RK3 stages of Timestep/rk3.cpp
 };
 
 template <class Cfg>

@@ -18,6 +18,8 @@
 //     iface_move, update_cell   Grid::update + the RK3 combines (2d.cpp:861-882,
 //                       rk3.cpp:98-194)
 //   -> inject particles.
+// With the Euler module (src/Timestep/euler.cpp:12-19) there is one stage and
+// no combine.
 //
 // Fields the reference keeps in its Cell records across stages and steps are
 // kept here too, because they feed later results: the moving-direction and
@@ -648,8 +650,8 @@ GB_HD void iface_move(const Grid2 &G, int j, int i, int stage) {
 }
 
 // Cell::update (cell.cpp:102-127) of an active cell, the stage's combine and
-// cons2prim; at stage 3 the particle injection of every cell (run after
-// evolve by Simu::run).  Every cell copies this stage's grad_f1 into the
+// cons2prim; at the last stage (3, or 1 with the Euler module) the particle
+// injection of every cell (run after evolve by Simu::run).  Every cell copies this stage's grad_f1 into the
 // persistent one.
 // The starting pressure of cons2prim: the cell's previous pressure (the
 // reference's warm start).  A learned guess replaces it through `guess`, which
@@ -751,11 +753,12 @@ GB_HD void update_cell(const Phys &ph, const Params2 &P, const Grid2 &G, int j, 
     G.x[g] = (cR + cL) / 2.;
     G.dx[g] = (cR - cL);
   }
-  if (stage == 3) {
+  const bool last = stage == (ph.euler ? 1 : 3);  // Grid::evolve ends (rk3.cpp, euler.cpp)
+  if (last) {
     const SynchConst sc{P.Nalpha, P.Nmp, P.Nme};
     inject_particles(ph, sc, prim, G.shocked[g] != 0, G.pspec[g]);
   }
-  if (active_track || stage == 3) {
+  if (active_track || last) {
 #pragma unroll
     for (int q = 0; q < NQ; ++q) G.prim[q * G.NC + g] = prim[q];
   }

@@ -3,6 +3,8 @@
 // Per step (src/simu.cpp:79-105): [regrid] -> reset shocks -> ghosts ->
 // stage-1 CFL candidates -> per-run dt (block min) -> stage-1 update ->
 // ghosts -> stage-2 fluxes+update+RK combine -> ghosts -> stage-3 -> inject.
+// With the Euler module (Timestep/euler.cpp:12-19) the step ends after the
+// stage-1 update: inject, and no RK combine.
 //
 // Each stage is one left-to-right sweep over the track in chunks of BS cells
 // (one interface and one cell per thread).  A chunk stages the stencil
@@ -497,7 +499,7 @@ struct TrackStep {
           }
         }
         if (upd) {
-          if (Cfg::SYNCH && stage == 3) {  // radiation_injectParticles, active cells
+          if (Cfg::SYNCH && stage == (ph.euler ? 1 : 3)) {  // radiation_injectParticles, active cells
             inject_particles<Cfg>(ph, sc, prim, T.shocked[g] != 0, T.pspec[g]);
           }
           store_prim(T, g, prim);
@@ -585,29 +587,33 @@ struct TrackStep {
     double m = sweep(T, ph, P, sc, sm, off, n, 1, 0, 0., t, st, inf);
     m = block_min(sm, m);
     const double dt = ph.cfl * m;
-    // stage 1 update
+    // stage 1 update (the whole Grid::evolve of Timestep/euler.cpp)
     sweep(T, ph, P, sc, sm, off, n, 1, 1, dt, t, st, inf);
     __syncthreads();
-    // stage 2
-    edge_geom(T, sm, off, n, ng, 2);
-    ghosts(T, ph, P, off, n, sm.edge, t);
-    __syncthreads();
-    sweep(T, ph, P, sc, sm, off, n, 2, 1, dt, t, st, inf);
-    __syncthreads();
-    // stage 3
-    edge_geom(T, sm, off, n, ng, 3);
-    ghosts(T, ph, P, off, n, sm.edge, t);
-    __syncthreads();
-    sweep(T, ph, P, sc, sm, off, n, 3, 1, dt, t, st, inf);
-    __syncthreads();
+    if (!ph.euler) {
+      // stage 2
+      edge_geom(T, sm, off, n, ng, 2);
+      ghosts(T, ph, P, off, n, sm.edge, t);
+      __syncthreads();
+      sweep(T, ph, P, sc, sm, off, n, 2, 1, dt, t, st, inf);
+      __syncthreads();
+      // stage 3
+      edge_geom(T, sm, off, n, ng, 3);
+      ghosts(T, ph, P, off, n, sm.edge, t);
+      __syncthreads();
+      sweep(T, ph, P, sc, sm, off, n, 3, 1, dt, t, st, inf);
+      __syncthreads();
+    }
 
-    // step-end cell geometry: ghosts 0 and n-1 keep the stage-3 ghost copies,
-    // cells 1..n-2 span their interfaces (CellGeomFromInterfacePos)
+    // step-end cell geometry.  RK3: ghosts 0 and n-1 keep the stage-3 ghost
+    // copies, cells 1..n-2 span their interfaces (CellGeomFromInterfacePos).
+    // Euler: only Cell::update moves cells (iL+1..iR-1); every ghost keeps
+    // its stage-1 copy.
     const int iL = ng - 1, iR = n - ng;
     for (int i = threadIdx.x; i < n; i += BS) {
       double gx, gdx;
-      if (i == 0 || i == n - 1) {
-        if (i == 0) {
+      if (ph.euler ? (i <= iL || i >= iR) : (i == 0 || i == n - 1)) {
+        if (i <= iL) {
           gx = sm.edge[0] - (iL - i + 1) * sm.edge[1];
           gdx = sm.edge[1];
         } else {

@@ -25,6 +25,7 @@ GEOM_SPHERICAL1D, GEOM_CARTESIAN = 0, 1
 HYDRO_REL_SPH, HYDRO_REL_CART = 0, 1
 EOS_IDEAL, EOS_SYNGE = 0, 1
 PROBLEM_BM1D, PROBLEM_TUBE = 0, 1
+TS_RK3, TS_EULER = 0, 1  # Timestep/rk3.cpp, Timestep/euler.cpp
 
 # every symbol include/gamma_gpu.h declares
 EXPORTS = (
@@ -53,7 +54,7 @@ class Config(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("geometry", "hydro", "eos", "nq", "shock_detection",
                                              "local_synchrotron", "problem", "ngst")] + \
                [(n, ctypes.c_double) for n in ("gamma_ad", "cfl", "vi")] + \
-               [("eos_wavespeeds", ctypes.c_int)]
+               [("eos_wavespeeds", ctypes.c_int), ("timestep", ctypes.c_int)]
 
 
 class RunParams(ctypes.Structure):
@@ -82,17 +83,19 @@ class MlpTrain(ctypes.Structure):
                 ("lr_final", ctypes.c_float), ("seed", ctypes.c_ulonglong)]
 
 
-def config_sph(gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=EOS_IDEAL, eos_wavespeeds=0) -> Config:
+def config_sph(gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=EOS_IDEAL, eos_wavespeeds=0, timestep=TS_RK3) -> Config:
     """spherical1D + rel_sph + radiation_sph, shock detection and local synchrotron (NUM_Q = 10).
     eos_wavespeeds=1 puts each state's Gamma_eff into the wave speeds and the
-    shock detector too (the reference uses GAMMA_ there)."""
+    shock detector too (the reference uses GAMMA_ there).  timestep: TS_RK3 or
+    TS_EULER, the reference's Timestep module."""
     return Config(GEOM_SPHERICAL1D, HYDRO_REL_SPH, eos, 10, 1, 1, PROBLEM_BM1D, 2, gamma_ad, cfl, vi,
-                  int(eos_wavespeeds))
+                  int(eos_wavespeeds), int(timestep))
 
 
-def config_cart(gamma_ad=5. / 3., cfl=0.2, vi=1.0) -> Config:
+def config_cart(gamma_ad=5. / 3., cfl=0.2, vi=1.0, timestep=TS_RK3) -> Config:
     """cartesian + rel_cart, no shock detection or synchrotron (NUM_Q = 6)."""
-    return Config(GEOM_CARTESIAN, HYDRO_REL_CART, EOS_IDEAL, 6, 0, 0, PROBLEM_TUBE, 2, gamma_ad, cfl, vi)
+    return Config(GEOM_CARTESIAN, HYDRO_REL_CART, EOS_IDEAL, 6, 0, 0, PROBLEM_TUBE, 2, gamma_ad, cfl, vi, 0,
+                  int(timestep))
 
 
 _dp = ctypes.POINTER(ctypes.c_double)

@@ -22,7 +22,7 @@ class Config2D(ctypes.Structure):
 
     _fields_ = [("ntheta", ctypes.c_int), ("nmax", ctypes.c_int), ("ngst", ctypes.c_int), ("nq", ctypes.c_int),
                 ("eos", ctypes.c_int), ("gamma_ad", ctypes.c_double), ("cfl", ctypes.c_double),
-                ("vi", ctypes.c_double), ("eos_wavespeeds", ctypes.c_int)]
+                ("vi", ctypes.c_double), ("eos_wavespeeds", ctypes.c_int), ("timestep", ctypes.c_int)]
 
 
 class Params2D(ctypes.Structure):
@@ -112,9 +112,9 @@ class Grid2DGPU:
     """One 2D run on the current CUDA device."""
 
     def __init__(self, ntheta: int, nmax: int, theta, dtheta, gamma_ad=4. / 3., cfl=0.2, vi=1.0,
-                 eos=gpu.EOS_IDEAL, eos_wavespeeds=0):
+                 eos=gpu.EOS_IDEAL, eos_wavespeeds=0, timestep=gpu.TS_RK3):
         self.cfg = Config2D(int(ntheta), int(nmax), 2, NQ, int(eos), float(gamma_ad), float(cfl), float(vi),
-                            int(eos_wavespeeds))
+                            int(eos_wavespeeds), int(timestep))
         th = np.ascontiguousarray(theta, dtype=np.float64)
         dth = np.ascontiguousarray(dtheta, dtype=np.float64)
         assert th.size == ntheta and dth.size == ntheta
@@ -216,9 +216,10 @@ class Grid2DGPU:
         return s
 
 
-def _config(ntheta, nmax, gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=gpu.EOS_IDEAL, eos_wavespeeds=0) -> Config2D:
+def _config(ntheta, nmax, gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=gpu.EOS_IDEAL, eos_wavespeeds=0,
+            timestep=gpu.TS_RK3) -> Config2D:
     return Config2D(int(ntheta), int(nmax), 2, NQ, int(eos), float(gamma_ad), float(cfl), float(vi),
-                    int(eos_wavespeeds))
+                    int(eos_wavespeeds), int(timestep))
 
 
 def text2d_write(path: str, s: State2D, theta, dtheta, **cfg):

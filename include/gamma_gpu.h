@@ -45,6 +45,9 @@ enum { GAMMA_GEOM_SPHERICAL1D = 0, GAMMA_GEOM_CARTESIAN = 1 };
 enum { GAMMA_HYDRO_REL_SPH = 0, GAMMA_HYDRO_REL_CART = 1 };
 enum { GAMMA_EOS_IDEAL = 0, GAMMA_EOS_SYNGE = 1 };
 enum { GAMMA_PROBLEM_BM1D = 0, GAMMA_PROBLEM_TUBE = 1 };
+/* the Timestep module: Grid::evolve of src/Timestep/rk3.cpp (SSP-RK3, three
+ * stages) or of src/Timestep/euler.cpp (one forward-Euler Grid::update) */
+enum { GAMMA_TS_RK3 = 0, GAMMA_TS_EULER = 1 };
 
 /* Module selection and switches (Makefile GEOMETRY/HYDRO/RADIATION/INITIAL,
  * environment.h GAMMA_, EOS_, CFL_, VI, SHOCK_DETECTION_, LOCAL_SYNCHROTRON_).
@@ -68,6 +71,7 @@ typedef struct {
    * 1: each state's Gamma_eff there too (rel_sph.cpp:37-52), the Synge EOS end
    * to end -- no counterpart in the reference.  No effect with the ideal EOS. */
   int eos_wavespeeds;
+  int timestep;  /* GAMMA_TS_*: the Makefile's TIMESTEP module */
 } gamma_config_t;
 
 /* Per-run parameters of the Blandford-McKee problem hooks
@@ -115,7 +119,8 @@ int gamma_gpu_upload(gamma_ctx_t *ctx, const int *ntrack, const double *t, const
 
 /* Advance every run by nsteps iterations of the Simu::run loop body
  * (src/simu.cpp:79-105: regrid, resetShock, updateGhosts, prepForUpdate,
- * detectShock, collect_dt, Grid::evolve (rk3.cpp:13-95), injectParticles),
+ * detectShock, collect_dt, Grid::evolve (rk3.cpp:13-95, or euler.cpp:12-19
+ * with GAMMA_TS_EULER), injectParticles),
  * each run with its own dt.  With stats == NULL the call only enqueues the
  * work; otherwise it waits and fills stats. */
 int gamma_gpu_step(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats);
@@ -230,7 +235,8 @@ int gamma_gpu_set_guess(gamma_ctx_t *ctx, const float *params);
  * updateGhosts 241-321, computeNeighbors 534-606, regrid 609-832,
  * movDir_ComputeLambda/updateKinematics/computeFluxes 735-839, collect_dt
  * 842-859, update 861-882) with the theta-wedge blast-wave hooks of
- * src/Initial/Tests/BM.cpp, and Grid::evolve (src/Timestep/rk3.cpp:98-194).
+ * src/Initial/Tests/BM.cpp, and Grid::evolve (src/Timestep/rk3.cpp:98-194, or
+ * src/Timestep/euler.cpp:12-19 with GAMMA_TS_EULER).
  *
  * A run has NJ = ntheta + 2 ngst tracks (ghost tracks included) of cap =
  * nmax + 2 ngst cells.  Per-cell arrays have NJ*cap entries, cell (j, i) at
@@ -246,6 +252,7 @@ typedef struct {
   int eos;      /* GAMMA_EOS_* */
   double gamma_ad, cfl, vi;
   int eos_wavespeeds;  /* as in gamma_config_t */
+  int timestep;        /* as in gamma_config_t */
 } gamma_2d_config_t;
 
 /* the problem module's constants (BM.cpp userKinematics, checkCellForRegrid)

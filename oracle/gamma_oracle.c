@@ -926,9 +926,13 @@ static void rk_combine(oc_sim *s, double w0, double w1) {
   }
 }
 
-/* Grid::evolve, RK3 (rk3.cpp:13-95) */
+/* Grid::evolve: RK3 (rk3.cpp:13-95) or Euler (euler.cpp:12-19) */
 static int evolve(oc_sim *s, double t, double dt) {
   int rc;
+  if (s->c.timestep == 1) {
+    grid_update(s, dt);
+    return 0;
+  }
   for (int i = 0; i < s->ntrack; ++i) { /* copyState0 (1d.cpp:813-828) */
     s->C[i].S0 = s->C[i].S;
     s->C[i].G0 = s->C[i].G;

@@ -53,6 +53,9 @@ typedef struct {
   /* 1: Gamma_eff of each state in the wave speeds and the shock detector too
    * (the reference uses GAMMA_ there whatever the EOS; 0 restates it) */
   int eos_wavespeeds;
+  /* Grid::evolve: 0 the SSP-RK3 of src/Timestep/rk3.cpp:13-95, 1 the single
+   * Grid::update of src/Timestep/euler.cpp:12-19 */
+  int timestep;
 } oc_config;
 
 typedef struct oc_sim oc_sim;

@@ -36,7 +36,7 @@ class OcConfig(ctypes.Structure):
                                           "merge_AR", "t_bm_until", "v_in", "v_out",
                                           "xmin", "xmax", "xmid", "rhoL", "pL", "vL", "trL",
                                           "rhoR", "pR", "vR", "trR", "c2p_epsrel")]
-        + [("eos_wavespeeds", ctypes.c_int)]
+        + [("eos_wavespeeds", ctypes.c_int), ("timestep", ctypes.c_int)]
     )
 
 

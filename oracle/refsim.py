@@ -52,7 +52,8 @@ class Snapshot:
 
 
 class RefSim:
-    """One reference build (``kind`` in {bm1d, bm1d_orig, tube, bm1d_synge}, or
+    """One reference build (``kind`` in {bm1d, bm1d_orig, tube, bm1d_synge,
+    bm1d_euler, tube_euler (Timestep/euler.cpp in place of rk3.cpp)}, or
     bm1d_io / tube_io: the reference's own text IO module linked, so printCols
     writes ../results/Last/phys*.out relative to the working directory and
     resume() reads the last one back)."""

@@ -48,6 +48,10 @@ CASES = {
                                    grid_log=1), (1, 2, 25, 100)),
     "bm1d_small": ("bm1d", dict(eta=1e-8, lorentz_mode=1, lfac_shock2=400., ncell=300, nmax=600, grid_log=1,
                                 r_lo=0.97, r_hi=1.03), (1, 10, 60)),
+    # the Euler time-stepping module (Timestep/euler.cpp linked in place of rk3.cpp)
+    "tube_euler": ("tube_euler", dict(ncell=300, nmax=300, vL=0.3, vR=0.3, rhoL=11., pL=12.), (1, 5, 60)),
+    "bm1d_small_euler": ("bm1d_euler", dict(eta=1e-8, lorentz_mode=1, lfac_shock2=400., ncell=300, nmax=600,
+                                            grid_log=1, r_lo=0.97, r_hi=1.03), (1, 10, 60)),
 }
 
 
@@ -57,7 +61,8 @@ def test_restatement_matches_reference(name):
     if not ref_available(kind):
         pytest.skip("reference build oracle/_ref absent")
     ref = run_isolated(kind, params, max(steps), snap_at=(0,) + steps)
-    cfg = port.tube_config(**params) if kind == "tube" else port.bm1d_config(**params)
+    ts = 1 if kind.endswith("_euler") else 0
+    cfg = port.tube_config(timestep=ts, **params) if kind.startswith("tube") else port.bm1d_config(timestep=ts, **params)
     mine = port_run(cfg, steps)
     for k in (0,) + steps:
         assert_same(mine[k], ref[k], f"{name} step {k}")
