@@ -278,17 +278,16 @@ GB_HD double c2p_f(const Phys &ph, double p, double D, double S2, double E, doub
 // with df/dp and lfac^2 on request.
 template <class Cfg>
 GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, double *df = nullptr,
-                       double *l2out = nullptr) {
+                       double *l2out = nullptr, double *lfac_out = nullptr) {
   const double W = E + p;
   const double x = (S * S) / (W * W);
   const double arg = Cfg::SPH ? fabs(1. - x) : (1. - x);
   const double lfac = 1. / sqrt(arg);
-  double gma;
-  if (Cfg::SPH) gma = eos_gamma(ph, D / lfac, p);
-  else gma = ph.gamma_ad;
+  const bool ideal = !Cfg::SPH || ph.eos == 0;
+  const double gma = ideal ? ph.gamma_ad : eos_gamma(ph, D / lfac, p);
   const double f = (E + p - D * lfac - (gma * p * lfac * lfac) / (gma - 1.));
   if (df) {
-    if (Cfg::SPH && ph.eos != 0) {  // Gamma_eff(p) terms: take them from the derivative form
+    if (!ideal) {  // Gamma_eff(p) terms: take them from the derivative form
       double dfast;
       c2p_f<Cfg>(ph, p, D, S * S, E, &dfast);
       *df = dfast;
@@ -296,11 +295,12 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
       const double sgn = (1. - x) >= 0. ? 1. : -1.;
       const double l2 = lfac * lfac;
       const double dl = -sgn * lfac * l2 * x / W;
-      const double k = gma / (gma - 1.);
-      *df = 1. - D * dl - k * (l2 + 2. * p * lfac * dl);
+      // kgam is GAMMA_/(GAMMA_-1) rounded once on the host: gma/(gma-1) exactly
+      *df = 1. - D * dl - ph.kgam * (l2 + 2. * p * lfac * dl);
     }
   }
   if (l2out) *l2out = lfac * lfac;
+  if (lfac_out) *lfac_out = arg >= 0. ? lfac : -1.;  // -1: no lfac of fabs(1 - x) here
   return f;
 }
 
@@ -308,17 +308,26 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
 // its no-solution tests and the warm start pCand are the reference's; the
 // Brent search is replaced by safeguarded Newton-Raphson.  Returns the
 // pressure the reference would go on with (pCand itself where it finds none).
+//
+// lfac_at (optional): the Lorentz factor 1/sqrt(|1 - S^2/(E+p)^2|) at the
+// returned pressure when the search evaluated f there (the same rounding as
+// f's), else -1.
 template <class Cfg>
-GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double E, double pCand, C2PStats *st) {
-  auto fval = [&](double p, double *df, double *l2) -> double {
-    return Cfg::FAST ? c2p_f<Cfg>(ph, p, D, S2, E, df, l2) : c2p_f_ref<Cfg>(ph, p, D, S, E, df, l2);
+GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double E, double pCand, C2PStats *st,
+                          double *lfac_at = nullptr) {
+  auto fval = [&](double p, double *df, double *l2, double *lf) -> double {
+    return Cfg::FAST ? c2p_f<Cfg>(ph, p, D, S2, E, df, l2) : c2p_f_ref<Cfg>(ph, p, D, S, E, df, l2, lf);
   };
   int iters = 0, fallback = 0;
-  const double f_init = fval(pCand, nullptr, nullptr);
+  // f at the warm start, with its slope: the search starts there when the
+  // warm start lies in the bracket (f does not depend on whether df is asked for)
+  double df0, l20, lf0 = -1.;
+  const double f_init = fval(pCand, &df0, &l20, &lf0);
+  if (lfac_at) *lfac_at = lf0;
   if (fabs(f_init) > 0.) {
     double p_lo = fmax(0., (1. + 1e-13) * S - E);
     bool find_p = true;
-    if (fval(p_lo, nullptr, nullptr) < 0) find_p = false;
+    if (fval(p_lo, nullptr, nullptr, nullptr) < 0) find_p = false;
     double p_hi;
     if (f_init < 0) {
       p_hi = 1. * pCand;
@@ -327,7 +336,7 @@ GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double 
       // the reference grows p_hi without bound (a zero guess would never end);
       // 400 decades reach infinity, where f is NaN and the loop stops anyway.
       // Its first test re-evaluates f(pCand), which is f_init.
-      for (int g = 0; g < 400 && (g == 0 ? f_init : fval(p_hi, nullptr, nullptr)) > 0; ++g) p_hi *= 10;
+      for (int g = 0; g < 400 && (g == 0 ? f_init : fval(p_hi, nullptr, nullptr, nullptr)) > 0; ++g) p_hi *= 10;
     }
     if (p_hi < p_lo) find_p = false;
     if (find_p) {
@@ -335,8 +344,9 @@ GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double 
       double lo = p_lo, hi = p_hi;
       if (f_init > 0.) lo = fmax(lo, pCand);
       double p = fmin(fmax(pCand, lo), hi);
-      double df, l2;
-      double f = fval(p, &df, &l2);
+      double df = df0, l2 = l20, lf = lf0;
+      double f = f_init;
+      if (!(p == pCand)) f = fval(p, &df, &l2, &lf);
       const int MAXIT = 100;
       const double eps = 2.220446049250313e-16;
       for (iters = 1; iters <= MAXIT; ++iters) {
@@ -351,8 +361,8 @@ GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double 
           pn = lo > 0. ? sqrt(lo) * sqrt(hi) : 0.5 * (lo + hi);
           if (!(pn > lo && pn < hi)) pn = 0.5 * (lo + hi);
         }
-        double dfn, l2n;
-        const double fn = fval(pn, &dfn, &l2n);
+        double dfn, l2n, lfn;
+        const double fn = fval(pn, &dfn, &l2n, &lfn);
         if (fn > 0.) lo = pn;
         else if (fn < 0.) hi = pn;
         const double step = fabs(pn - p);
@@ -360,10 +370,12 @@ GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double 
         f = fn;
         df = dfn;
         l2 = l2n;
+        lf = lfn;
         if (fn == 0. || step <= 1.e-14 * pn || (hi - lo) <= 1.e-14 * hi) break;
       }
       if (iters > MAXIT) fallback = 1;
       pCand = p;
+      if (lfac_at) *lfac_at = lf;
     }
   }
   if (st) {
@@ -385,7 +397,9 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
   double S2 = 0.;
   S2 += ss * ss;
   const double S = Cfg::FAST ? fabs(ss) : sqrt(S2);
-  const double pCand = c2p_pressure<Cfg>(ph, D, S, S2, E, Cfg::SPH ? fmax(1.e-13, prim[PPP]) : prim[PPP], st);
+  double lf_root = -1.;
+  const double pCand =
+      c2p_pressure<Cfg>(ph, D, S, S2, E, Cfg::SPH ? fmax(1.e-13, prim[PPP]) : prim[PPP], st, &lf_root);
 
   double p = pCand;
   double rho, uu;
@@ -396,15 +410,21 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
     rho = D * s1;
     uu = (fabs(S) == 0.) ? 0. : (ss * rW) / s1;
   } else {  // rel_sph.cpp:288-302
-    double Ep2 = (E + p) * (E + p);
-    double v2 = S2 / Ep2;
-    double lfac = 1. / sqrt(fabs(1. - v2));
+    // lfac = 1/sqrt(|1 - S2/(E+p)^2|): the root search's last f evaluation
+    // formed the same quotient from S*S, which is S2 whenever S*S == S2
+    double lfac = lf_root;
+    if (!(lfac > 0. && S * S == S2)) {
+      double Ep2 = (E + p) * (E + p);
+      double v2 = S2 / Ep2;
+      lfac = 1. / sqrt(fabs(1. - v2));
+    }
     rho = D / lfac;
     if (fabs(S) == 0.) {
       uu = 0;
     } else {
       double v = sqrt(1. - 1. / (lfac * lfac));
-      uu = lfac * v * (ss / S);
+      // ss/S is exactly +-1 when S == |ss|
+      uu = lfac * v * (fabs(ss) == S ? (ss > 0. ? 1. : -1.) : ss / S);
     }
   }
   if (Cfg::SPH) p = fmax(p, P_FLOOR);
