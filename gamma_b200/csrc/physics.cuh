@@ -2,8 +2,9 @@
 //
 // Each function restates one member of the GAMMA reference and keeps its
 // floating-point operation order, so that with -fmad=false the only
-// differences to the CPU reference come from libm (pow, tanh) and from the
-// pressure root finder (Newton-Raphson here, GSL Brent there).
+// differences to the CPU reference come from libm (tanh, and pow other than
+// the correctly rounded x^(3/4) of the shock detector) and from the pressure
+// root finder (Newton-Raphson here, GSL Brent there).
 //
 // Variable slots follow src/environment.h:33-82.  Slot 3 (the theta momentum /
 // 4-velocity) is identically zero in 1D: it is only ever multiplied by r
@@ -128,6 +129,39 @@ GB_HD double eos_gamma(const Phys &ph, double rho, double p) {
   double e_ratio = a + sqrt(a * a + 1.);
   return G - (G - 1.) / 2. * (1. - 1. / (e_ratio * e_ratio));
 }
+
+// 1/x to about 2^-22, for correction terms only
+GB_HD double recip_approx(double x) {
+#ifdef __CUDA_ARCH__
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  return r;
+#else
+  return 1. / x;
+#endif
+}
+
+// x^(3/4) rounded to nearest: the isentrope rho1 (p/p1)^(1/GAMMA_) of the shock
+// detector when 1/GAMMA_ is exactly 3/4 (GAMMA_ = 4/3), as the C library's pow
+// returns it.  sqrt(x) and then x^(1/4) are carried as double-double pairs:
+// the remainder of a correctly rounded square root, x - s^2, is exact as one
+// FMA (Markstein 1990; Boldo & Daumas 2003), so sqrt(x) = s + (x - s^2)/(2s)
+// to twice the precision, and Dekker's exact product (the FMA form) gives the
+// pair s*q; it is rounded once.  The correction terms need ~20 bits, hence the
+// approximate reciprocal.  Outside [2^-900, 2^900] (or NaN): pow itself.
+GB_HD double pow_3_4(double x) {
+  if (!(x >= 0x1p-900 && x <= 0x1p900)) return pow(x, 0.75);
+  const double s = sqrt(x);
+  const double sl = fma(-s, s, x) * 0.5 * recip_approx(s);  // sqrt(x) = s + sl
+  const double q = sqrt(s);
+  const double ql = (fma(-q, q, s) + sl) * 0.5 * recip_approx(q);  // sqrt(s + sl) = q + ql
+  const double ph = s * q;
+  const double lo = fma(s, q, -ph) + (s * ql + sl * q);
+  return ph + lo;
+}
+
+// (p/p1)^(1/GAMMA_) of the isentrope
+GB_HD double isentrope_pow(double x, double ginv) { return ginv == 0.75 ? pow_3_4(x) : pow(x, ginv); }
 
 template <class Cfg>
 GB_HD double state_gamma(const Phys &ph, const double *prim) {
@@ -632,10 +666,13 @@ GB_HD bool compute_Sd(const Phys &ph, const FState<Cfg> &S1, const FState<Cfg> &
 #pragma unroll 2
   for (int ip = 0; ip < n_evals; ++ip) {
     double p = p1 + (ip + .5) * dp;
-    double rho = rho1 * pow(p / p1, ginv);
+    double rho = rho1 * isentrope_pow(p / p1, ginv);
     double h = 1 + p * G / (G - 1.) / rho;
     double cs = sqrt(G * p / (rho + p * G / (G - 1.)));
-    double dI = sqrt(h * h + A1 * A1 * (1. - cs * cs)) / ((h * h + A1 * A1) * rho * cs) * dp;
+    // with A1 = 0 (1D: no transverse velocity) the root is sqrt(h*h) = h exactly
+    // (h >= 1, and sqrt of a rounded square is the number itself)
+    const double num = A1 == 0. ? h : sqrt(h * h + A1 * A1 * (1. - cs * cs));
+    double dI = num / ((h * h + A1 * A1) * rho * cs) * dp;
     I += dI;
   }
   double vSR = tanh(I);

@@ -239,7 +239,7 @@ GB_HD bool compute_Sd(const Phys &ph, const St &S1, const St &S2, int dim, bool 
   double I = 0;
   for (int ip = 0; ip < n_evals; ++ip) {
     double p = p1 + (ip + .5) * dp;
-    double rho = rho1 * pow(p / p1, 1. / G);
+    double rho = rho1 * isentrope_pow(p / p1, 1. / G);
     double h = 1 + p * G / (G - 1.) / rho;
     double cs = sqrt(G * p / (rho + p * G / (G - 1.)));
     double dI = sqrt(h * h + A1 * A1 * (1. - cs * cs)) / ((h * h + A1 * A1) * rho * cs) * dp;

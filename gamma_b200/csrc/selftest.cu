@@ -1,0 +1,39 @@
+// Device-side checks of numerical helpers for the test suite
+// (gamma_b200/lib/libgamma_selftest.so; nothing on the product path loads it).
+#include <cuda_runtime.h>
+
+#include "physics.cuh"
+
+namespace {
+
+__global__ void pow_3_4_kernel(const double *x, double *mine, double *libm, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    mine[i] = gb::pow_3_4(x[i]);
+    libm[i] = pow(x[i], 0.75);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// x^(3/4) of n host values by gb::pow_3_4 (mine) and by CUDA's pow (libm),
+// both evaluated on the current device.  Returns 0 or the CUDA error code.
+__attribute__((visibility("default"))) int gb_selftest_pow_3_4(const double *x, double *mine, double *libm, int n) {
+  if (n <= 0) return 0;
+  double *d = nullptr;
+  const size_t b = (size_t)n * sizeof(double);
+  cudaError_t e = cudaMalloc(&d, 3 * b);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaMemcpy(d, x, b, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    pow_3_4_kernel<<<(n + 255) / 256, 256>>>(d, d + n, d + 2 * (size_t)n, n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(mine, d + n, b, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(libm, d + 2 * (size_t)n, b, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return (int)e;
+}
+
+}  // extern "C"
