@@ -130,6 +130,19 @@ GB_HD double eos_gamma(const Phys &ph, double rho, double p) {
   return G - (G - 1.) / 2. * (1. - 1. / (e_ratio * e_ratio));
 }
 
+// a / b, bit for bit, for quotients whose numerator is often zero (uniform
+// tracers, flat gradients, gas at rest).  With a = +-0 the IEEE quotient is a
+// signed zero (b finite or infinite, nonzero) or NaN (b zero or NaN), which is
+// a * (1 / s) with s = +-1, +-0 or NaN as b's class; the divide then never
+// sees a zero numerator, which sends the whole warp through the division's
+// slow path.
+GB_HD double qdiv(double a, double b) {
+  const bool z = a == 0.;
+  const double s = z ? ((b != 0. && b == b) ? copysign(1., b) : b) : b;
+  const double q = (z ? 1. : a) / s;
+  return z ? a * q : q;
+}
+
 // 1/x to about 2^-22, for correction terms only
 GB_HD double recip_approx(double x) {
 #ifdef __CUDA_ARCH__
@@ -214,7 +227,7 @@ GB_HD void fill_state(const Phys &ph, FState<Cfg> &S) {
     prim2cons<Cfg>(ph, S.prim, S.cons);
     state2flux<Cfg>(S.prim, S.cons, S.flux);
     S.lfac = lfac_of(S.prim[UU1]);
-    S.v = S.prim[UU1] / S.lfac;
+    S.v = qdiv(S.prim[UU1], S.lfac);
     return;
   }
   const double rho = S.prim[RHO], p = S.prim[PPP], uu = S.prim[UU1];
@@ -248,12 +261,12 @@ GB_HD void state2flux(const double *prim, const double *cons, double *flux) {
   double lfac = lfac_of(uu);
   double D = cons[DEN];
   double ss = cons[SS1];
-  flux[DEN] = D * uu / lfac;
-  flux[SS1] = ss * uu / lfac + p;
+  flux[DEN] = qdiv(D * uu, lfac);
+  flux[SS1] = qdiv(ss * uu, lfac) + p;
   flux[SS2] = 0.;
-  flux[TAU] = ss - D * uu / lfac;
+  flux[TAU] = ss - qdiv(D * uu, lfac);
 #pragma unroll
-  for (int t = TR1; t < Cfg::NQ; ++t) flux[t] = cons[t] * uu / lfac;
+  for (int t = TR1; t < Cfg::NQ; ++t) flux[t] = qdiv(cons[t] * uu, lfac);
 }
 
 // ---------------------------------------------------------------------------
@@ -314,7 +327,7 @@ template <class Cfg>
 GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, double *df = nullptr,
                        double *l2out = nullptr, double *lfac_out = nullptr) {
   const double W = E + p;
-  const double x = (S * S) / (W * W);
+  const double x = qdiv(S * S, W * W);
   const double arg = Cfg::SPH ? fabs(1. - x) : (1. - x);
   const double lfac = 1. / sqrt(arg);
   const bool ideal = !Cfg::SPH || ph.eos == 0;
@@ -328,7 +341,7 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
     } else {  // d lfac/dp = -lfac^3 x / W with the same lfac and x as f
       const double sgn = (1. - x) >= 0. ? 1. : -1.;
       const double l2 = lfac * lfac;
-      const double dl = -sgn * lfac * l2 * x / W;
+      const double dl = qdiv(-sgn * lfac * l2 * x, W);
       // kgam is GAMMA_/(GAMMA_-1) rounded once on the host: gma/(gma-1) exactly
       *df = 1. - D * dl - ph.kgam * (l2 + 2. * p * lfac * dl);
     }
@@ -449,7 +462,7 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
     double lfac = lf_root;
     if (!(lfac > 0. && S * S == S2)) {
       double Ep2 = (E + p) * (E + p);
-      double v2 = S2 / Ep2;
+      double v2 = qdiv(S2, Ep2);
       lfac = 1. / sqrt(fabs(1. - v2));
     }
     rho = D / lfac;
@@ -472,7 +485,7 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
     for (int t = TR1; t < Cfg::NQ; ++t) prim[t] = cons[t] * rD;
   } else {
 #pragma unroll
-    for (int t = TR1; t < Cfg::NQ; ++t) prim[t] = cons[t] / D;
+    for (int t = TR1; t < Cfg::NQ; ++t) prim[t] = qdiv(cons[t], D);
   }
   prim2cons<Cfg>(ph, prim, cons);
 }
@@ -519,13 +532,13 @@ GB_HD Waves compute_lambda_ref(const Phys &ph, const FState<Cfg> &L, const FStat
   double AR = lR * ER - mmR;
   double BL = mmL * (lL - vL) - pL;
   double BR = mmR * (lR - vR) - pR;
-  double FhllE = (lL * AR - lR * AL) / (lR - lL);
+  double FhllE = qdiv(lL * AR - lR * AL, lR - lL);
   double Ehll = (AR - AL) / (lR - lL);
   double Fhllm = (lL * BR - lR * BL) / (lR - lL);
-  double mhll = (BR - BL) / (lR - lL);
+  double mhll = qdiv(BR - BL, lR - lL);
   bool linear = Cfg::SPH ? (fabs(FhllE) == 0) : (fabs(FhllE) < 1.e-15);
   if (linear) {
-    w.lS = mhll / (Ehll + Fhllm);
+    w.lS = qdiv(mhll, Ehll + Fhllm);
   } else {
     // pow(x, 2.) of the C library is the correctly rounded square: x*x
     const double ef = Ehll + Fhllm;
@@ -646,7 +659,7 @@ GB_HD bool compute_Sd(const Phys &ph, const FState<Cfg> &S1, const FState<Cfg> &
   const double chi = 0.5;
   double p1 = S1.prim[PPP];
   double p2 = S2.prim[PPP];
-  if (fabs((p1 - p2) / p1) < 1.e-10 || p1 < p2) {
+  if (fabs(qdiv(p1 - p2, p1)) < 1.e-10 || p1 < p2) {
     *Sd = -1;
     return false;
   }

@@ -74,16 +74,16 @@ GB_HD void state2flux(const double *prim, const double *cons, int n, double r, d
   double lf = sqrt(1 + u * u);
   double D = cons[DEN];
   double ss[2] = {cons[SS1], cons[SS2]};
-  ss[1] /= r;
-  flux[DEN] = D * uu[n] / lf;
+  ss[1] = qdiv(ss[1], r);
+  flux[DEN] = qdiv(D * uu[n], lf);
   for (int i = 0; i < 2; ++i) {
-    if (i == n) flux[SS1 + i] = ss[i] * uu[n] / lf + p;
-    else flux[SS1 + i] = ss[i] * uu[n] / lf;
+    if (i == n) flux[SS1 + i] = qdiv(ss[i] * uu[n], lf) + p;
+    else flux[SS1 + i] = qdiv(ss[i] * uu[n], lf);
   }
   flux[SS2] *= r;
-  flux[TAU] = ss[n] - D * uu[n] / lf;
+  flux[TAU] = ss[n] - qdiv(D * uu[n], lf);
 #pragma unroll
-  for (int t = TR1; t < NQ; ++t) flux[t] = cons[t] * uu[n] / lf;
+  for (int t = TR1; t < NQ; ++t) flux[t] = qdiv(cons[t] * uu[n], lf);
 }
 
 // One side of a Riemann problem: the state, its flux along the interface
@@ -113,8 +113,8 @@ GB_HD Waves compute_lambda(const Phys &ph, const St &L, const St &R, int dim, do
   const int u = UU1 + dim, s = SS1 + dim;
   Waves w;
   double lfacL = L.lfac, lfacR = R.lfac;
-  double vL = L.prim[u] / lfacL;
-  double vR = R.prim[u] / lfacR;
+  double vL = qdiv(L.prim[u], lfacL);
+  double vR = qdiv(R.prim[u], lfacR);
   double cSL = sqrt(GL * L.prim[PPP] / (L.prim[RHO] + L.prim[PPP] * GL / (GL - 1.)));
   double cSR = sqrt(GR * R.prim[PPP] / (R.prim[RHO] + R.prim[PPP] * GR / (GR - 1.)));
   double sgSL = cSL * cSL / (lfacL * lfacL * (1. - cSL * cSL));
@@ -129,8 +129,8 @@ GB_HD Waves compute_lambda(const Phys &ph, const St &L, const St &R, int dim, do
 
   const double d = dim == F1 ? xr : 1.;
   const double lL = w.lL, lR = w.lR;
-  double mmL = L.cons[s] / d;
-  double mmR = R.cons[s] / d;
+  double mmL = qdiv(L.cons[s], d);
+  double mmR = qdiv(R.cons[s], d);
   double pL = L.prim[PPP];
   double pR = R.prim[PPP];
   double EL = L.cons[TAU] + L.cons[DEN];
@@ -139,12 +139,12 @@ GB_HD Waves compute_lambda(const Phys &ph, const St &L, const St &R, int dim, do
   double AR = lR * ER - mmR;
   double BL = mmL * (lL - vL) - pL;
   double BR = mmR * (lR - vR) - pR;
-  double FhllE = (lL * AR - lR * AL) / (lR - lL);
+  double FhllE = qdiv(lL * AR - lR * AL, lR - lL);
   double Ehll = (AR - AL) / (lR - lL);
   double Fhllm = (lL * BR - lR * BL) / (lR - lL);
-  double mhll = (BR - BL) / (lR - lL);
+  double mhll = qdiv(BR - BL, lR - lL);
   if (fabs(FhllE) == 0) {
-    w.lS = mhll / (Ehll + Fhllm);
+    w.lS = qdiv(mhll, Ehll + Fhllm);
     return w;
   }
   // pow(x, 2.) of the C library is the correctly rounded square: x*x
@@ -159,9 +159,9 @@ GB_HD void star_state(const St &Sin, double lbda, double lS, int dim, double xr,
   const int u = UU1 + dim, s = SS1 + dim, so = SS1 + (1 - dim);
   double r = xr;
   double mm[2] = {Sin.cons[SS1], Sin.cons[SS2]};
-  mm[1] /= r;
+  mm[1] = qdiv(mm[1], r);
   double lf = Sin.lfac;
-  double v = Sin.prim[u] / lf;
+  double v = qdiv(Sin.prim[u], lf);
   double m = mm[dim];
   double p = Sin.prim[PPP];
   double D = Sin.cons[DEN];
@@ -216,7 +216,7 @@ GB_HD bool compute_Sd(const Phys &ph, const St &S1, const St &S2, int dim, bool 
   const double chi = 0.5;
   double p1 = S1.prim[PPP];
   double p2 = S2.prim[PPP];
-  if (fabs((p1 - p2) / p1) < 1.e-10 || p1 < p2) {
+  if (fabs(qdiv(p1 - p2, p1)) < 1.e-10 || p1 < p2) {
     *Sd = -1;
     return false;
   }
@@ -227,14 +227,14 @@ GB_HD bool compute_Sd(const Phys &ph, const St &S1, const St &S2, int dim, bool 
   double h1 = 1 + p1 * G / (G - 1.) / rho1;
   double h2 = 1 + p2 * G / (G - 1.) / rho2;
   double lfac2 = S2.lfac;
-  double vx1 = S1.prim[uux] / S1.lfac;
-  double vx2 = S2.prim[uux] / lfac2;
+  double vx1 = qdiv(S1.prim[uux], S1.lfac);
+  double vx2 = qdiv(S2.prim[uux], lfac2);
   if (reverse) {
     vx1 *= -1;
     vx2 *= -1;
   }
   double ut1 = S1.prim[uut];
-  double v12 = (vx1 - vx2) / (1 - vx1 * vx2);
+  double v12 = qdiv(vx1 - vx2, 1 - vx1 * vx2);
   double A1 = h1 * ut1;
   double I = 0;
   for (int ip = 0; ip < n_evals; ++ip) {
@@ -278,13 +278,13 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, double r, C2PSt
   double tau = cons[TAU];
   double E = D + tau;
   double ss[2] = {cons[SS1], cons[SS2]};
-  ss[1] /= r;
+  ss[1] = qdiv(ss[1], r);
   double S2 = 0.;
   for (int d = 0; d < 2; ++d) S2 += ss[d] * ss[d];
   double S = sqrt(S2);
   double p = c2p_pressure<Cfg2>(ph, D, S, S2, E, fmax(1.e-13, prim[PPP]), st);
   double Ep2 = (E + p) * (E + p);
-  double v2 = S2 / Ep2;
+  double v2 = qdiv(S2, Ep2);
   double lf = 1. / sqrt(fabs(1. - v2));
   double rho = D / lf;
   double uu[2];
@@ -292,7 +292,7 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, double r, C2PSt
     uu[0] = uu[1] = 0;
   } else {
     double v = sqrt(1. - 1. / (lf * lf));
-    for (int d = 0; d < 2; ++d) uu[d] = lf * v * (ss[d] / S);
+    for (int d = 0; d < 2; ++d) uu[d] = lf * v * qdiv(ss[d], S);
   }
   p = fmax(p, P_FLOOR);
   prim[PPP] = p;
@@ -300,7 +300,7 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, double r, C2PSt
   prim[UU1] = uu[0];
   prim[UU2] = uu[1];
 #pragma unroll
-  for (int t = TR1; t < NQ; ++t) prim[t] = cons[t] / D;
+  for (int t = TR1; t < NQ; ++t) prim[t] = qdiv(cons[t], D);
   prim2cons(ph, prim, cons, r);
 }
 

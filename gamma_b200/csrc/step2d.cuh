@@ -222,9 +222,9 @@ GB_HD void mv_interface(const Phys &ph, const Params2 &P, const Grid2 &G, int j,
     for (int q = 0; q < NQ; ++q) {
       const double qLL = G.prim[q * G.NC + g - 1], qL = G.prim[q * G.NC + g];
       const double qR = G.prim[q * G.NC + g + 1], qRR = G.prim[q * G.NC + g + 2];
-      double gL = (qL - qLL) / (cL - cLL);
-      const double gN = (qR - qL) / (cR - cL);
-      double gR = (qRR - qR) / (cRR - cR);
+      double gL = qdiv(qL - qLL, cL - cLL);
+      const double gN = qdiv(qR - qL, cR - cL);
+      double gR = qdiv(qRR - qR, cRR - cR);
       gL = minmod(gL, gN);
       gR = minmod(gR, gN);
       // grad_mv stored in the cells; cell i from its right interface, except
@@ -342,7 +342,7 @@ GB_HD void neighbour_grad(const Grid2 &G, long long gn, double xm, double cr0, d
   for (int q = 0; q < NQ; ++q) {
     const double qL = p0[q] + m0[q] * dxmL;
     const double qR = G.prim[q * G.NC + gn] + G.gmv[q * G.NC + gn] * dxmR;
-    grad[q] = (qR - qL) / dcen;
+    grad[q] = qdiv(qR - qL, dcen);
   }
 }
 
@@ -393,7 +393,7 @@ GB_HD void trans_grad(const Grid2 &G, int j, int i) {
     }
   }
 #pragma unroll
-  for (int q = 0; q < NQ; ++q) avg[q] /= dAtot;
+  for (int q = 0; q < NQ; ++q) avg[q] = qdiv(avg[q], dAtot);
   kn = 0;
   for (int d = 0; d < 2; ++d) {
     const int first = d == 0 ? f0 : f1, cnt = d == 0 ? c0 : c1;
@@ -705,7 +705,7 @@ GB_HD void update_cell(const Phys &ph, const Params2 &P, const Grid2 &G, int j, 
     const double xL = G.xIm[g - 1], xR = G.xIm[g];
     const Geom G1 = make_geom((xR + xL) / 2., (xR - xL), tj);
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) cons[q] /= G1.dV;
+    for (int q = 0; q < NQ; ++q) cons[q] = q <= TAU ? cons[q] / G1.dV : qdiv(cons[q], G1.dV);
     r1 = G1.cen_r;
     dV1 = G1.dV;
     xn = G1.r;
@@ -729,7 +729,7 @@ GB_HD void update_cell(const Phys &ph, const Params2 &P, const Grid2 &G, int j, 
       const double cL = G.xI[g - 1], cR = G.xI[g];  // combined positions
       const Geom G2 = make_geom((cR + cL) / 2., (cR - cL), tj);
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) cons[q] /= G2.dV;
+      for (int q = 0; q < NQ; ++q) cons[q] = q <= TAU ? cons[q] / G2.dV : qdiv(cons[q], G2.dV);
       r2 = G2.r;
       xn = G2.r;
       dxn = G2.dr;

@@ -313,7 +313,7 @@ struct TrackStep {
           if ((a > 0 || k > 0) && a + k < n) {  // slots k and k+1 both hold cells
             const double d = sm.cen[k + 1] - sm.cen[k];
 #pragma unroll
-            for (int s = 0; s < NQS; ++s) sm.gp[s][k] = (sm.cp[s][k + 1] - sm.cp[s][k]) / d;
+            for (int s = 0; s < NQS; ++s) sm.gp[s][k] = qdiv(sm.cp[s][k + 1] - sm.cp[s][k], d);
           }
         }
         __syncthreads();
@@ -467,7 +467,7 @@ struct TrackStep {
             for (int q = 0; q < NQ; ++q) cons[q] *= rdV1;
           } else {
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) cons[q] /= G1.dV;
+            for (int q = 0; q < NQ; ++q) cons[q] = q <= TAU ? cons[q] / G1.dV : qdiv(cons[q], G1.dV);
           }
         }
         if (GUESS) learned_guess(*inf, cons, prim, upd);
@@ -489,7 +489,7 @@ struct TrackStep {
               for (int q = 0; q < NQ; ++q) cons[q] *= rdV2;
             } else {
 #pragma unroll
-              for (int q = 0; q < NQ; ++q) cons[q] /= G2.dV;
+              for (int q = 0; q < NQ; ++q) cons[q] = q <= TAU ? cons[q] / G2.dV : qdiv(cons[q], G2.dV);
             }
           }
           if (GUESS) learned_guess(*inf, cons, prim, upd);
