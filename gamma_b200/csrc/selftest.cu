@@ -13,9 +13,37 @@ __global__ void pow_3_4_kernel(const double *x, double *mine, double *libm, int 
   }
 }
 
+__global__ void qdiv_kernel(const double *a, const double *b, double *mine, double *ieee, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    mine[i] = gb::qdiv(a[i], b[i]);
+    ieee[i] = a[i] / b[i];
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+// gb::qdiv(a, b) and the plain IEEE quotient a / b of n host pairs, on the
+// current device.  Returns 0 or the CUDA error code.
+__attribute__((visibility("default"))) int gb_selftest_qdiv(const double *a, const double *b, double *mine,
+                                                            double *ieee, int n) {
+  if (n <= 0) return 0;
+  double *d = nullptr;
+  const size_t s = (size_t)n * sizeof(double);
+  cudaError_t e = cudaMalloc(&d, 4 * s);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaMemcpy(d, a, s, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + n, b, s, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    qdiv_kernel<<<(n + 255) / 256, 256>>>(d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n, n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(mine, d + 2 * (size_t)n, s, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(ieee, d + 3 * (size_t)n, s, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return (int)e;
+}
 
 // x^(3/4) of n host values by gb::pow_3_4 (mine) and by CUDA's pow (libm),
 // both evaluated on the current device.  Returns 0 or the CUDA error code.
