@@ -15,6 +15,7 @@
 // The state conversions are the step's own (physics.cuh, physics2d.cuh),
 // compiled here for the host.
 #define GB_HD __host__ __device__ inline
+#define GB_HD_OUTLINE __host__ __device__ inline
 #include "io.h"
 #include "physics.cuh"
 #include "physics2d.cuh"

@@ -18,6 +18,11 @@
 #ifndef GB_HD
 #define GB_HD __device__ __forceinline__
 #endif
+// one out-of-line copy (the pressure root search is called from several places
+// of a step, and its inlined copies crowd the instruction cache)
+#ifndef GB_HD_OUTLINE
+#define GB_HD_OUTLINE __device__ __noinline__
+#endif
 
 namespace gb {
 
@@ -360,8 +365,8 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
 // returned pressure when the search evaluated f there (the same rounding as
 // f's), else -1.
 template <class Cfg>
-GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double E, double pCand, C2PStats *st,
-                          double *lfac_at = nullptr) {
+GB_HD_OUTLINE double c2p_pressure(const Phys &ph, double D, double S, double S2, double E, double pCand,
+                                  C2PStats *st, double *lfac_at = nullptr) {
   auto fval = [&](double p, double *df, double *l2, double *lf) -> double {
     return Cfg::FAST ? c2p_f<Cfg>(ph, p, D, S2, E, df, l2) : c2p_f_ref<Cfg>(ph, p, D, S, E, df, l2, lf);
   };
