@@ -18,8 +18,7 @@
 #ifndef GB_HD
 #define GB_HD __device__ __forceinline__
 #endif
-// one out-of-line copy (the pressure root search is called from several places
-// of a step, and its inlined copies crowd the instruction cache)
+// one out-of-line copy per kernel (see c2p_pressure)
 #ifndef GB_HD_OUTLINE
 #define GB_HD_OUTLINE __device__ __noinline__
 #endif
@@ -365,8 +364,8 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
 // returned pressure when the search evaluated f there (the same rounding as
 // f's), else -1.
 template <class Cfg>
-GB_HD_OUTLINE double c2p_pressure(const Phys &ph, double D, double S, double S2, double E, double pCand,
-                                  C2PStats *st, double *lfac_at = nullptr) {
+GB_HD double c2p_pressure_body(const Phys &ph, double D, double S, double S2, double E, double pCand,
+                               C2PStats *st, double *lfac_at) {
   auto fval = [&](double p, double *df, double *l2, double *lf) -> double {
     return Cfg::FAST ? c2p_f<Cfg>(ph, p, D, S2, E, df, l2) : c2p_f_ref<Cfg>(ph, p, D, S, E, df, l2, lf);
   };
@@ -435,6 +434,23 @@ GB_HD_OUTLINE double c2p_pressure(const Phys &ph, double D, double S, double S2,
     st->fallback = fallback;
   }
   return pCand;
+}
+
+template <class Cfg>
+GB_HD_OUTLINE double c2p_pressure_outline(const Phys &ph, double D, double S, double S2, double E, double pCand,
+                                          C2PStats *st, double *lfac_at) {
+  return c2p_pressure_body<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at);
+}
+
+// The cartesian step calls the search from one out-of-line copy: inlined at
+// every call site of the fused step kernel it crowds the instruction cache
+// (3% slower).  The spherical kernels, the 2D passes and the batch cons2prim
+// keep it inline, which is as fast or faster there.
+template <class Cfg>
+GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double E, double pCand, C2PStats *st,
+                          double *lfac_at = nullptr) {
+  if (Cfg::SPH) return c2p_pressure_body<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at);
+  return c2p_pressure_outline<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at);
 }
 
 // FluidState::cons2prim (rel_sph.cpp:213-320; rel_cart.cpp:125-229).
