@@ -336,7 +336,8 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
   const double lfac = 1. / sqrt(arg);
   const bool ideal = !Cfg::SPH || ph.eos == 0;
   const double gma = ideal ? ph.gamma_ad : eos_gamma(ph, D / lfac, p);
-  const double f = (E + p - D * lfac - (gma * p * lfac * lfac) / (gma - 1.));
+  // p = 0 at the bracket's lower end p_lo, which every search evaluates
+  const double f = (E + p - D * lfac - qdiv(gma * p * lfac * lfac, gma - 1.));
   if (df) {
     if (!ideal) {  // Gamma_eff(p) terms: take them from the derivative form
       double dfast;
