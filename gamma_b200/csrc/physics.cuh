@@ -329,7 +329,7 @@ GB_HD double c2p_f(const Phys &ph, double p, double D, double S2, double E, doub
 // with df/dp and lfac^2 on request.
 template <class Cfg>
 GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, double *df = nullptr,
-                       double *l2out = nullptr, double *lfac_out = nullptr) {
+                       double *l2out = nullptr, double *lfac_out = nullptr, bool p_may_be_zero = false) {
   const double W = E + p;
   const double x = qdiv(S * S, W * W);
   const double arg = Cfg::SPH ? fabs(1. - x) : (1. - x);
@@ -337,7 +337,8 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
   const bool ideal = !Cfg::SPH || ph.eos == 0;
   const double gma = ideal ? ph.gamma_ad : eos_gamma(ph, D / lfac, p);
   // p = 0 at the bracket's lower end p_lo, which every search evaluates
-  const double f = (E + p - D * lfac - qdiv(gma * p * lfac * lfac, gma - 1.));
+  const double kp = gma * p * lfac * lfac;
+  const double f = (E + p - D * lfac - (p_may_be_zero ? qdiv(kp, gma - 1.) : kp / (gma - 1.)));
   if (df) {
     if (!ideal) {  // Gamma_eff(p) terms: take them from the derivative form
       double dfast;
@@ -367,8 +368,9 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
 template <class Cfg>
 GB_HD double c2p_pressure_body(const Phys &ph, double D, double S, double S2, double E, double pCand,
                                C2PStats *st, double *lfac_at) {
-  auto fval = [&](double p, double *df, double *l2, double *lf) -> double {
-    return Cfg::FAST ? c2p_f<Cfg>(ph, p, D, S2, E, df, l2) : c2p_f_ref<Cfg>(ph, p, D, S, E, df, l2, lf);
+  auto fval = [&](double p, double *df, double *l2, double *lf, bool p_may_be_zero = false) -> double {
+    return Cfg::FAST ? c2p_f<Cfg>(ph, p, D, S2, E, df, l2)
+                     : c2p_f_ref<Cfg>(ph, p, D, S, E, df, l2, lf, p_may_be_zero);
   };
   int iters = 0, fallback = 0;
   // f at the warm start, with its slope: the search starts there when the
@@ -379,7 +381,7 @@ GB_HD double c2p_pressure_body(const Phys &ph, double D, double S, double S2, do
   if (fabs(f_init) > 0.) {
     double p_lo = fmax(0., (1. + 1e-13) * S - E);
     bool find_p = true;
-    if (fval(p_lo, nullptr, nullptr, nullptr) < 0) find_p = false;
+    if (fval(p_lo, nullptr, nullptr, nullptr, true) < 0) find_p = false;
     double p_hi;
     if (f_init < 0) {
       p_hi = 1. * pCand;
