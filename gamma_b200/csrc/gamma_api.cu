@@ -7,13 +7,35 @@
 #include <cstdio>
 #include <cstdint>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "io.h"
+#include "smem_limit.h"
 #include "track_step.cuh"
 #include "tune.h"
+
+namespace gb {
+
+cudaError_t raise_smem_limit(const void *fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> high;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t &cur = high[{dev, fn}];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
+
+}  // namespace gb
 
 namespace {
 
@@ -112,7 +134,7 @@ template <class Cfg, bool GUESS>
 int configure_launch(gamma_ctx *c, int *grid, size_t *smem) {
   auto kern = gb::track_step_kernel<Cfg, kBlock, GUESS>;
   *smem = smem_bytes<Cfg, GUESS>(c->max_cap);
-  GB_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+  GB_CUDA(c, gb::raise_smem_limit((const void *)kern, *smem));
   int dev = 0, nsm = 0, occ = 0;
   GB_CUDA(c, cudaGetDevice(&dev));
   GB_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));

@@ -27,6 +27,7 @@
 
 #include <mutex>
 
+#include "smem_limit.h"
 #include "track_step.cuh"
 
 namespace {
@@ -81,8 +82,12 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
     return GAMMA_ERR_INVALID;
   if (!offsets || !capacity || !runs || !prim || !x || !dx || !dt_loc || !xI) return GAMMA_ERR_INVALID;
 
-  // workspace layout; reject before touching anything if it does not fit
+  // workspace layout; reject before touching anything if it does not fit.
+  // The per-item bounds come first so that no size product below can wrap.
   constexpr int NQS = gb::CfgCart::NQ - 1;
+  if ((unsigned long long)total > kNoAllocBytes / sizeof(double) ||
+      (size_t)nruns > kNoAllocBytes / sizeof(gb::RunParams))
+    return GAMMA_ERR_CAPACITY;
   const size_t n = (size_t)total;
   const size_t off_queue = 0;
   const size_t off_stats = align256(off_queue + sizeof(int));
@@ -134,8 +139,8 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
 
   auto kern = gb::track_step_kernel<gb::CfgCart, kBlock>;
   const size_t smem = sizeof(gb::TrackStep<gb::CfgCart, kBlock>::Smem) + 4u * 4u * (size_t)gb::regrid_words(32);
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return GAMMA_ERR_CUDA;
+  // contexts launch the same kernel with larger limits: never lower them
+  if (gb::raise_smem_limit((const void *)kern, smem) != cudaSuccess) return GAMMA_ERR_CUDA;
   int dev = 0, nsm = 0, occ = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return GAMMA_ERR_CUDA;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return GAMMA_ERR_CUDA;

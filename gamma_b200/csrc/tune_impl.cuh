@@ -5,6 +5,7 @@
 
 #include <algorithm>
 
+#include "smem_limit.h"
 #include "tune.h"
 
 namespace gb {
@@ -27,7 +28,7 @@ template <int V>
 cudaError_t configure_v(int nruns, int max_cap, int *grid, size_t *smem) {
   using K = Kern<V>;
   *smem = K::smem(max_cap);
-  cudaError_t e = cudaFuncSetAttribute(K::fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+  cudaError_t e = raise_smem_limit((const void *)K::fn, *smem);
   if (e != cudaSuccess) return e;
   int dev = 0, nsm = 0, occ = 0;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
