@@ -1,7 +1,8 @@
 """Writes the golden fixtures of this directory from the GAMMA reference itself.
 
-The reference is the one compiled from its sources under /root/reference by
-oracle/Makefile (oracle/_ref/libref_*.so).  Each fixture holds the reference's
+The reference is the one compiled from its sources by oracle/Makefile
+(oracle/_ref/libref_*.so; the checkout is $GAMMA_REFERENCE, else the directory
+"reference" beside this repository).  Each fixture holds the reference's
 track state at a few steps of a small case, so that the oracle restatement and
 the GPU path can be pinned on machines without the reference sources:
 
