@@ -21,6 +21,8 @@ constexpr int MV = 0, F1 = 1;
 // rel_sph with synchrotron tracers and shock detection, 2D
 struct Cfg2 {
   static constexpr bool FAST = false;
+  static constexpr bool FAST_RIEMANN = false;
+  static constexpr bool FAST_ROOT = false;
   static constexpr int NQ = 10;
   static constexpr bool SPH = true;
   static constexpr bool SHOCK = true;

@@ -105,7 +105,7 @@ struct TrackStep {
     double fl[NQS][CH + 1];  // interface fluxes; slot 0 = carry (interface a-1)
     double lL[CH + 1], lR[CH + 1], v[CH + 1];
     double xold[CH + 1], xnew[CH + 1], xcmb[CH + 1];
-    double gp[Cfg::FAST ? 1 : NQS][Cfg::FAST ? 1 : NC];  // gradient between slots k and k+1 (grad())
+    double gp[NQS][NC];  // gradient between slots k and k+1 (grad())
     double red[BS / 32];
     double edge[4];  // x, dx of the left and right edge cells this stage
     int ints[4];
@@ -214,23 +214,15 @@ struct TrackStep {
       }
     } else {
       // cells i-1 .. i+2 (i+2 <= n-1 for every interior interface)
-      const double cenLL = sm.cen[c - 1], cenL = sm.cen[c], cenR = sm.cen[c + 1], cenRR = sm.cen[c + 2];
-      const double d1 = cenL - cenLL, d2 = cenR - cenL, d3 = cenRR - cenR;
-      const double r1 = 1. / d1, r2 = 1. / d2, r3 = 1. / d3;
+      const double cenL = sm.cen[c], cenR = sm.cen[c + 1];
       const double dL = xI - cenL, dR = xI - cenR;
 #pragma unroll
       for (int s = 0; s < NQS; ++s) {
-        const double qLL = sm.cp[s][c - 1], qL = sm.cp[s][c], qR = sm.cp[s][c + 1], qRR = sm.cp[s][c + 2];
-        double gN, gL, gR;
-        if (Cfg::FAST) {
-          gN = (qR - qL) * r2;
-          gL = (qL - qLL) * r1;
-          gR = (qRR - qR) * r3;
-        } else {  // grad() of 1d.cpp:262-274, formed once per cell pair (pair_gradients)
-          gN = sm.gp[s][c];
-          gL = sm.gp[s][c - 1];
-          gR = sm.gp[s][c + 1];
-        }
+        const double qL = sm.cp[s][c], qR = sm.cp[s][c + 1];
+        // grad() of 1d.cpp:262-274, formed once per cell pair in the sweep
+        const double gN = sm.gp[s][c];
+        double gL = sm.gp[s][c - 1];
+        double gR = sm.gp[s][c + 1];
         gL = minmod(gL, gN);
         gR = minmod(gR, gN);
         L.prim[Slots<Cfg>::q_of(s)] = qL + gL * dL;
@@ -306,14 +298,20 @@ struct TrackStep {
         }
       }
       __syncthreads();
-      if (!Cfg::FAST && !(mode == 1 && stage == 1)) {
+      if (!(mode == 1 && stage == 1)) {
         // grad() between staged cells k and k+1: (q[k+1] - q[k]) / (cen[k+1] - cen[k]),
         // each used by the three interfaces around it (slots past the track end unused)
         for (int k = tid; k < NC - 1; k += BS) {
           if ((a > 0 || k > 0) && a + k < n) {  // slots k and k+1 both hold cells
             const double d = sm.cen[k + 1] - sm.cen[k];
+            if (Cfg::FAST) {
+              const double rd = 1. / d;
 #pragma unroll
-            for (int s = 0; s < NQS; ++s) sm.gp[s][k] = qdiv(sm.cp[s][k + 1] - sm.cp[s][k], d);
+              for (int s = 0; s < NQS; ++s) sm.gp[s][k] = (sm.cp[s][k + 1] - sm.cp[s][k]) * rd;
+            } else {
+#pragma unroll
+              for (int s = 0; s < NQS; ++s) sm.gp[s][k] = qdiv(sm.cp[s][k + 1] - sm.cp[s][k], d);
+            }
           }
         }
         __syncthreads();

@@ -94,3 +94,20 @@ def within_sensitivity(got, ref, sens, gamma_ad, rtol=1e-12, k=4.0, qs=(0, 1, 2)
         worst[q] = float(np.max(d / np.maximum(bound, 1e-300)))
         frac[q] = float(np.mean(d <= rtol * scale))
     return worst, frac
+
+
+def record(quantity, measured, bar, better="lower"):
+    """Append one measured parity figure to $GAMMA_PARITY_RECORD (JSON lines).
+
+    Tests call this before asserting, so a run over several builds (arithmetic
+    forms, FMA contraction) yields a table of what each build measures against
+    each bar, failures included.  Without the variable it does nothing."""
+    import json
+    import os
+    path = os.environ.get("GAMMA_PARITY_RECORD")
+    if not path:
+        return
+    test = os.environ.get("PYTEST_CURRENT_TEST", "?").split(" ")[0]
+    with open(path, "a") as f:
+        f.write(json.dumps({"test": test, "quantity": quantity, "measured": float(measured), "bar": float(bar),
+                            "better": better, "lib": os.environ.get("GAMMA_B200_LIB", "default")}) + "\n")

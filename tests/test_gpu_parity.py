@@ -20,7 +20,7 @@ import numpy as np
 import pytest
 
 from conftest import ref_available
-from helpers import energy_scale, l1_rel, solver_sensitivity, within_sensitivity
+from helpers import energy_scale, l1_rel, record, solver_sensitivity, within_sensitivity
 
 pytestmark = pytest.mark.gpu
 
@@ -93,6 +93,11 @@ def test_tubes_one_step_match_converged_oracle(gpu_available):
     for s, g in zip(setups, got):
         ref, sens = solver_sensitivity(lambda eps: _port_tube(s, 1, epsrel=eps))
         worst, frac = within_sensitivity(g, ref, sens, 5. / 3., k=10.0, qs=(0, 1, 2, 4))
+        record(f"tube{s.ncell} worst/bound", max(worst.values()), 1.0)
+        record(f"tube{s.ncell} cells within 1e-12", min(frac.values()), 0.995, "higher")
+        for f in ("x", "dx", "xI"):
+            a, b = getattr(g, f), getattr(ref, f)
+            record(f"tube{s.ncell} {f} rel", np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)), 1e-12)
         assert max(worst.values()) <= 1.0, (worst, frac)
         assert min(frac.values()) >= 0.995, frac
         for f in ("x", "dx", "xI"):  # the right ghost cell has zero width (1d.cpp:241)
@@ -109,6 +114,8 @@ def test_tubes_100_steps_l1(gpu_available):
         ref = _port_tube(s, 100)
         assert g.ntrack == ref.ntrack
         a = slice(2, g.ntrack - 2)
+        record(f"tube{s.ncell} L1 max over slots", max(l1_rel(g.prim[q, a], ref.prim[q, a]) for q in (0, 1, 2, 4)),
+               1e-8)
         for q in (0, 1, 2, 4):
             assert l1_rel(g.prim[q, a], ref.prim[q, a]) <= 1e-8, q
         assert l1_rel(g.xI, ref.xI) <= 1e-8
@@ -156,8 +163,12 @@ def test_bm1d_one_step_matches_converged_oracle(gpu_available):
     # 1e-12 for >= 99 % of cells; the rest (relativistic cells, where a root one
     # ulp away moves rho by ~lfac^2 ulp) within 2e-12 or 10x the solver sensitivity
     worst, frac = within_sensitivity(got, ref, sens, 4. / 3., rtol=2e-12, k=10.0, qs=(0, 1, 2, 4, 6, 7))
-    assert max(worst.values()) <= 1.0, (worst, frac)
     _, frac12 = within_sensitivity(got, ref, sens, 4. / 3., rtol=1e-12, k=10.0, qs=(0, 1, 2, 4, 6, 7))
+    record("worst/bound", max(worst.values()), 1.0)
+    record("cells within 1e-12", min(frac12.values()), 0.99, "higher")
+    record("x rel", max(np.max(np.abs(got.x - ref.x) / np.abs(ref.x)), np.max(np.abs(got.xI - ref.xI) / np.abs(ref.xI))),
+           1e-12)
+    assert max(worst.values()) <= 1.0, (worst, frac)
     assert min(frac12.values()) >= 0.99, frac12
     # positions at 1e-12; widths dx = xR - xL relative to the position they are
     # differences of (a width of 1e3 at r = 5.5e6 carries 5.5e3 ulps of x)
@@ -185,6 +196,10 @@ def test_bm1d_regrid_decisions_bit_exact(gpu_available):
         g.close()
         ps.regrid()
         ref = ps.snapshot()
+        record(f"regrid {k} cell-count difference", abs(got.ntrack - ref.ntrack), 0)
+        if got.ntrack == ref.ntrack:
+            record(f"regrid {k} geometry/dt_loc values not bit-equal",
+                   sum(int(np.sum(getattr(got, f) != getattr(ref, f))) for f in ("x", "dx", "xI", "dt_loc")), 0)
         assert got.ntrack == ref.ntrack, k
         for f in ("x", "dx", "xI", "dt_loc"):
             assert np.array_equal(getattr(got, f), getattr(ref, f)), (k, f)
@@ -206,14 +221,19 @@ def test_bm1d_1000_steps(gpu_available):
     _, problems = _gpu()
     g = _bm_gpu(BM_CFG0)
     ps = _bm_port(BM_CFG0)
+    g_steps = 0
     for chunk in (1, 9, 90, 900):
         st = g.step(chunk)
         assert st["status"] == 0 and st["c2p_fallbacks"] == 0
         ps.step(chunk)
         got = problems.unpack(g.download(), 0, g.offsets)
         ref = ps.snapshot()
+        record(f"after {g_steps + chunk} steps: cell-count difference", abs(got.ntrack - ref.ntrack), 0)
         assert got.ntrack == ref.ntrack, (chunk, got.ntrack, ref.ntrack)
         a = slice(2, got.ntrack - 2)
+        record(f"after {g_steps + chunk} steps: L1 max over slots",
+               max(l1_rel(got.prim[q, a], ref.prim[q, a]) for q in (0, 1, 2, 4, 6, 7)), 1e-8)
+        g_steps += chunk
         for q in (0, 1, 2, 4, 6, 7):
             assert l1_rel(got.prim[q, a], ref.prim[q, a]) <= 1e-8, (chunk, q)
         assert l1_rel(got.x, ref.x) <= 1e-10
@@ -245,6 +265,7 @@ def test_bm1d_analytic_error_matches_reference(gpu_available):
         return np.sum(w * np.abs(rho_num - rho)) / np.sum(w * rho)
 
     e_gpu, e_ref = l1_vs_bm(got), l1_vs_bm(ref)
+    record("|err_gpu - err_ref| / err_ref", abs(e_gpu - e_ref) / e_ref, 1e-6)
     assert abs(e_gpu - e_ref) <= 1e-6 * e_ref, (e_gpu, e_ref)
 
 
@@ -271,8 +292,10 @@ def test_batched_bm1d_runs(gpu_available):
         ps.step(20)
         ref = ps.snapshot()
         got = problems.unpack(out, r, g.offsets)
+        record(f"run {r} cell-count difference", abs(got.ntrack - ref.ntrack), 0)
         assert got.ntrack == ref.ntrack, r
         a = slice(2, got.ntrack - 2)
+        record(f"run {r} L1 max over slots", max(l1_rel(got.prim[q, a], ref.prim[q, a]) for q in (0, 1, 2)), 1e-8)
         for q in (0, 1, 2):
             assert l1_rel(got.prim[q, a], ref.prim[q, a]) <= 1e-8, (r, q)
     g.close()
@@ -305,6 +328,8 @@ def test_cons2prim_kernel_matches_tight_oracle(gpu_available):
         E = cons[0] + cons[1]
         # rho and u inherit eps*lfac^2 from lfac = (1 - S^2/W^2)^(-1/2)
         cond = 1e-12 + 64 * 2.2e-16 * lg ** 2
+        record(f"nq{nq} rho err / bound", np.max(np.abs(gp[0] - rp[0]) / rp[0] / cond), 1.0)
+        record(f"nq{nq} p err vs max(p, 1e-2 E)", np.max(np.abs(gp[1] - rp[1]) / np.maximum(rp[1], 1e-2 * E)), 1e-12)
         assert np.all(np.abs(gp[0] - rp[0]) / rp[0] <= cond)
         assert np.all(np.abs(gp[2] - rp[2]) / np.maximum(np.abs(rp[2]), 1e-12) <= cond)
         assert np.max(np.abs(gp[1] - rp[1]) / np.maximum(rp[1], 1e-2 * E)) <= 1e-12
@@ -370,6 +395,8 @@ def test_full_size_batch_properties(gpu_available):
         assert np.all(np.diff(tr.xI[1:tr.ntrack - 2]) > 0)  # interfaces of active cells stay ordered
         if r in sample:
             ref = _port_tube(setups[r], 3)
+            record(f"tube {r} L1 max over slots", max(l1_rel(tr.prim[q, a], ref.prim[q, a]) for q in (0, 1, 2)),
+                   1e-10)
             for q in (0, 1, 2):
                 assert l1_rel(tr.prim[q, a], ref.prim[q, a]) <= 1e-10
     g.close()
@@ -402,6 +429,8 @@ def test_synge_eos_bm1d(gpu_available):
     assert got.ntrack == ref.ntrack
     assert abs(got.t - ref.t) <= 1e-14 * ref.t
     err = _tol_errors(got, ref, 5. / 3., 10)
+    record("one step x/xI rel", max(err["x"], err["xI"]), 1e-12)
+    record("one step max rel over slots 0,1,4,6,7", max(err[q] for q in (0, 1, 4, 6, 7)), 1e-9)
     assert err["x"] <= 1e-12 and err["xI"] <= 1e-12, err
     for q in (0, 1, 4, 6, 7):
         assert err[q] <= 1e-9, (q, err)
@@ -409,8 +438,10 @@ def test_synge_eos_bm1d(gpu_available):
     assert st["status"] == 0 and st["c2p_fallbacks"] == 0
     got = problems.unpack(g.download(), 0, g.offsets)
     ref = plain[40]
+    record("40 steps cell-count difference", abs(got.ntrack - ref.ntrack), 0)
     assert got.ntrack == ref.ntrack
     a = slice(2, got.ntrack - 2)
+    record("40 steps L1 max over slots", max(l1_rel(got.prim[q, a], ref.prim[q, a]) for q in (0, 1, 2)), 1e-8)
     for q in (0, 1, 2):
         assert l1_rel(got.prim[q, a], ref.prim[q, a]) <= 1e-8, q
     g.close()
