@@ -51,14 +51,16 @@ constexpr int kThreads = 256;
 
 struct Stats2 {
   unsigned long long c2p_calls, c2p_iters, c2p_fallbacks, c2p_max_iters, splits, merges, zone_updates;
+  unsigned long long c2p_guesses;
 };
 
 __device__ void add_stats(Stats2 *S, unsigned long long calls, unsigned long long iters, unsigned long long fb,
-                          unsigned long long mx) {
+                          unsigned long long mx, unsigned long long guesses = 0) {
   for (int o = 16; o > 0; o >>= 1) {
     calls += __shfl_xor_sync(0xffffffffu, calls, o);
     iters += __shfl_xor_sync(0xffffffffu, iters, o);
     fb += __shfl_xor_sync(0xffffffffu, fb, o);
+    guesses += __shfl_xor_sync(0xffffffffu, guesses, o);
     const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, mx, o);
     mx = m2 > mx ? m2 : mx;
   }
@@ -66,6 +68,7 @@ __device__ void add_stats(Stats2 *S, unsigned long long calls, unsigned long lon
     atomicAdd(&S->c2p_calls, calls);
     atomicAdd(&S->c2p_iters, iters);
     if (fb) atomicAdd(&S->c2p_fallbacks, fb);
+    if (guesses) atomicAdd(&S->c2p_guesses, guesses);
     atomicMax(&S->c2p_max_iters, mx);
   }
 }
@@ -241,20 +244,35 @@ __global__ void k_iface(Grid2 G, int stage) {
 // cores, mlp.cuh).  The network sees |S| = sqrt(S_r^2 + (S_theta / r)^2), the
 // momentum magnitude cons2prim solves with; a non-finite or non-positive
 // guess keeps the warm start.
+// The learned start of the 2D cell update: f at the warm start first; the
+// network's pressure replaces the warm start only where |f| exceeds
+// mlp::kGuessGate of E (c2p[4] counts those calls), and runs only when a lane
+// of the warp needs it.
 struct LearnedStart {
   const mlp::InferSmem *inf;
-  __device__ void operator()(const double *cons, double *prim, bool on, double r) const {
-    float f[3] = {0.f, 0.f, 0.f}, o[2] = {0.f, 0.f};
-    if (on) {
-      const double s1 = cons[SS1], s2 = cons[SS2] / r;
-      mlp::features(cons[DEN], cons[TAU], sqrt(s1 * s1 + s2 * s2), f);
+  __device__ const C2PStart *operator()(const Phys &ph, const double *cons, double *prim, bool upd, double r,
+                                        C2PStart &wbuf, unsigned long long *c2p) const {
+    bool need = false;
+    if (upd) {
+      const C2PInput2 in = c2p_input(cons, prim, r);
+      wbuf = c2p_start<Cfg2>(ph, in.D, in.S, in.S2, in.E, in.pCand);
+      need = !(fabs(wbuf.f) <= mlp::kGuessGate * in.E);
     }
-    __syncwarp();
-    mlp::infer_warp(*inf, f, o);
-    if (on) {
-      const double pg = mlp::guess_pressure(cons[DEN], o[0]);
-      if (isfinite(pg) && pg > 0.) prim[PPP] = pg;
+    if (__any_sync(0xffffffffu, need)) {
+      float f[3] = {0.f, 0.f, 0.f}, o[2] = {0.f, 0.f};
+      if (need) {
+        const double s1 = cons[SS1], s2 = cons[SS2] / r;
+        mlp::features(cons[DEN], cons[TAU], sqrt(s1 * s1 + s2 * s2), f);
+      }
+      __syncwarp();
+      mlp::infer_warp(*inf, f, o);
+      if (need) {
+        const double pg = mlp::guess_pressure(cons[DEN], o[0]);
+        if (isfinite(pg) && pg > 0.) prim[PPP] = pg;
+        c2p[4] += 1;
+      }
     }
+    return need ? nullptr : &wbuf;
   }
 };
 
@@ -265,7 +283,7 @@ struct LearnedStart {
 template <bool GUESS>
 __global__ void __launch_bounds__(kThreads, GB2_MINB_UP)
     k_update(Phys ph, Params2 P, Grid2 G, int stage, Stats2 *S, const float *guess) {
-  unsigned long long c2p[4] = {0, 0, 0, 0};
+  unsigned long long c2p[5] = {0, 0, 0, 0, 0};  // calls, iterations, fallbacks, max, learned starts
   if (!GUESS) {
     FOR_LIVE_CELLS(G, j, i) update_cell(ph, P, G, j, i, stage, c2p, true, WarmStart{});
   } else {
@@ -283,7 +301,7 @@ __global__ void __launch_bounds__(kThreads, GB2_MINB_UP)
       update_cell(ph, P, G, j, i, stage, c2p, live, ls);
     }
   }
-  add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3]);
+  add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3], c2p[4]);
 }
 
 // Grid::printCols' side effect with shock detection (text2d.cpp:147-153):
@@ -311,6 +329,7 @@ struct gamma_2d {
   long long NC = 0;
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
+  bool no_graphs = false;  // gamma_2d_use_graphs(ctx, 0): launch each step's kernels directly
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<void *> allocs;
@@ -377,36 +396,10 @@ int ghost_blocks(const gamma_2d *c, bool reset) {
   return (int)std::max(1LL, std::min((n + kThreads - 1) / kThreads, 148LL * 8));
 }
 
-// The first part of a step: regrid, reset shocks, ghosts and the stage-1
-// fluxes (everything before collect_dt).
-int enqueue_prepare(gamma_2d *c) {
-  const Phys ph = phys_of(c->cfg);
-  const Params2 P = params_of(c->par);
-  const Grid2 &G = c->G;
-  cudaStream_t s = c->stream;
-  const int nb = cell_blocks(c);
-  k_regrid_check<<<1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst);
-  k_regrid<<<1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst, 1);
-  if (c->cfg.ntheta > 1) {
-    k_regrid_check<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst + 1);
-    k_regrid<<<c->cfg.ntheta - 1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst + 1, 0);
-  }
-  k_ghosts_copy<<<ghost_blocks(c, true), kThreads, 0, s>>>(G, 1);
-  k_ghost_cells<<<c->NJ, 32, 0, s>>>(G);
-  k_prefix<<<1, 1024, 0, s>>>(G);
-  k_mv<<<nb, kThreads, 0, s>>>(ph, P, G);
-  k_cellmv<<<nb, kThreads, 0, s>>>(G);
-  k_stale_clear<<<(c->NJ + 255) / 256, 256, 0, s>>>(G);
-  k_stale<<<(c->NJ + 127) / 128, 128, 0, s>>>(G);
-  k_tgrad<<<nb, kThreads, 0, s>>>(G);
-  k_f1own<<<nb, kThreads, 0, s>>>(ph, G);
-  k_f1gather<<<nb, kThreads, 0, s>>>(ph, G);
-  G2_CUDA(c, cudaGetLastError());
-  return GAMMA_OK;
-}
-
-// one step's launches on the context's stream
-int enqueue_step(gamma_2d *c) {
+// One step's launches on the context's stream.  upto > 0 stops after the
+// flux passes of stage `upto` (everything before that stage's collect_dt or
+// update): the diagnostics of gamma_2d_prepare_stage.
+int enqueue_step_until(gamma_2d *c, int upto) {
   const Phys ph = phys_of(c->cfg);
   const Params2 P = params_of(c->par);
   const Grid2 &G = c->G;
@@ -430,6 +423,10 @@ int enqueue_step(gamma_2d *c) {
     k_tgrad<<<nb, kThreads, 0, s>>>(G);
     k_f1own<<<nb, kThreads, 0, s>>>(ph, G);
     k_f1gather<<<nb, kThreads, 0, s>>>(ph, G);
+    if (stage == upto) {
+      G2_CUDA(c, cudaGetLastError());
+      return GAMMA_OK;
+    }
     if (stage == 1) {
       k_dtpart<<<nb, kThreads, 0, s>>>(G);
       k_dtfinal<<<1, kThreads, 0, s>>>(G, nb, c->cfg.cfl);
@@ -445,6 +442,8 @@ int enqueue_step(gamma_2d *c) {
   G2_CUDA(c, cudaGetLastError());
   return GAMMA_OK;
 }
+
+int enqueue_step(gamma_2d *c) { return enqueue_step_until(c, 0); }
 
 }  // namespace
 
@@ -661,11 +660,23 @@ GAMMA_API int gamma_2d_upload(gamma_2d_t *ctx, const int *ntrack, const double *
   return GAMMA_OK;
 }
 
+GAMMA_API int gamma_2d_use_graphs(gamma_2d_t *ctx, int on) {
+  if (!ctx) return GAMMA_ERR_INVALID;
+  ctx->no_graphs = on == 0;
+  return GAMMA_OK;
+}
+
 GAMMA_API int gamma_2d_step(gamma_2d_t *ctx, int nsteps, gamma_step_stats_t *stats) {
   if (!ctx || nsteps < 0) return GAMMA_ERR_INVALID;
   gamma_2d *c = ctx;
   G2_CUDA(c, cudaMemsetAsync(c->d_stats, 0, sizeof(Stats2), c->stream));
-  if (!c->exec && nsteps > 0) {
+  if (c->no_graphs) {  // every launch of every step from the host
+    G2_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    for (int k = 0; k < nsteps; ++k) {
+      const int rc = enqueue_step(c);
+      if (rc != GAMMA_OK) return rc;
+    }
+  } else if (!c->exec && nsteps > 0) {
     G2_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     const int rc = enqueue_step(c);
     cudaGraph_t g = nullptr;
@@ -675,8 +686,10 @@ GAMMA_API int gamma_2d_step(gamma_2d_t *ctx, int nsteps, gamma_step_stats_t *sta
     c->graph = g;
     G2_CUDA(c, cudaGraphInstantiate(&c->exec, c->graph, 0));
   }
-  G2_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-  for (int k = 0; k < nsteps; ++k) G2_CUDA(c, cudaGraphLaunch(c->exec, c->stream));
+  if (!c->no_graphs) {
+    G2_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    for (int k = 0; k < nsteps; ++k) G2_CUDA(c, cudaGraphLaunch(c->exec, c->stream));
+  }
   G2_CUDA(c, cudaEventRecord(c->ev1, c->stream));
   if (stats) {
     Stats2 h;
@@ -695,6 +708,7 @@ GAMMA_API int gamma_2d_step(gamma_2d_t *ctx, int nsteps, gamma_step_stats_t *sta
     stats->c2p_max_iters = (int)h.c2p_max_iters;
     stats->status = status == 30 ? GAMMA_ERR_NEG_DT : (status ? GAMMA_ERR_INVALID : GAMMA_OK);
     stats->device_ms = ms;
+    stats->c2p_guesses = h.c2p_guesses;
   }
   return GAMMA_OK;
 }
@@ -729,9 +743,11 @@ GAMMA_API int gamma_2d_download(gamma_2d_t *ctx, int *ntrack, double *t, double 
   return GAMMA_OK;
 }
 
-GAMMA_API int gamma_2d_prepare(gamma_2d_t *ctx) {
-  if (!ctx) return GAMMA_ERR_INVALID;
-  const int rc = enqueue_prepare(ctx);
+GAMMA_API int gamma_2d_prepare(gamma_2d_t *ctx) { return gamma_2d_prepare_stage(ctx, 1); }
+
+GAMMA_API int gamma_2d_prepare_stage(gamma_2d_t *ctx, int stage) {
+  if (!ctx || stage < 1 || stage > (ctx->cfg.timestep == GAMMA_TS_EULER ? 1 : 3)) return GAMMA_ERR_INVALID;
+  const int rc = enqueue_step_until(ctx, stage);
   if (rc != GAMMA_OK) return rc;
   G2_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return GAMMA_OK;

@@ -15,11 +15,45 @@
 #include <vector>
 
 #include "io.h"
+#include "problem_module.cuh"
 #include "smem_limit.h"
 #include "track_step.cuh"
 #include "tune.h"
 
 namespace gb {
+
+// The problem registry.  Module files register from their static
+// initialisers (GAMMA_PROBLEM_MODULE), in any order; these arrays are
+// zero-initialised before any of them runs.
+namespace {
+constexpr int kMaxProblems = 64;
+constexpr int kFirstFreeId = 16;  // ids below are the fixed GAMMA_PROBLEM_* values
+const ProblemEntry *g_problems[kMaxProblems];
+int g_nproblems;
+int g_next_free_id = kFirstFreeId;
+}  // namespace
+
+int register_problem(ProblemEntry *e) {
+  if (!e || g_nproblems >= kMaxProblems) return -1;
+  for (int k = 0; k < g_nproblems; ++k)
+    if (std::strcmp(g_problems[k]->name, e->name) == 0 || (e->id >= 0 && g_problems[k]->id == e->id)) return -1;
+  g_problems[g_nproblems++] = e;
+  if (e->id < 0) e->id = g_next_free_id++;
+  return e->id;
+}
+
+const ProblemEntry *find_problem(int id) {
+  for (int k = 0; k < g_nproblems; ++k)
+    if (g_problems[k]->id == id) return g_problems[k];
+  return nullptr;
+}
+
+int problem_id(const char *name) {
+  if (!name) return -1;
+  for (int k = 0; k < g_nproblems; ++k)
+    if (std::strcmp(g_problems[k]->name, name) == 0) return g_problems[k]->id;
+  return -1;
+}
 
 cudaError_t raise_smem_limit(const void *fn, size_t bytes) {
   static std::mutex mu;
@@ -39,15 +73,13 @@ cudaError_t raise_smem_limit(const void *fn, size_t bytes) {
 
 namespace {
 
-enum Kind { KIND_CART = 0, KIND_SPH = 1 };
-
 constexpr int kBlock = 128;
 
 }  // namespace
 
 struct gamma_ctx {
   gamma_config_t cfg{};
-  int kind = KIND_CART;
+  const gb::ProblemEntry *prob = nullptr;  // the problem module
   int nq = 0, nqs = 0;
   int nruns = 0;
   int max_cap = 0;
@@ -88,24 +120,35 @@ int fail_cuda(gamma_ctx *c, cudaError_t e, const char *what) {
     if (e_ != cudaSuccess) return fail_cuda(ctx, e_, #call); \
   } while (0)
 
-int check_cfg(const gamma_config_t *cfg, int *kind) {
-  if (!cfg) return GAMMA_ERR_INVALID;
-  if (cfg->ngst != 2) return GAMMA_ERR_INVALID;
-  if (!(cfg->gamma_ad > 1.) || !(cfg->cfl > 0.)) return GAMMA_ERR_INVALID;
-  if (cfg->timestep != GAMMA_TS_RK3 && cfg->timestep != GAMMA_TS_EULER) return GAMMA_ERR_INVALID;
+// The module set a configuration selects (Makefile GEOMETRY/HYDRO/RADIATION),
+// or -1 for a combination this library does not build.
+int modules_of(const gamma_config_t *cfg) {
+  if (!cfg || cfg->ngst != 2) return -1;
+  if (!(cfg->gamma_ad > 1.) || !(cfg->cfl > 0.)) return -1;
+  if (cfg->timestep != GAMMA_TS_RK3 && cfg->timestep != GAMMA_TS_EULER) return -1;
   if (cfg->geometry == GAMMA_GEOM_SPHERICAL1D && cfg->hydro == GAMMA_HYDRO_REL_SPH && cfg->nq == 10 &&
-      cfg->shock_detection && cfg->local_synchrotron && cfg->problem == GAMMA_PROBLEM_BM1D) {
-    *kind = KIND_SPH;
-    return GAMMA_OK;
-  }
-  if (cfg->geometry == GAMMA_GEOM_CARTESIAN && cfg->hydro == GAMMA_HYDRO_REL_CART && cfg->nq == 6 &&
-      !cfg->shock_detection && !cfg->local_synchrotron && cfg->problem == GAMMA_PROBLEM_TUBE &&
+      cfg->shock_detection && cfg->local_synchrotron)
+    return gamma_problem::MODULES_SPHERICAL1D;
+  if (cfg->geometry == GAMMA_GEOM_CARTESIAN && cfg->nq == 6 && !cfg->shock_detection && !cfg->local_synchrotron &&
       cfg->eos == GAMMA_EOS_IDEAL) {
-    *kind = KIND_CART;
-    return GAMMA_OK;
+    if (cfg->hydro == GAMMA_HYDRO_REL_CART) return gamma_problem::MODULES_CARTESIAN;
+    if (cfg->hydro == GAMMA_HYDRO_REL_CYL) return gamma_problem::MODULES_CARTESIAN_REL_CYL;
   }
-  return GAMMA_ERR_INVALID;
+  return -1;
 }
+
+// The configuration's problem module (INITIAL), which must run with the
+// configuration's module set.
+int check_cfg(const gamma_config_t *cfg, const gb::ProblemEntry **prob) {
+  const int m = modules_of(cfg);
+  if (m < 0) return GAMMA_ERR_INVALID;
+  const gb::ProblemEntry *e = gb::find_problem(cfg->problem);
+  if (!e || e->modules != m) return GAMMA_ERR_INVALID;
+  *prob = e;
+  return GAMMA_OK;
+}
+
+bool is_sph(const gamma_ctx *c) { return c->prob->modules == gamma_problem::MODULES_SPHERICAL1D; }
 
 gb::Phys phys_of(const gamma_config_t &c) {
   gb::Phys p;
@@ -120,38 +163,9 @@ gb::Phys phys_of(const gamma_config_t &c) {
   return p;
 }
 
-unsigned words_bytes(int max_cap) { return 4u * 4u * (unsigned)gb::regrid_words(max_cap); }
-
-template <class Cfg, bool GUESS>
-size_t smem_bytes(int max_cap) {
-  using TS = gb::TrackStep<Cfg, kBlock, GUESS>;
-  size_t b = sizeof(typename TS::Smem) + words_bytes(max_cap);
-  if (GUESS) b = ((b + 15u) & ~size_t(15)) + sizeof(gb::mlp::InferSmem);
-  return b;
-}
-
-template <class Cfg, bool GUESS>
-int configure_launch(gamma_ctx *c, int *grid, size_t *smem) {
-  auto kern = gb::track_step_kernel<Cfg, kBlock, GUESS>;
-  *smem = smem_bytes<Cfg, GUESS>(c->max_cap);
-  GB_CUDA(c, gb::raise_smem_limit((const void *)kern, *smem));
-  int dev = 0, nsm = 0, occ = 0;
-  GB_CUDA(c, cudaGetDevice(&dev));
-  GB_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  GB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlock, *smem));
-  if (occ < 1) occ = 1;
-  *grid = std::min(c->nruns, nsm * occ);
-  return GAMMA_OK;
-}
-
-template <class Cfg, bool GUESS>
-int launch_step(gamma_ctx *c, int nsteps, int regrid_only) {
-  const int grid = GUESS ? c->grid_guess : c->grid;
-  const size_t smem = GUESS ? c->smem_guess : c->smem;
-  gb::track_step_kernel<Cfg, kBlock, GUESS><<<grid, kBlock, smem, c->stream>>>(
-      c->T, phys_of(c->cfg), nsteps, c->d_order, c->nruns, c->d_queue, c->d_stats, regrid_only,
-      words_bytes(c->max_cap));
-  GB_CUDA(c, cudaGetLastError());
+// Launch shape v (with the learned guess: v = 0) of the context's step kernel.
+int configure_launch(gamma_ctx *c, int v, bool guess, int *grid, size_t *smem) {
+  GB_CUDA(c, c->prob->configure(v, guess, c->nruns, c->max_cap, grid, smem));
   return GAMMA_OK;
 }
 
@@ -210,8 +224,8 @@ GAMMA_API void *gamma_gpu_stream(gamma_ctx_t *ctx) { return ctx ? (void *)ctx->s
 GAMMA_API int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *capacity, gamma_ctx_t **out) {
   if (!out || nruns <= 0 || !capacity) return GAMMA_ERR_INVALID;
   *out = nullptr;
-  int kind;
-  if (check_cfg(cfg, &kind) != GAMMA_OK) return GAMMA_ERR_INVALID;
+  const gb::ProblemEntry *prob = nullptr;
+  if (check_cfg(cfg, &prob) != GAMMA_OK) return GAMMA_ERR_INVALID;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GAMMA_ERR_NO_DEVICE;
   int dev = 0;
@@ -221,7 +235,7 @@ GAMMA_API int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *
 
   gamma_ctx *c = new gamma_ctx();
   c->cfg = *cfg;
-  c->kind = kind;
+  c->prob = prob;
   c->nq = cfg->nq;
   c->nqs = cfg->nq - 1;
   c->nruns = nruns;
@@ -274,10 +288,12 @@ GAMMA_API int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *
   GB_ALLOC(T.xI0, N * d);
   GB_ALLOC(T.fl1, nqs * N * d);
   GB_ALLOC(T.v1, N * d);
-  if (kind == KIND_SPH) {
+  if (cfg->shock_detection) {
     GB_ALLOC(T.sd, N * d);
     GB_ALLOC(T.pspec, N * d);
     GB_ALLOC(T.shocked, (size_t)N);
+  }
+  if (prob->regrid) {
     gb::RegridScratch &S = T.rg;
     S.N = N;
     GB_ALLOC(S.nprim, nqs * 2 * N * d);
@@ -297,11 +313,11 @@ GAMMA_API int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *
   long long *d_off;
   int *d_cap;
   gb::RunState *d_run;
-  gb::RunParams *d_par;
+  double *d_par;
   GB_ALLOC(d_off, nruns * sizeof(long long));
   GB_ALLOC(d_cap, nruns * sizeof(int));
   GB_ALLOC(d_run, nruns * sizeof(gb::RunState));
-  GB_ALLOC(d_par, nruns * sizeof(gb::RunParams));
+  GB_ALLOC(d_par, (size_t)nruns * gamma_problem::PARAM_WORDS * d);
   GB_ALLOC(c->d_order, nruns * sizeof(int));
   GB_ALLOC(c->d_queue, sizeof(int));
   GB_ALLOC(c->d_stats, sizeof(gb::StepStats));
@@ -317,8 +333,7 @@ GAMMA_API int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *
       cudaSuccess)
     return fail(e, "copy capacities");
   if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return fail(e, "sync");
-  int rc = kind == KIND_SPH ? configure_launch<gb::CfgSph, false>(c, &c->grid, &c->smem)
-                            : configure_launch<gb::CfgCart, false>(c, &c->grid, &c->smem);
+  int rc = configure_launch(c, 0, false, &c->grid, &c->smem);
   if (rc != GAMMA_OK) {
     gamma_gpu_destroy(c);
     return rc;
@@ -334,13 +349,37 @@ GAMMA_API int gamma_gpu_layout(const gamma_ctx_t *ctx, long long *offsets, long 
   return GAMMA_OK;
 }
 
-GAMMA_API int gamma_gpu_set_params(gamma_ctx_t *ctx, const gamma_run_params_t *params) {
-  if (!ctx || !params) return GAMMA_ERR_INVALID;
-  static_assert(sizeof(gamma_run_params_t) == sizeof(gb::RunParams), "run parameter record layout");
-  GB_CUDA(ctx, cudaMemcpyAsync((void *)ctx->T.par, params, ctx->nruns * sizeof(gb::RunParams),
-                               cudaMemcpyHostToDevice, ctx->stream));
+GAMMA_API int gamma_gpu_set_params_words(gamma_ctx_t *ctx, const double *words, int nwords) {
+  if (!ctx || !words || nwords < 0 || nwords > gamma_problem::PARAM_WORDS) return GAMMA_ERR_INVALID;
+  constexpr int W = gamma_problem::PARAM_WORDS;
+  std::vector<double> all((size_t)ctx->nruns * W, 0.);
+  for (int r = 0; r < ctx->nruns; ++r) std::copy(words + (size_t)r * nwords, words + (size_t)(r + 1) * nwords,
+                                                 all.begin() + (size_t)r * W);
+  GB_CUDA(ctx, cudaMemcpyAsync((void *)ctx->T.par, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice,
+                               ctx->stream));
   GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return GAMMA_OK;
+}
+
+GAMMA_API int gamma_gpu_set_params(gamma_ctx_t *ctx, const gamma_run_params_t *params) {
+  static_assert(sizeof(gamma_run_params_t) % sizeof(double) == 0, "run parameter record layout");
+  constexpr int n = (int)(sizeof(gamma_run_params_t) / sizeof(double));
+  static_assert(n <= gamma_problem::PARAM_WORDS, "run parameter record layout");
+  return gamma_gpu_set_params_words(ctx, reinterpret_cast<const double *>(params), n);
+}
+
+GAMMA_API int gamma_gpu_problem_id(const char *name) { return gb::problem_id(name); }
+
+GAMMA_API int gamma_gpu_initial_state(const gamma_config_t *cfg, const double *params, int nwords, int cap,
+                                      int *ntrack, double *t, double *prim, double *x, double *dx, double *xI,
+                                      double *dt_loc) {
+  const gb::ProblemEntry *prob = nullptr;
+  if (check_cfg(cfg, &prob) != GAMMA_OK || nwords < 0 || nwords > gamma_problem::PARAM_WORDS || cap < 7)
+    return GAMMA_ERR_INVALID;
+  if (!ntrack || !t || !prim || !x || !dx || !xI || !dt_loc || (nwords > 0 && !params)) return GAMMA_ERR_INVALID;
+  double words[gamma_problem::PARAM_WORDS] = {};
+  std::copy(params, params + nwords, words);
+  return prob->initial_state(phys_of(*cfg), words, cap, ntrack, t, prim, x, dx, xI, dt_loc);
 }
 
 GAMMA_API int gamma_gpu_upload(gamma_ctx_t *ctx, const int *ntrack, const double *t, const long long *it, const double *prim,
@@ -398,27 +437,15 @@ int enqueue_steps(gamma_ctx_t *ctx, int nsteps, int regrid_only) {
   GB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(int), ctx->stream));
   GB_CUDA(ctx, cudaMemsetAsync(ctx->d_stats, 0, sizeof(gb::StepStats), ctx->stream));
   const bool guess = ctx->T.mlp != nullptr && !regrid_only;
-  int rc;
-  if (!guess && ctx->variant > 0) {  // a tuned launch shape of the plain kernel
-    const int v = ctx->variant;
-    const cudaError_t e =
-        ctx->kind == KIND_SPH
-            ? gb::tune::launch_sph(v, ctx->vgrid[v], ctx->vsmem[v], ctx->stream, ctx->T, phys_of(ctx->cfg), nsteps,
-                                   ctx->d_order, ctx->nruns, ctx->d_queue, ctx->d_stats, regrid_only,
-                                   words_bytes(ctx->max_cap))
-            : gb::tune::launch_cart(v, ctx->vgrid[v], ctx->vsmem[v], ctx->stream, ctx->T, phys_of(ctx->cfg),
-                                    nsteps, ctx->d_order, ctx->nruns, ctx->d_queue, ctx->d_stats, regrid_only,
-                                    words_bytes(ctx->max_cap));
-    if (e != cudaSuccess) return fail_cuda(ctx, e, "variant launch");
-    rc = GAMMA_OK;
-  } else if (ctx->kind == KIND_SPH) {
-    rc = guess ? launch_step<gb::CfgSph, true>(ctx, nsteps, regrid_only)
-               : launch_step<gb::CfgSph, false>(ctx, nsteps, regrid_only);
-  } else {
-    rc = guess ? launch_step<gb::CfgCart, true>(ctx, nsteps, regrid_only)
-               : launch_step<gb::CfgCart, false>(ctx, nsteps, regrid_only);
-  }
-  return rc;
+  // the learned guess has the default shape only; the plain kernel the tuned one
+  const int v = guess ? 0 : ctx->variant;
+  const int grid = guess ? ctx->grid_guess : (v > 0 ? ctx->vgrid[v] : ctx->grid);
+  const size_t smem = guess ? ctx->smem_guess : (v > 0 ? ctx->vsmem[v] : ctx->smem);
+  const cudaError_t e = ctx->prob->launch(v, guess, grid, smem, ctx->stream, ctx->T, phys_of(ctx->cfg), nsteps,
+                                          ctx->d_order, ctx->nruns, ctx->d_queue, ctx->d_stats, regrid_only,
+                                          ctx->max_cap);
+  if (e != cudaSuccess) return fail_cuda(ctx, e, "step launch");
+  return GAMMA_OK;
 }
 
 int run_steps(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats, int regrid_only) {
@@ -462,6 +489,7 @@ int run_steps(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats, int regri
     stats->splits = h.splits;
     stats->merges = h.merges;
     stats->c2p_max_iters = h.c2p_max_iters;
+    stats->c2p_guesses = h.c2p_guesses;
     stats->status = h.status == 30 ? GAMMA_ERR_NEG_DT : (h.status ? GAMMA_ERR_INVALID : GAMMA_OK);
     stats->device_ms = ms;
   }
@@ -476,8 +504,7 @@ GAMMA_API int gamma_gpu_step(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *s
 GAMMA_API int gamma_gpu_set_guess(gamma_ctx_t *ctx, const float *params) {
   if (!ctx) return GAMMA_ERR_INVALID;
   if (params && !ctx->grid_guess) {
-    int rc = ctx->kind == KIND_SPH ? configure_launch<gb::CfgSph, true>(ctx, &ctx->grid_guess, &ctx->smem_guess)
-                                   : configure_launch<gb::CfgCart, true>(ctx, &ctx->grid_guess, &ctx->smem_guess);
+    int rc = configure_launch(ctx, 0, true, &ctx->grid_guess, &ctx->smem_guess);
     if (rc != GAMMA_OK) return rc;
   }
   ctx->T.mlp = params;
@@ -485,7 +512,7 @@ GAMMA_API int gamma_gpu_set_guess(gamma_ctx_t *ctx, const float *params) {
 }
 
 GAMMA_API int gamma_gpu_regrid(gamma_ctx_t *ctx, gamma_step_stats_t *stats) {
-  if (ctx && ctx->kind != KIND_SPH) return GAMMA_OK;  // problems without a regrid criterion
+  if (ctx && !ctx->prob->regrid) return GAMMA_OK;  // problems without a regrid criterion
   return run_steps(ctx, 1, stats, 1);
 }
 
@@ -521,8 +548,8 @@ GAMMA_API int gamma_gpu_download(gamma_ctx_t *ctx, int *ntrack, double *t, doubl
 }
 
 GAMMA_API int gamma_gpu_cons2prim(const gamma_config_t *cfg, double *cons, double *prim, int n, int *iters, void *stream) {
-  int kind;
-  if (check_cfg(cfg, &kind) != GAMMA_OK || !cons || !prim || n < 0) return GAMMA_ERR_INVALID;
+  const int modules = modules_of(cfg);
+  if (modules < 0 || !cons || !prim || n < 0) return GAMMA_ERR_INVALID;
   if (n == 0) return GAMMA_OK;
   cudaStream_t s = (cudaStream_t)stream;
   const int bs = 128;
@@ -530,8 +557,10 @@ GAMMA_API int gamma_gpu_cons2prim(const gamma_config_t *cfg, double *cons, doubl
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::min((n + bs - 1) / bs, nsm * 16);
-  if (kind == KIND_SPH)
+  if (modules == gamma_problem::MODULES_SPHERICAL1D)
     cons2prim_kernel<gb::CfgSph><<<grid, bs, 0, s>>>(phys_of(*cfg), cons, prim, n, iters);
+  else if (modules == gamma_problem::MODULES_CARTESIAN_REL_CYL)
+    cons2prim_kernel<gb::CfgCyl><<<grid, bs, 0, s>>>(phys_of(*cfg), cons, prim, n, iters);
   else
     cons2prim_kernel<gb::CfgCart><<<grid, bs, 0, s>>>(phys_of(*cfg), cons, prim, n, iters);
   if (cudaGetLastError() != cudaSuccess) return GAMMA_ERR_CUDA;
@@ -572,7 +601,7 @@ GAMMA_API int gamma_gpu_save(gamma_ctx_t *ctx, const char *path) {
   const int R = ctx->nruns;
   const size_t N = (size_t)ctx->N, d = sizeof(double);
   std::vector<gb::RunState> rs(R);
-  std::vector<gb::RunParams> par(R);
+  std::vector<double> par((size_t)R * gamma_problem::PARAM_WORDS);
   std::vector<double> buf((size_t)ctx->nqs * N);
   std::vector<unsigned char> sh(N);
   gb::io::CkptOut out(path);
@@ -582,10 +611,10 @@ GAMMA_API int gamma_gpu_save(gamma_ctx_t *ctx, const char *path) {
   out.block("config", &ctx->cfg, sizeof(ctx->cfg));
   out.block("capacity", ctx->cap.data(), R * sizeof(int));
   GB_CUDA(ctx, cudaMemcpyAsync(rs.data(), T.run, R * sizeof(gb::RunState), cudaMemcpyDeviceToHost, ctx->stream));
-  GB_CUDA(ctx, cudaMemcpyAsync(par.data(), T.par, R * sizeof(gb::RunParams), cudaMemcpyDeviceToHost, ctx->stream));
+  GB_CUDA(ctx, cudaMemcpyAsync(par.data(), T.par, par.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   out.block("runs", rs.data(), R * sizeof(gb::RunState));
-  out.block("params", par.data(), R * sizeof(gb::RunParams));
+  out.block("params", par.data(), par.size() * sizeof(double));
   auto arr = [&](const char *name, const void *src, size_t bytes) -> int {
     GB_CUDA(ctx, cudaMemcpyAsync(buf.data(), src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -623,9 +652,9 @@ GAMMA_API int gamma_gpu_load(gamma_ctx_t *ctx, const char *path) {
     return GAMMA_ERR_INVALID;
   if (!in.block("capacity", cap.data(), R * sizeof(int)) || cap != ctx->cap) return GAMMA_ERR_INVALID;
   std::vector<gb::RunState> rs(R);
-  std::vector<gb::RunParams> par(R);
+  std::vector<double> par((size_t)R * gamma_problem::PARAM_WORDS);
   if (!in.block("runs", rs.data(), R * sizeof(gb::RunState))) return GAMMA_ERR_IO;
-  if (!in.block("params", par.data(), R * sizeof(gb::RunParams))) return GAMMA_ERR_IO;
+  if (!in.block("params", par.data(), par.size() * sizeof(double))) return GAMMA_ERR_IO;
   std::vector<double> buf((size_t)ctx->nqs * N);
   std::vector<unsigned char> sh(N);
   auto arr = [&](const char *name, void *dst, size_t bytes) -> int {
@@ -650,7 +679,7 @@ GAMMA_API int gamma_gpu_load(gamma_ctx_t *ctx, const char *path) {
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rs[a].ntrack > rs[b].ntrack; });
   GB_CUDA(ctx, cudaMemcpyAsync(T.run, rs.data(), R * sizeof(gb::RunState), cudaMemcpyHostToDevice, ctx->stream));
-  GB_CUDA(ctx, cudaMemcpyAsync((void *)T.par, par.data(), R * sizeof(gb::RunParams), cudaMemcpyHostToDevice,
+  GB_CUDA(ctx, cudaMemcpyAsync((void *)T.par, par.data(), par.size() * sizeof(double), cudaMemcpyHostToDevice,
                                ctx->stream));
   GB_CUDA(ctx, cudaMemcpyAsync(ctx->d_order, order.data(), R * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -667,12 +696,8 @@ GAMMA_API int gamma_gpu_variant_info(int variant, int *threads, int *cells_per_t
 GAMMA_API int gamma_gpu_set_variant(gamma_ctx_t *ctx, int variant) {
   if (!ctx || variant < 0 || variant >= gb::tune::kVariants) return GAMMA_ERR_INVALID;
   if (variant > 0 && ctx->vgrid[variant] == 0) {
-    const cudaError_t e =
-        ctx->kind == KIND_SPH
-            ? gb::tune::configure_sph(variant, ctx->nruns, ctx->max_cap, &ctx->vgrid[variant], &ctx->vsmem[variant])
-            : gb::tune::configure_cart(variant, ctx->nruns, ctx->max_cap, &ctx->vgrid[variant],
-                                       &ctx->vsmem[variant]);
-    if (e != cudaSuccess) return fail_cuda(ctx, e, "variant set-up");
+    const int rc = configure_launch(ctx, variant, false, &ctx->vgrid[variant], &ctx->vsmem[variant]);
+    if (rc != GAMMA_OK) return rc;
   }
   ctx->variant = variant;
   return GAMMA_OK;

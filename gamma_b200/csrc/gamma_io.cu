@@ -119,8 +119,8 @@ int write_text1d(const char *path, const gamma_config_t &cfg, int ntrack, long l
     double p[10] = {0}, c[10] = {0};
     for (int q = 0; q < nq; ++q) p[q] = prim[q * stride + i];
     // Cell::S.cons at a dump: cons2prim ends with prim2cons (rel_sph.cpp:318)
-    if (is_sph(cfg)) prim2cons<CfgSph>(ph, p, c);
-    else prim2cons<CfgCart>(ph, p, c);
+    if (is_sph(cfg)) prim2cons<RefOrder<CfgSph>>(ph, p, c);
+    else prim2cons<RefOrder<CfgCart>>(ph, p, c);
     const double lfac = lfac_of(p[UU1]);
     // spherical1D and cartesian: dl = dx (spherical1D.cpp:23-33, cartesian.cpp:20-26)
     if (synch) {

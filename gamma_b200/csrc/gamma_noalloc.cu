@@ -27,14 +27,13 @@
 
 #include <mutex>
 
-#include "smem_limit.h"
-#include "track_step.cuh"
+#include "problem_module.cuh"
 
 namespace {
 
 constexpr size_t kNoAllocBytes = size_t(64) << 20;
-constexpr int kBlock = 128;
 constexpr int kMaxDevices = 64;
+constexpr size_t kParBytes = gamma_problem::PARAM_WORDS * sizeof(double);  // one run's parameter words
 
 // The workspace.  In host code this name is only a stand-in for the device
 // symbol: its device address comes from cudaGetSymbolAddress below.
@@ -85,15 +84,14 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
   // workspace layout; reject before touching anything if it does not fit.
   // The per-item bounds come first so that no size product below can wrap.
   constexpr int NQS = gb::CfgCart::NQ - 1;
-  if ((unsigned long long)total > kNoAllocBytes / sizeof(double) ||
-      (size_t)nruns > kNoAllocBytes / sizeof(gb::RunParams))
+  if ((unsigned long long)total > kNoAllocBytes / sizeof(double) || (size_t)nruns > kNoAllocBytes / kParBytes)
     return GAMMA_ERR_CAPACITY;
   const size_t n = (size_t)total;
   const size_t off_queue = 0;
   const size_t off_stats = align256(off_queue + sizeof(int));
   const size_t off_order = align256(off_stats + sizeof(gb::StepStats));
   const size_t off_par = align256(off_order + (size_t)nruns * sizeof(int));
-  const size_t off_u0 = align256(off_par + (size_t)nruns * sizeof(gb::RunParams));
+  const size_t off_u0 = align256(off_par + (size_t)nruns * kParBytes);
   const size_t off_xI0 = align256(off_u0 + NQS * n * sizeof(double));
   const size_t off_fl1 = align256(off_xI0 + n * sizeof(double));
   const size_t off_v1 = align256(off_fl1 + NQS * n * sizeof(double));
@@ -107,7 +105,7 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
 
   if (cudaMemsetAsync(ws + off_queue, 0, sizeof(int), s) != cudaSuccess) return GAMMA_ERR_CUDA;
   if (cudaMemsetAsync(ws + off_stats, 0, sizeof(gb::StepStats), s) != cudaSuccess) return GAMMA_ERR_CUDA;
-  if (cudaMemsetAsync(ws + off_par, 0, (size_t)nruns * sizeof(gb::RunParams), s) != cudaSuccess)
+  if (cudaMemsetAsync(ws + off_par, 0, (size_t)nruns * kParBytes, s) != cudaSuccess)
     return GAMMA_ERR_CUDA;
   identity_order<<<(nruns + 255) / 256, 256, 0, s>>>(reinterpret_cast<int *>(ws + off_order), nruns);
 
@@ -125,7 +123,7 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
   T.off = offsets;
   T.cap = capacity;
   T.run = reinterpret_cast<gb::RunState *>(runs);
-  T.par = reinterpret_cast<const gb::RunParams *>(ws + off_par);
+  T.par = reinterpret_cast<const double *>(ws + off_par);
 
   gb::Phys ph{};
   ph.gamma_ad = cfg->gamma_ad;
@@ -137,20 +135,18 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
   ph.eos_ws = cfg->eos_wavespeeds;
   ph.euler = cfg->timestep == GAMMA_TS_EULER;
 
-  auto kern = gb::track_step_kernel<gb::CfgCart, kBlock>;
-  const size_t smem = sizeof(gb::TrackStep<gb::CfgCart, kBlock>::Smem) + 4u * 4u * (size_t)gb::regrid_words(32);
-  // contexts launch the same kernel with larger limits: never lower them
-  if (gb::raise_smem_limit((const void *)kern, smem) != cudaSuccess) return GAMMA_ERR_CUDA;
-  int dev = 0, nsm = 0, occ = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return GAMMA_ERR_CUDA;
-  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return GAMMA_ERR_CUDA;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlock, smem) != cudaSuccess) return GAMMA_ERR_CUDA;
-  const int grid = nruns < nsm * (occ > 0 ? occ : 1) ? nruns : nsm * (occ > 0 ? occ : 1);
+  // the tube module's step kernel in its default launch shape (the module has
+  // no refinement criterion, so the capacity does not size any shared memory)
+  const gb::ProblemEntry *tube = gb::find_problem(GAMMA_PROBLEM_TUBE);
+  if (!tube) return GAMMA_ERR_INVALID;
+  int grid = 0;
+  size_t smem = 0;
+  if (tube->configure(0, false, nruns, 0, &grid, &smem) != cudaSuccess) return GAMMA_ERR_CUDA;
   auto *qs = reinterpret_cast<int *>(ws + off_queue);
   auto *st = reinterpret_cast<gb::StepStats *>(ws + off_stats);
-  kern<<<grid, kBlock, smem, s>>>(T, ph, nsteps, reinterpret_cast<const int *>(ws + off_order), nruns, qs, st, 0,
-                                  4u * 4u * (unsigned)gb::regrid_words(32));
-  if (cudaGetLastError() != cudaSuccess) return GAMMA_ERR_CUDA;
+  if (tube->launch(0, false, grid, smem, s, T, ph, nsteps, reinterpret_cast<const int *>(ws + off_order), nruns, qs,
+                   st, 0, 0) != cudaSuccess)
+    return GAMMA_ERR_CUDA;
 
   if (stats) {
     gb::StepStats h;
@@ -163,6 +159,7 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
     stats->splits = h.splits;
     stats->merges = h.merges;
     stats->c2p_max_iters = h.c2p_max_iters;
+    stats->c2p_guesses = h.c2p_guesses;
     stats->status = h.status == 30 ? GAMMA_ERR_NEG_DT : (h.status ? GAMMA_ERR_INVALID : GAMMA_OK);
     stats->device_ms = 0.f;
   }

@@ -44,13 +44,14 @@ __device__ __forceinline__ float dsilu(float z) {
   return s + z * s * (1.f - s);
 }
 
-// network inputs of a conserved state (D, tau, S_r)
+// network inputs of a conserved state (D, tau, S_r): the ratios and the
+// thermal part in FP64 (the thermal part cancels), the logarithms in FP32
 __device__ __forceinline__ void features(double D, double tau, double S, float f[3]) {
   const double s = fabs(S) / D, t = tau / D;
   const double th = t - (sqrt(1. + s * s) - 1.);
-  f[0] = (float)(log1p(s) * 0.125);
-  f[1] = (float)(log10(fmax(th, 1e-30)) * 0.1);
-  f[2] = (float)(log10(D) * (1. / 6.));
+  f[0] = log1pf((float)s) * 0.125f;
+  f[1] = __log10f(fmaxf((float)th, 1e-30f)) * 0.1f;
+  f[2] = __log10f((float)D) * (1.f / 6.f);
 }
 
 __device__ __forceinline__ void targets(double D, double p, double lfac, float y[2]) {
@@ -58,7 +59,14 @@ __device__ __forceinline__ void targets(double D, double p, double lfac, float y
   y[1] = (float)(log(lfac) * (1. / 3.));
 }
 
-__device__ __forceinline__ double guess_pressure(double D, float y0) { return D * exp(10. * (double)y0 - 14.); }
+__device__ __forceinline__ double guess_pressure(double D, float y0) {
+  return D * (double)__expf(10.f * y0 - 14.f);
+}
+
+// Inside a time step the previous pressure is the better start almost
+// everywhere (Newton stops after one or two iterations).  The network starts
+// cons2prim only where f at that warm start exceeds this fraction of E = D + tau.
+constexpr double kGuessGate = 1e-4;
 
 // FP32 forward of one sample; optional pre-activations and activations for
 // the backward pass (h1, h2 may be strided rows of shared memory)

@@ -15,6 +15,8 @@
 #include <cstdint>
 #include <math.h>
 
+#include "gamma_problem.h"
+
 #ifndef GB_HD
 #define GB_HD __device__ __forceinline__
 #endif
@@ -80,7 +82,15 @@ struct CfgCart {
   static constexpr bool SPH = false;    // rel_sph hydro and spherical1D geometry
   static constexpr bool SHOCK = false;  // SHOCK_DETECTION_
   static constexpr bool SYNCH = false;  // LOCAL_SYNCHROTRON_
-  static constexpr bool BM = false;     // Blandford-McKee problem hooks + regrid
+  static constexpr bool CYL = false;    // rel_cyl hydro (Hydro/rel_cyl.cpp)
+};
+
+// cartesian + rel_cyl (Hydro/rel_cyl.cpp, the HYDRO module whose GEOMETRY
+// partner, Geometry/cylindrical.cpp, does not compile): rel_cart with the
+// cylindrical source p/r on S_r, a root search only where |f| at the previous
+// pressure exceeds 1e-13, and a zero velocity below |S| = 1e-14 (NUM_Q = 6).
+struct CfgCyl : CfgCart {
+  static constexpr bool CYL = true;
 };
 
 // spherical1D + rel_sph + radiation_sph: NUM_Q = 10.
@@ -96,7 +106,17 @@ struct CfgSph {
   static constexpr bool SPH = true;
   static constexpr bool SHOCK = true;
   static constexpr bool SYNCH = true;
-  static constexpr bool BM = true;
+  static constexpr bool CYL = false;
+};
+
+// A module set with every formula in the reference's operation order, whatever
+// GB_FAST_ARITH says: for results that must equal the reference's bit for bit
+// (the text dump's conserved columns).
+template <class Cfg>
+struct RefOrder : Cfg {
+  static constexpr bool FAST = false;
+  static constexpr bool FAST_RIEMANN = false;
+  static constexpr bool FAST_ROOT = false;
 };
 
 // Run-time constants shared by every run of a context.
@@ -369,6 +389,22 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
   return f;
 }
 
+// f(p) of the cons2prim root search at its starting pressure, with the slope
+// and Lorentz factor the search reuses (c2p_start below).
+struct C2PStart {
+  double f, df, l2, lf;
+};
+
+// The root search's first evaluation, f at the starting pressure pCand.
+template <class Cfg>
+GB_HD C2PStart c2p_start(const Phys &ph, double D, double S, double S2, double E, double pCand) {
+  C2PStart w;
+  w.lf = -1.;
+  w.f = Cfg::FAST_ROOT ? c2p_f<Cfg>(ph, pCand, D, S2, E, &w.df, &w.l2)
+                       : c2p_f_ref<Cfg>(ph, pCand, D, S, E, &w.df, &w.l2, &w.lf);
+  return w;
+}
+
 // Pressure root of the cons2prim driver (rel_sph.cpp:243-286): the bracket,
 // its no-solution tests and the warm start pCand are the reference's; the
 // Brent search is replaced by safeguarded Newton-Raphson.  Returns the
@@ -377,9 +413,12 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
 // lfac_at (optional): the Lorentz factor 1/sqrt(|1 - S^2/(E+p)^2|) at the
 // returned pressure when the search evaluated f there (the same rounding as
 // f's), else -1.
+//
+// start (optional): f at pCand with its slope, as c2p_start evaluated it for
+// the same pCand; the search then does not evaluate it again.
 template <class Cfg>
 GB_HD double c2p_pressure_body(const Phys &ph, double D, double S, double S2, double E, double pCand,
-                               C2PStats *st, double *lfac_at) {
+                               C2PStats *st, double *lfac_at, const C2PStart *start) {
   auto fval = [&](double p, double *df, double *l2, double *lf, bool p_may_be_zero = false) -> double {
     return Cfg::FAST_ROOT ? c2p_f<Cfg>(ph, p, D, S2, E, df, l2)
                      : c2p_f_ref<Cfg>(ph, p, D, S, E, df, l2, lf, p_may_be_zero);
@@ -388,9 +427,18 @@ GB_HD double c2p_pressure_body(const Phys &ph, double D, double S, double S2, do
   // f at the warm start, with its slope: the search starts there when the
   // warm start lies in the bracket (f does not depend on whether df is asked for)
   double df0, l20, lf0 = -1.;
-  const double f_init = fval(pCand, &df0, &l20, &lf0);
+  double f_init;
+  if (start) {
+    f_init = start->f;
+    df0 = start->df;
+    l20 = start->l2;
+    lf0 = start->lf;
+  } else {
+    f_init = fval(pCand, &df0, &l20, &lf0);
+  }
   if (lfac_at) *lfac_at = lf0;
-  if (fabs(f_init) > 0.) {
+  // rel_cyl.cpp:161 searches only where |f| exceeds 1e-13 (rel_sph, rel_cart: 0)
+  if (fabs(f_init) > (Cfg::CYL ? 1.e-13 : 0.)) {
     double p_lo = fmax(0., (1. + 1e-13) * S - E);
     bool find_p = true;
     if (fval(p_lo, nullptr, nullptr, nullptr, true) < 0) find_p = false;
@@ -453,8 +501,8 @@ GB_HD double c2p_pressure_body(const Phys &ph, double D, double S, double S2, do
 
 template <class Cfg>
 GB_HD_OUTLINE double c2p_pressure_outline(const Phys &ph, double D, double S, double S2, double E, double pCand,
-                                          C2PStats *st, double *lfac_at) {
-  return c2p_pressure_body<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at);
+                                          C2PStats *st, double *lfac_at, const C2PStart *start) {
+  return c2p_pressure_body<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at, start);
 }
 
 // The cartesian step calls the search from one out-of-line copy: inlined at
@@ -463,26 +511,46 @@ GB_HD_OUTLINE double c2p_pressure_outline(const Phys &ph, double D, double S, do
 // keep it inline, which is as fast or faster there.
 template <class Cfg>
 GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double E, double pCand, C2PStats *st,
-                          double *lfac_at = nullptr) {
-  if (Cfg::SPH) return c2p_pressure_body<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at);
-  return c2p_pressure_outline<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at);
+                          double *lfac_at = nullptr, const C2PStart *start = nullptr) {
+  if (Cfg::SPH) return c2p_pressure_body<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at, start);
+  return c2p_pressure_outline<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at, start);
+}
+
+// What cons2prim's root search is given: D, E = D + tau, S and S^2 of the
+// momentum, and the starting pressure (the previous one, floored in rel_sph).
+struct C2PInput {
+  double D, E, ss, S2, S, pCand;
+};
+
+template <class Cfg>
+GB_HD C2PInput c2p_input(const double *cons, const double *prim) {
+  C2PInput in;
+  in.D = cons[DEN];
+  const double tau = cons[TAU];
+  in.E = in.D + tau;
+  in.ss = cons[SS1];
+  double S2 = 0.;
+  S2 += in.ss * in.ss;
+  in.S2 = S2;
+  in.S = Cfg::FAST_ROOT ? fabs(in.ss) : sqrt(S2);
+  in.pCand = Cfg::SPH ? fmax(1.e-13, prim[PPP]) : prim[PPP];
+  return in;
 }
 
 // FluidState::cons2prim (rel_sph.cpp:213-320; rel_cart.cpp:125-229).
 // On entry prim holds the previous primitives (pressure warm start); on exit
 // prim holds the recovered primitives and cons is rewritten by prim2cons.
-template <class Cfg>
-GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
-  const double D = cons[DEN];
-  const double tau = cons[TAU];
-  const double E = D + tau;
-  const double ss = cons[SS1];
-  double S2 = 0.;
-  S2 += ss * ss;
-  const double S = Cfg::FAST_ROOT ? fabs(ss) : sqrt(S2);
+// Hooks::cons2prim_user (the problem module's FluidState::cons2prim_user,
+// rel_sph.cpp:304) sees rho, p and u before the pressure floor; par is the
+// run's parameter words.
+// start (optional): c2p_start at this state's starting pressure.
+template <class Cfg, class Hooks = gamma_problem::Problem>
+GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st, const double *par = nullptr,
+                     const C2PStart *start = nullptr) {
+  const C2PInput in = c2p_input<Cfg>(cons, prim);
+  const double D = in.D, E = in.E, ss = in.ss, S2 = in.S2, S = in.S;
   double lf_root = -1.;
-  const double pCand =
-      c2p_pressure<Cfg>(ph, D, S, S2, E, Cfg::SPH ? fmax(1.e-13, prim[PPP]) : prim[PPP], st, &lf_root);
+  const double pCand = c2p_pressure<Cfg>(ph, D, S, S2, E, in.pCand, st, &lf_root, start);
 
   double p = pCand;
   double rho, uu;
@@ -502,7 +570,7 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
       lfac = 1. / sqrt(fabs(1. - v2));
     }
     rho = D / lfac;
-    if (fabs(S) == 0.) {
+    if (Cfg::CYL ? fabs(S) < 1.e-14 : fabs(S) == 0.) {  // rel_cyl.cpp:207
       uu = 0;
     } else {
       double v = sqrt(1. - 1. / (lfac * lfac));
@@ -510,6 +578,7 @@ GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st) {
       uu = lfac * v * (fabs(ss) == S ? (ss > 0. ? 1. : -1.) : ss / S);
     }
   }
+  Hooks::cons2prim_user(par, &rho, &p, &uu);
   if (Cfg::SPH) p = fmax(p, P_FLOOR);
   prim[PPP] = p;
   prim[RHO] = rho;

@@ -23,6 +23,7 @@ struct Cfg2 {
   static constexpr bool FAST = false;
   static constexpr bool FAST_RIEMANN = false;
   static constexpr bool FAST_ROOT = false;
+  static constexpr bool CYL = false;
   static constexpr int NQ = 10;
   static constexpr bool SPH = true;
   static constexpr bool SHOCK = true;
@@ -273,18 +274,38 @@ GB_HD bool compute_Sd(const Phys &ph, const St &S1, const St &S2, int dim, bool 
   return true;  // spectral index: p_ (VARIABLE_PSPEC_ disabled)
 }
 
-// FluidState::cons2prim (rel_sph.cpp:213-320) at radius r: warm start from
-// prim[PPP]; cons is rewritten by the closing prim2cons(r).
-GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, double r, C2PStats *st) {
-  double D = cons[DEN];
+// What the root search of cons2prim at radius r is given (rel_sph.cpp:215-250).
+struct C2PInput2 {
+  double D, E, ss[2], S2, S, pCand;
+};
+
+GB_HD C2PInput2 c2p_input(const double *cons, const double *prim, double r) {
+  C2PInput2 in;
+  in.D = cons[DEN];
   double tau = cons[TAU];
-  double E = D + tau;
-  double ss[2] = {cons[SS1], cons[SS2]};
-  ss[1] = qdiv(ss[1], r);
+  in.E = in.D + tau;
+  in.ss[0] = cons[SS1];
+  in.ss[1] = qdiv(cons[SS2], r);
   double S2 = 0.;
-  for (int d = 0; d < 2; ++d) S2 += ss[d] * ss[d];
-  double S = sqrt(S2);
-  double p = c2p_pressure<Cfg2>(ph, D, S, S2, E, fmax(1.e-13, prim[PPP]), st);
+  for (int d = 0; d < 2; ++d) S2 += in.ss[d] * in.ss[d];
+  in.S2 = S2;
+  in.S = sqrt(S2);
+  in.pCand = fmax(1.e-13, prim[PPP]);
+  return in;
+}
+
+// FluidState::cons2prim (rel_sph.cpp:213-320) at radius r: warm start from
+// prim[PPP]; cons is rewritten by the closing prim2cons(r).  start
+// (optional): c2p_start at this state's starting pressure.
+GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, double r, C2PStats *st,
+                     const C2PStart *start = nullptr) {
+  const C2PInput2 in = c2p_input(cons, prim, r);
+  double D = in.D;
+  double E = in.E;
+  double ss[2] = {in.ss[0], in.ss[1]};
+  double S2 = in.S2;
+  double S = in.S;
+  double p = c2p_pressure<Cfg2>(ph, D, S, S2, E, in.pCand, st, nullptr, start);
   double Ep2 = (E + p) * (E + p);
   double v2 = qdiv(S2, Ep2);
   double lf = 1. / sqrt(fabs(1. - v2));

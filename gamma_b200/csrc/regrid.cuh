@@ -1,5 +1,6 @@
 // Per-track AMR split/merge (Grid::regrid, src/Dimensions/1d.cpp:484-728) with
-// the Blandford-McKee refinement criterion (src/Initial/Tests/BM1D.cpp:277-319).
+// the problem module's refinement criterion (Hooks::check_cell_for_regrid, e.g.
+// src/Initial/Tests/BM1D.cpp:277-319).
 //
 // The reference walks the active cells left to right and acts immediately:
 // a split inserts a cell (the right half is examined next), a merge removes one
@@ -76,18 +77,6 @@ struct RegridView {
     return c;
   }
 };
-
-// checkCellForRegrid of BM1D.cpp:277-319 for a cell at position i.
-template <class Cfg>
-__device__ __forceinline__ int bm_criterion(const RunParams &P, double dx, double uu, int i, double iS, double rOut) {
-  double ar = dx / (rOut * P.dth);
-  double dist = i - iS;
-  if (0 < dist && dist < 10) ar *= 10;
-  double lfac = lfac_of(uu);
-  if (ar > P.split_AR * P.target_ar / pow(lfac, 3. / 2.)) return SPLIT;
-  if (ar < P.merge_AR * P.target_ar / pow(lfac, 3. / 2.)) return MERGE;
-  return SKIP;
-}
 
 __device__ __forceinline__ bool bit_of(const uint32_t *w, int k) { return (w[k >> 5] >> (k & 31)) & 1u; }
 
@@ -167,9 +156,9 @@ __device__ void split_cells(const RCell<Cfg> &cL, const RCell<Cfg> &c, const RCe
 }
 
 // Merge cell c with victim v (Grid::merge, 1d.cpp:665-728).
-template <class Cfg>
+template <class Cfg, class Hooks>
 __device__ void merge_cells(const Phys &ph, const RCell<Cfg> &c, const RCell<Cfg> &v, bool left, RCell<Cfg> &M,
-                            C2PStats *cs) {
+                            C2PStats *cs, const double *par) {
   constexpr int NQ = Cfg::NQ;
   double cc[NQ], cv[NQ], cons[NQ];
   prim2cons<Cfg>(ph, c.prim, cc);
@@ -183,7 +172,7 @@ __device__ void merge_cells(const Phys &ph, const RCell<Cfg> &c, const RCell<Cfg
   M.dx = c.dx + v.dx;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) M.prim[q] = c.prim[q];
-  cons2prim<Cfg>(ph, cons, M.prim, cs);
+  cons2prim<Cfg, Hooks>(ph, cons, M.prim, cs, par);
   M.dtl = c.dtl;
   if (left) {
     M.rif = c.rif;
@@ -201,9 +190,17 @@ __host__ __device__ constexpr int regrid_words(int cap) { return (cap + 31) / 32
 
 // Regrid one track; returns the new ntrack.  Called by all threads of the CTA.
 // words: 4 * regrid_words(cap) uint32 of shared memory.
-template <class Cfg, int BS>
+//
+// The criterion: Hooks::check_cell_for_regrid(par, dx, prim, i, iS, rOut) for
+// the cell at live position i, where iS is the live position of the rightmost
+// active cell marked by Hooks::regrid_marker (iLbnd+1 if none) and rOut the
+// centre of the outermost active cell -- the two things BM1D.cpp:285-301 reads
+// from the live track.  The criterion may depend on i - iS only through whether
+// 0 < i - iS < Hooks::REGRID_WINDOW, so a cell's decision in the original track
+// stays valid while that test gives the same answer as in the original track.
+template <class Cfg, class Hooks, int BS>
 __device__ int regrid_track(double *prim, long long N, double *x, double *dx, double *dtl, double *xI,
-                            long long off, int n, int cap, const Phys &ph, const RunParams &P,
+                            long long off, int n, int cap, const Phys &ph, const double *par,
                             const RegridScratch &S, uint32_t *words, unsigned long long &nsplit,
                             unsigned long long &nmerge) {
   constexpr int NQ = Cfg::NQ;
@@ -212,8 +209,12 @@ __device__ int regrid_track(double *prim, long long N, double *x, double *dx, do
   const int nw = regrid_words(cap);
   uint32_t *hpw = words, *spw = words + nw, *mgw = words + 2 * nw, *outhp = words + 3 * nw;
   __shared__ int s_hpmax, s_nnew, s_nseg, s_first;
-  const double thr = 1.5 * P.eta;
   const double rOut0 = x[off + iR0 - 1];
+  auto load = [&](long long g, double *p) {
+#pragma unroll
+    for (int s = 0; s < NQS; ++s) p[s < 3 ? s : s + 1] = prim[s * N + g];
+    p[UU2] = 0.;
+  };
 
   // ---- A. high-pressure bits and the original shock index
   if (threadIdx.x == 0) s_hpmax = -1;
@@ -222,7 +223,11 @@ __device__ int regrid_track(double *prim, long long N, double *x, double *dx, do
   for (int base = 0; base < n; base += BS) {
     const int k = base + threadIdx.x;
     bool hp = false;
-    if (k < n && k >= iL + 1 && k <= iR0 - 1) hp = prim[1 * N + off + k] > thr;
+    if (k < n && k >= iL + 1 && k <= iR0 - 1) {
+      double p[NQ];
+      load(off + k, p);
+      hp = Hooks::regrid_marker(par, p);
+    }
     const uint32_t b = __ballot_sync(0xffffffffu, hp);
     if ((threadIdx.x & 31) == 0 && k < n) hpw[k >> 5] = b;
     if (hp) atomicMax(&s_hpmax, k);
@@ -234,8 +239,11 @@ __device__ int regrid_track(double *prim, long long N, double *x, double *dx, do
   for (int base = 0; base < n; base += BS) {
     const int k = base + threadIdx.x;
     int a = SKIP;
-    if (k < n && k >= iL + 1 && k <= iR0 - 1)
-      a = bm_criterion<Cfg>(P, dx[off + k], prim[2 * N + off + k], k, iS0, rOut0);
+    if (k < n && k >= iL + 1 && k <= iR0 - 1) {
+      double p[NQ];
+      load(off + k, p);
+      a = Hooks::check_cell_for_regrid(par, dx[off + k], p, k, (int)iS0, rOut0);
+    }
     const uint32_t bs = __ballot_sync(0xffffffffu, a == SPLIT);
     const uint32_t bm = __ballot_sync(0xffffffffu, a == MERGE);
     if ((threadIdx.x & 31) == 0 && k < n) {
@@ -289,12 +297,12 @@ __device__ int regrid_track(double *prim, long long N, double *x, double *dx, do
       ++nseg;
       seg_next_orig = -2;
       if (first_change > out) first_change = out;
-      if (out > iL && c.prim[PPP] > thr) hp_final = max(hp_final, out);
+      if (out > iL && Hooks::regrid_marker(par, c.prim)) hp_final = max(hp_final, out);
       ++out;
     };
     auto is_hp = [&](const RCell<Cfg> &c) -> bool {
       if (c.orig >= 0) return bit_of(hpw, c.orig);
-      return c.prim[PPP] > thr;
+      return Hooks::regrid_marker(par, c.prim);
     };
 
     int ntrack = n, iR = iR0;
@@ -318,7 +326,7 @@ __device__ int regrid_track(double *prim, long long N, double *x, double *dx, do
       bool valid = false;
       if (curc.orig >= 0) {
         const int dc = i - iS, d0 = curc.orig - (int)iS0;
-        const bool mc = 0 < dc && dc < 10, m0 = 0 < d0 && d0 < 10;
+        const bool mc = 0 < dc && dc < Hooks::REGRID_WINDOW, m0 = 0 < d0 && d0 < Hooks::REGRID_WINDOW;
         if (mc == m0) {
           valid = true;
           action = bit_of(spw, curc.orig) ? SPLIT : (bit_of(mgw, curc.orig) ? MERGE : SKIP);
@@ -329,7 +337,7 @@ __device__ int regrid_track(double *prim, long long N, double *x, double *dx, do
         double rOut;
         if (iR - 1 == i) rOut = curc.x;
         else rOut = x[off + k + (iR - 1 - (i + 1))];
-        action = bm_criterion<Cfg>(P, curc.dx, curc.prim[UU1], i, (double)iS, rOut);
+        action = Hooks::check_cell_for_regrid(par, curc.dx, curc.prim, i, iS, rOut);
       } else if (action == SKIP) {
         // skip a run of original no-op cells whose distance to the shock
         // matches the original context (no action moves anything meanwhile)
@@ -341,10 +349,10 @@ __device__ int regrid_track(double *prim, long long N, double *x, double *dx, do
           // stop before either shock window
           const int w0 = (int)iS0 + 1;
           if (w0 > kc) lim = min(lim, w0);
-          else if ((int)iS0 + 9 > kc) lim = kc + 1;
+          else if ((int)iS0 + Hooks::REGRID_WINDOW - 1 > kc) lim = kc + 1;
           const int w1 = iS - delta + 1;
           if (w1 > kc) lim = min(lim, w1);
-          else if (iS - delta + 9 > kc) lim = kc + 1;
+          else if (iS - delta + Hooks::REGRID_WINDOW - 1 > kc) lim = kc + 1;
         }
         // first original > kc whose precomputed action is not a no-op
         int m = kc + 1;
@@ -390,12 +398,12 @@ __device__ int regrid_track(double *prim, long long N, double *x, double *dx, do
         const bool left = (prev.dx < nxt.dx && i != ng) || i == iR - 1;
         RCell<Cfg> M;
         if (left) {
-          merge_cells<Cfg>(ph, curc, prev, true, M, &cs);
+          merge_cells<Cfg, Hooks>(ph, curc, prev, true, M, &cs, par);
           emit(M);
           prev = nxt;
           curc = V.orig_cell(k + 1);
         } else {
-          merge_cells<Cfg>(ph, curc, nxt, false, M, &cs);
+          merge_cells<Cfg, Hooks>(ph, curc, nxt, false, M, &cs, par);
           emit(prev);
           prev = M;
           curc = V.orig_cell(k + 1);

@@ -657,9 +657,14 @@ GB_HD void iface_move(const Grid2 &G, int j, int i, int stage) {
 // reference's warm start).  A learned guess replaces it through `guess`, which
 // is called the same number of times (1 in stage 1, 2 after) by every lane of a
 // warp whether or not the lane's cell is updated (`upd`), so that it may work
-// across the warp; `r` is the radius cons2prim divides S_theta by.
+// across the warp; `r` is the radius cons2prim divides S_theta by.  It returns
+// the root search's first evaluation when it kept the warm start and made it
+// (into wbuf), else nullptr.
 struct WarmStart {
-  GB_HD void operator()(const double *, double *, bool, double) const {}
+  GB_HD const C2PStart *operator()(const Phys &, const double *, double *, bool, double, C2PStart &,
+                                   unsigned long long *) const {
+    return nullptr;
+  }
 };
 
 // `live` = false: a lane without a cell (the learned guess' warp-uniform loop).
@@ -711,10 +716,11 @@ GB_HD void update_cell(const Phys &ph, const Params2 &P, const Grid2 &G, int j, 
     xn = G1.r;
     dxn = G1.dr;
   }
-  guess(cons, prim, upd, r1);
+  C2PStart wbuf;
+  const C2PStart *w = guess(ph, cons, prim, upd, r1, wbuf, c2p);
   C2PStats cs;
   if (upd) {
-    cons2prim(ph, cons, prim, r1, &cs);
+    cons2prim(ph, cons, prim, r1, &cs, w);
     c2p[0] += 1;
     c2p[1] += cs.iters;
     c2p[2] += cs.fallback;
@@ -734,9 +740,9 @@ GB_HD void update_cell(const Phys &ph, const Params2 &P, const Grid2 &G, int j, 
       xn = G2.r;
       dxn = G2.dr;
     }
-    guess(cons, prim, upd, r2);
+    const C2PStart *w2 = guess(ph, cons, prim, upd, r2, wbuf, c2p);
     if (upd) {
-      cons2prim(ph, cons, prim, r2, &cs);
+      cons2prim(ph, cons, prim, r2, &cs, w2);
       c2p[0] += 1;
       c2p[1] += cs.iters;
       c2p[2] += cs.fallback;

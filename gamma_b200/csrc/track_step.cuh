@@ -17,6 +17,7 @@
 // without any grid-wide synchronisation.
 #pragma once
 
+#include "gamma_problem.h"
 #include "mlp.cuh"
 #include "physics.cuh"
 #include "regrid.cuh"
@@ -47,7 +48,7 @@ struct Tracks {
   const long long *off;
   const int *cap;
   RunState *run;    // per-run scalars (ntrack, t, dt, it, status)
-  const RunParams *par;
+  const double *par;  // [nruns][gamma_problem::PARAM_WORDS] problem parameters
   RegridScratch rg;
   const float *mlp;  // learned cons2prim guess parameters (kernels built with GUESS only)
 };
@@ -66,33 +67,15 @@ struct StepStats {
   unsigned long long splits, merges;
   int c2p_max_iters;
   int status;
+  unsigned long long c2p_guesses;  // cons2prim calls started from the learned guess
 };
 
-// calcBM (BM1D.cpp:62-86) with per-run parameters; r in code units (ls).
-__device__ __forceinline__ void calc_bm(const Phys &ph, const RunParams &P, double r_code, double t,
-                                        double *rho, double *u, double *p) {
-  const double G = ph.gamma_ad;
-  const double r = r_code * P.lNorm;
-  const double c5 = C_LIGHT * C_LIGHT * C_LIGHT * C_LIGHT * C_LIGHT;
-  double lfacShock2 = P.Etot * (17. - 4. * P.k) / (8. * PI_ * P.n_ext * MP * (t * t * t) * c5);
-  double RShock = C_LIGHT * t * (1. - 1. / (1. + 2. * (4. - P.k) * lfacShock2));
-  double rhoa = P.n_ext * MP * pow(RShock / P.Rscale, -P.k);
-  double pa = rhoa * P.eta * C_LIGHT * C_LIGHT;
-  double ha = C_LIGHT * C_LIGHT + pa * G / (G - 1.) / rhoa;
-  double pf = 2. / 3. * lfacShock2 * ha * rhoa;
-  double lfacf = sqrt(fmax(1., .5 * lfacShock2));
-  double Df = 2. * lfacShock2 * rhoa;
-  double chi = (1. + 2. * (4. - P.k) * lfacShock2) * (1. - r / (C_LIGHT * t));
-  *p = pf * pow(chi, -(17. - 4. * P.k) / (12. - 3. * P.k)) / P.pNorm;
-  double lfac = sqrt(lfacf * lfacf / chi + 1);
-  double D = Df * pow(chi, -(7. - 2. * P.k) / (4. - P.k));
-  *rho = D / lfac / P.rhoNorm;
-  *u = C_LIGHT * sqrt(1. - 1. / (lfac * lfac)) * lfac / P.vNorm;
-}
-
 // BS threads advance one run; each sweep chunk holds CPT cells per thread
-// (CH = BS * CPT), which a thread takes in turn.
-template <class Cfg, int BS, bool GUESS = false, int CPT = 1>
+// (CH = BS * CPT), which a thread takes in turn.  Hooks: the problem module
+// (include/gamma_problem.h), whose hooks run where the reference calls its
+// own: userBoundaries in ghosts, userKinematics and userSourceTerms in the
+// sweep, cons2prim_user in cons2prim, checkCellForRegrid in regrid_track.
+template <class Cfg, class Hooks, int BS, bool GUESS = false, int CPT = 1>
 struct TrackStep {
   static constexpr int NQ = Cfg::NQ;
   static constexpr int NQS = Cfg::NQ - 1;
@@ -138,9 +121,9 @@ struct TrackStep {
   }
 
   // Ghost cells and ghost interfaces (Grid::updateGhosts, 1d.cpp:217-246) and
-  // the problem's boundary hook.  ex/edx: geometry of the two edge cells.
-  __device__ static void ghosts(const Tracks &T, const Phys &ph, const RunParams &P, long long off, int n,
-                                const double *edge, double t) {
+  // the problem's boundary hook.  edge: geometry of the two edge cells.
+  __device__ static void ghosts(const Tracks &T, const Phys &ph, const gamma_problem::HookArgs &A, long long off,
+                                int n, const double *edge) {
     const int ng = ph.ngst, iL = ng - 1, iR = n - ng;
     const int tid = threadIdx.x;
     if (tid < 2 * ng) {
@@ -150,17 +133,9 @@ struct TrackStep {
       const long long ge = off + e, gi = off + i;
       double p[NQ];
       load_prim(T, ge, p);
-      const double ex = left ? edge[0] : edge[2];
-      const double edx = left ? edge[1] : edge[3];
-      if (Cfg::BM && left && t < P.t_bm_until) {
-        const double gx = ex - (iL - i + 1) * edx;
-        double rho, u, pp;
-        calc_bm(ph, P, gx, t, &rho, &u, &pp);
-        p[RHO] = rho;
-        p[UU1] = u;
-        p[PPP] = pp;
-        p[TR1] = 2.;
-      }
+      // the ghost's centre as updateGhosts shifts it (1d.cpp:221, 234)
+      const double gx = left ? edge[0] - (iL - i + 1) * edge[1] : edge[2] + (i - iR + 1) * edge[3];
+      Hooks::user_boundaries(A, i, gx, p);  // Grid::userBoundaries (1d.cpp:244)
       store_prim(T, gi, p);
       T.dtl[gi] = T.dtl[ge];
       if (Cfg::SHOCK) {
@@ -266,12 +241,31 @@ struct TrackStep {
     }
   }
 
+  // The starting pressure of one cons2prim with the learned guess: f at the
+  // warm start first; where it is within mlp::kGuessGate of E the warm start
+  // stays and its evaluation is handed to the search (returned pointer, into
+  // wbuf), elsewhere the network's pressure replaces it (nullptr).  Every lane
+  // of the warp calls (upd = false: no cell); the network runs only when a lane
+  // of the warp needs it.
+  __device__ static const C2PStart *guessed_start(const mlp::InferSmem &inf, const Phys &ph, const double *cons,
+                                                  double *prim, bool upd, StepStats &st, C2PStart &wbuf) {
+    bool need = false;
+    if (upd) {
+      const C2PInput in = c2p_input<Cfg>(cons, prim);
+      wbuf = c2p_start<Cfg>(ph, in.D, in.S, in.S2, in.E, in.pCand);
+      need = !(fabs(wbuf.f) <= mlp::kGuessGate * in.E);
+    }
+    if (__any_sync(0xffffffffu, need)) learned_guess(inf, cons, prim, need);
+    if (need) st.c2p_guesses++;
+    return need ? nullptr : &wbuf;
+  }
+
   // --- one stage sweep ------------------------------------------------------
   // mode 0: stage-1 CFL candidates only (returns the run's min dt_loc and
   //         resets dt_loc); mode 1: fluxes + update (+ RK combine for stage>1).
   // Inlined into the step (measured faster than one shared out-of-line copy,
   // whose call frame costs local-memory traffic).
-  __device__ GB_SWEEP_ATTR static double sweep(const Tracks &T, const Phys &ph, const RunParams &P,
+  __device__ GB_SWEEP_ATTR static double sweep(const Tracks &T, const Phys &ph, const gamma_problem::HookArgs &A,
                                               const SynchConst &sc,
                                  Smem &sm, long long off, int n, int stage, int mode, double dt, double t,
                                  StepStats &st, const mlp::InferSmem *inf) {
@@ -342,10 +336,7 @@ struct TrackStep {
           reconstruct(sm, ph, i, n, c, xI, L, R);
           const Waves w = compute_lambda<Cfg>(ph, L, R);
           double v = ph.vi * w.lS;
-          if (Cfg::BM) {  // userKinematics (BM1D.cpp:188-246)
-            if (i < ng) v = P.v_in;
-            if (i >= n - 1 - ng) v = P.v_out;
-          }
+          Hooks::user_kinematics(A, i, &v);  // Grid::userKinematics (1d.cpp:749)
           my_lL = w.lL;
           my_lR = w.lR;
           my_v = v;
@@ -429,6 +420,7 @@ struct TrackStep {
         double prim[NQ], cons[NQ];
         Geom G1;
         C2PStats cs;
+        C2PStart wbuf;
         if (upd) {
 #pragma unroll
           for (int s = 0; s < NQS; ++s) prim[Slots<Cfg>::q_of(s)] = sm.cp[s][c];
@@ -453,6 +445,10 @@ struct TrackStep {
             double rsq = (r2 * r2 + r1 * r1 + r2 * r1) / 3.;
             cons[SS1] += (2. * p) * (r / rsq) * dV * dt;
           }
+          if (Cfg::CYL) {  // Cell::sourceTerms of rel_cyl.cpp:358-364, r = G.x[r_]
+            cons[SS1] += prim[PPP] / G0.x * G0.dV * dt;
+          }
+          Hooks::user_source_terms(A, G0.x, G0.dx, G0.dV, prim, cons, dt);  // Cell::userSourceTerms
           if (Cfg::SYNCH) {
             const double dg = radiative_source<Cfg>(ph, sc, prim, G0.dV, dt);
             cons[GMX] += dg;
@@ -468,9 +464,10 @@ struct TrackStep {
             for (int q = 0; q < NQ; ++q) cons[q] = q <= TAU ? cons[q] / G1.dV : qdiv(cons[q], G1.dV);
           }
         }
-        if (GUESS) learned_guess(*inf, cons, prim, upd);
+        // every lane of the warp meets here (the network works across it)
+        const C2PStart *w = GUESS ? guessed_start(*inf, ph, cons, prim, upd, st, wbuf) : nullptr;
         if (upd) {
-          cons2prim<Cfg>(ph, cons, prim, &cs);
+          cons2prim<Cfg, Hooks>(ph, cons, prim, &cs, A.par, w);
           count_c2p(st, cs);
         }
         if (stage > 1) {
@@ -490,9 +487,9 @@ struct TrackStep {
               for (int q = 0; q < NQ; ++q) cons[q] = q <= TAU ? cons[q] / G2.dV : qdiv(cons[q], G2.dV);
             }
           }
-          if (GUESS) learned_guess(*inf, cons, prim, upd);
+          const C2PStart *w2 = GUESS ? guessed_start(*inf, ph, cons, prim, upd, st, wbuf) : nullptr;
           if (upd) {
-            cons2prim<Cfg>(ph, cons, prim, &cs);
+            cons2prim<Cfg, Hooks>(ph, cons, prim, &cs, A.par, w2);
             count_c2p(st, cs);
           }
         }
@@ -552,18 +549,20 @@ struct TrackStep {
   __device__ static void step(const Tracks &T, const Phys &ph, Smem &sm, uint32_t *words, int r, StepStats &st,
                               bool regrid_only, const mlp::InferSmem *inf) {
     const long long off = T.off[r];
-    const RunParams P = T.par[r];
-    const SynchConst sc{P.Nalpha, P.Nmp, P.Nme};
+    const double *par = T.par + (size_t)r * gamma_problem::PARAM_WORDS;
+    SynchConst sc;
+    Hooks::synchrotron_norm(par, &sc.Nalpha, &sc.Nmp, &sc.Nme);
     RunState &R = T.run[r];
     int n = R.ntrack;
     const double t = R.t;
     const int ng = ph.ngst;
 
-    if (Cfg::BM) {
-      n = regrid_track<Cfg, BS>(T.prim, T.N, T.x, T.dx, T.dtl, T.xI, off, n, T.cap[r], ph, P, T.rg, words,
-                                st.splits, st.merges);
+    if (Hooks::REGRID) {
+      n = regrid_track<Cfg, Hooks, BS>(T.prim, T.N, T.x, T.dx, T.dtl, T.xI, off, n, T.cap[r], ph, par, T.rg,
+                                       words, st.splits, st.merges);
       __syncthreads();
     }
+    const gamma_problem::HookArgs A{par, ph.gamma_ad, t, R.it, n, ng - 1, n - ng};
     if (regrid_only) {
       if (threadIdx.x == 0) R.ntrack = n;
       __syncthreads();
@@ -580,26 +579,26 @@ struct TrackStep {
 
     // stage 1: ghosts, CFL candidates, dt
     edge_geom(T, sm, off, n, ng, 1);
-    ghosts(T, ph, P, off, n, sm.edge, t);
+    ghosts(T, ph, A, off, n, sm.edge);
     __syncthreads();
-    double m = sweep(T, ph, P, sc, sm, off, n, 1, 0, 0., t, st, inf);
+    double m = sweep(T, ph, A, sc, sm, off, n, 1, 0, 0., t, st, inf);
     m = block_min(sm, m);
     const double dt = ph.cfl * m;
     // stage 1 update (the whole Grid::evolve of Timestep/euler.cpp)
-    sweep(T, ph, P, sc, sm, off, n, 1, 1, dt, t, st, inf);
+    sweep(T, ph, A, sc, sm, off, n, 1, 1, dt, t, st, inf);
     __syncthreads();
     if (!ph.euler) {
       // stage 2
       edge_geom(T, sm, off, n, ng, 2);
-      ghosts(T, ph, P, off, n, sm.edge, t);
+      ghosts(T, ph, A, off, n, sm.edge);
       __syncthreads();
-      sweep(T, ph, P, sc, sm, off, n, 2, 1, dt, t, st, inf);
+      sweep(T, ph, A, sc, sm, off, n, 2, 1, dt, t, st, inf);
       __syncthreads();
       // stage 3
       edge_geom(T, sm, off, n, ng, 3);
-      ghosts(T, ph, P, off, n, sm.edge, t);
+      ghosts(T, ph, A, off, n, sm.edge);
       __syncthreads();
-      sweep(T, ph, P, sc, sm, off, n, 3, 1, dt, t, st, inf);
+      sweep(T, ph, A, sc, sm, off, n, 3, 1, dt, t, st, inf);
       __syncthreads();
     }
 
@@ -647,11 +646,11 @@ struct TrackStep {
 
 // Dynamic shared memory: TrackStep::Smem, the regrid bit words (words_bytes),
 // then, with GUESS, the tensor-core weights of the learned guess.
-template <class Cfg, int BS, bool GUESS = false, int CPT = 1, int MINB = Cfg::MIN_BLOCKS>
+template <class Cfg, class Hooks, int BS, bool GUESS = false, int CPT = 1, int MINB = Cfg::MIN_BLOCKS>
 __global__ void __launch_bounds__(BS, MINB)
     track_step_kernel(Tracks T, Phys ph, int nsteps, const int *order, int nruns, int *queue, StepStats *stats,
                       int regrid_only, unsigned words_bytes) {
-  using TS = TrackStep<Cfg, BS, GUESS, CPT>;
+  using TS = TrackStep<Cfg, Hooks, BS, GUESS, CPT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typename TS::Smem &sm = *reinterpret_cast<typename TS::Smem *>(smem_raw);
   uint32_t *words = reinterpret_cast<uint32_t *>(smem_raw + sizeof(typename TS::Smem));
@@ -682,6 +681,7 @@ __global__ void __launch_bounds__(BS, MINB)
   }
   // fold the per-thread statistics into the launch totals
   __syncthreads();
+  if (st.c2p_guesses) atomicAdd(&stats->c2p_guesses, st.c2p_guesses);
   if (st.c2p_calls) {
     atomicAdd(&stats->c2p_calls, st.c2p_calls);
     atomicAdd(&stats->c2p_iters, st.c2p_iters);

@@ -22,7 +22,7 @@ GAMMA_ERR_NO_DEVICE = -4
 GAMMA_ERR_NEG_DT = -30
 
 GEOM_SPHERICAL1D, GEOM_CARTESIAN = 0, 1
-HYDRO_REL_SPH, HYDRO_REL_CART = 0, 1
+HYDRO_REL_SPH, HYDRO_REL_CART, HYDRO_REL_CYL = 0, 1, 2
 EOS_IDEAL, EOS_SYNGE = 0, 1
 PROBLEM_BM1D, PROBLEM_TUBE = 0, 1
 TS_RK3, TS_EULER = 0, 1  # Timestep/rk3.cpp, Timestep/euler.cpp
@@ -38,8 +38,9 @@ EXPORTS = (
     "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess",
     "gamma_text1d_write", "gamma_text1d_read", "gamma_gpu_print_cols", "gamma_gpu_save", "gamma_gpu_load",
     "gamma_gpu_variant_info", "gamma_gpu_set_variant", "gamma_gpu_get_variant", "gamma_gpu_autotune",
-    "gamma_gpu_use_graphs",
+    "gamma_gpu_use_graphs", "gamma_gpu_problem_id", "gamma_gpu_set_params_words", "gamma_gpu_initial_state",
 )
+PARAM_WORDS = 32  # gamma_problem::PARAM_WORDS
 
 
 class GammaError(RuntimeError):
@@ -70,7 +71,8 @@ class StepStats(ctypes.Structure):
 
     _fields_ = [(n, ctypes.c_ulonglong) for n in ("c2p_calls", "c2p_iters", "c2p_fallbacks", "zone_updates",
                                                   "splits", "merges")] + \
-               [("c2p_max_iters", ctypes.c_int), ("status", ctypes.c_int), ("device_ms", ctypes.c_float)]
+               [("c2p_max_iters", ctypes.c_int), ("status", ctypes.c_int), ("device_ms", ctypes.c_float),
+                ("c2p_guesses", ctypes.c_ulonglong)]
 
     def as_dict(self) -> dict:
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
@@ -92,10 +94,41 @@ def config_sph(gamma_ad=4. / 3., cfl=0.2, vi=1.0, eos=EOS_IDEAL, eos_wavespeeds=
                   int(eos_wavespeeds), int(timestep))
 
 
-def config_cart(gamma_ad=5. / 3., cfl=0.2, vi=1.0, timestep=TS_RK3) -> Config:
-    """cartesian + rel_cart, no shock detection or synchrotron (NUM_Q = 6)."""
-    return Config(GEOM_CARTESIAN, HYDRO_REL_CART, EOS_IDEAL, 6, 0, 0, PROBLEM_TUBE, 2, gamma_ad, cfl, vi, 0,
+def config_cart(gamma_ad=5. / 3., cfl=0.2, vi=1.0, timestep=TS_RK3, problem=PROBLEM_TUBE) -> Config:
+    """cartesian + rel_cart, no shock detection or synchrotron (NUM_Q = 6).
+    problem: a problem module's id (problem_id) running with these modules."""
+    return Config(GEOM_CARTESIAN, HYDRO_REL_CART, EOS_IDEAL, 6, 0, 0, int(problem), 2, gamma_ad, cfl, vi, 0,
                   int(timestep))
+
+
+def config_cyl(gamma_ad=5. / 3., cfl=0.2, vi=1.0, timestep=TS_RK3, problem=None) -> Config:
+    """cartesian + rel_cyl (Hydro/rel_cyl.cpp), no shock detection or synchrotron
+    (NUM_Q = 6); problem: a module built for it (default: tube_cyl)."""
+    pid = problem_id("tube_cyl") if problem is None else int(problem)
+    return Config(GEOM_CARTESIAN, HYDRO_REL_CYL, EOS_IDEAL, 6, 0, 0, pid, 2, gamma_ad, cfl, vi, 0, int(timestep))
+
+
+def problem_id(name: str) -> int:
+    """gamma_gpu_problem_id: the id of a problem module compiled into the library."""
+    pid = lib().gamma_gpu_problem_id(name.encode())
+    if pid < 0:
+        raise KeyError(f"no problem module {name!r} in {LIB_PATH}")
+    return pid
+
+
+def initial_state(cfg: Config, words, cap: int):
+    """gamma_gpu_initial_state: Simu::initialise of one run from the problem
+    module's set-up hooks, on the host.  Returns (ntrack, t, prim [nq][cap], x,
+    dx, xI, dt_loc)."""
+    w = np.ascontiguousarray(words, dtype=np.float64)
+    prim = np.zeros((cfg.nq, cap))
+    x, dx, xI, dtl = np.zeros(cap), np.zeros(cap), np.zeros(cap), np.zeros(cap)
+    nt, t = ctypes.c_int(), ctypes.c_double()
+    rc = lib().gamma_gpu_initial_state(ctypes.byref(cfg), _p(w), int(w.size), int(cap), ctypes.byref(nt),
+                                       ctypes.byref(t), _p(prim), _p(x), _p(dx), _p(xI), _p(dtl))
+    if rc != GAMMA_OK:
+        raise GammaError(rc)
+    return int(nt.value), float(t.value), prim, x, dx, xI, dtl
 
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -152,6 +185,10 @@ def lib() -> ctypes.CDLL:
         L.gamma_gpu_autotune.argtypes = [v, ctypes.c_int, ctypes.POINTER(ctypes.c_float), _ip]
         L.gamma_gpu_use_graphs.argtypes = [v, ctypes.c_int]
         L.gamma_gpu_save.argtypes = [v, ctypes.c_char_p]
+        L.gamma_gpu_problem_id.argtypes = [ctypes.c_char_p]
+        L.gamma_gpu_set_params_words.argtypes = [v, _dp, ctypes.c_int]
+        L.gamma_gpu_initial_state.argtypes = [ctypes.POINTER(Config), _dp, ctypes.c_int, ctypes.c_int, _ip, _dp,
+                                              _dp, _dp, _dp, _dp, _dp]
         L.gamma_gpu_load.argtypes = [v, ctypes.c_char_p]
         for name in ("gamma_gpu_create", "gamma_gpu_layout", "gamma_gpu_set_params", "gamma_gpu_upload",
                      "gamma_gpu_step", "gamma_gpu_regrid", "gamma_gpu_download", "gamma_gpu_cons2prim",
@@ -159,7 +196,8 @@ def lib() -> ctypes.CDLL:
                      "gamma_mlp_forward", "gamma_gpu_cons2prim_guess", "gamma_gpu_set_guess", "gamma_mlp_loss_grad",
                      "gamma_text1d_write", "gamma_text1d_read", "gamma_gpu_print_cols", "gamma_gpu_save",
                      "gamma_gpu_load", "gamma_gpu_variant_info", "gamma_gpu_set_variant", "gamma_gpu_get_variant",
-                     "gamma_gpu_autotune", "gamma_gpu_use_graphs"):
+                     "gamma_gpu_autotune", "gamma_gpu_use_graphs", "gamma_gpu_problem_id",
+                     "gamma_gpu_set_params_words", "gamma_gpu_initial_state"):
             getattr(L, name).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -215,6 +253,12 @@ class GammaGPU:
     def set_params(self, params):
         arr = (RunParams * self.nruns)(*params)
         self._check(lib().gamma_gpu_set_params(self.h, arr))
+
+    def set_params_words(self, words):
+        """The problem module's parameter words of every run ([nruns][nwords], nwords <= PARAM_WORDS)."""
+        w = np.ascontiguousarray(np.atleast_2d(words), dtype=np.float64)
+        assert w.shape[0] == self.nruns
+        self._check(lib().gamma_gpu_set_params_words(self.h, _p(w), int(w.shape[1])))
 
     def upload(self, ntrack, prim, x, dx, xI, dt_loc=None, t=None, it=None):
         nt = np.ascontiguousarray(ntrack, dtype=np.int32)

@@ -84,8 +84,12 @@ def lib() -> ctypes.CDLL:
         L.gamma_text2d_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config2D), v, v, v, v, v, v, v, v, v]
         L.gamma_2d_upload.argtypes = [v] + [v] * 9 + [ctypes.c_double, ctypes.c_longlong, ctypes.c_int]
         L.gamma_2d_step.argtypes = [v, ctypes.c_int, ctypes.POINTER(gpu.StepStats)]
+        L.gamma_2d_use_graphs.argtypes = [v, ctypes.c_int]
+        L.gamma_2d_use_graphs.restype = ctypes.c_int
         L.gamma_2d_download.argtypes = [v] * 17
         L.gamma_2d_prepare.argtypes = [v]
+        L.gamma_2d_prepare_stage.argtypes = [v, ctypes.c_int]
+        L.gamma_2d_prepare_stage.restype = ctypes.c_int
         L.gamma_2d_download_fluxes.argtypes = [v] * 8
         L.gamma_2d_stream.argtypes = [v]
         L.gamma_2d_stream.restype = v
@@ -147,6 +151,11 @@ class Grid2DGPU:
     def set_params(self, p: Params2D):
         self._check(lib().gamma_2d_set_params(self.h, ctypes.byref(p)))
 
+    def use_graphs(self, on: bool):
+        """Each step replayed from a captured CUDA graph (default), or its
+        kernels launched one by one."""
+        self._check(lib().gamma_2d_use_graphs(self.h, int(bool(on))))
+
     def set_guess(self, params_ptr: int):
         """Learned cons2prim starting pressure in every cell update (device
         parameter pointer), or 0 for the warm start of the reference."""
@@ -170,6 +179,10 @@ class Grid2DGPU:
     def prepare(self):
         """regrid, ghosts and the stage-1 fluxes only (diagnostics)"""
         self._check(lib().gamma_2d_prepare(self.h))
+
+    def prepare_stage(self, stage: int):
+        """gamma_2d_prepare_stage: the loop body up to stage `stage`'s fluxes."""
+        self._check(lib().gamma_2d_prepare_stage(self.h, int(stage)))
 
     def download_fluxes(self) -> dict:
         NC = self.NC
@@ -253,4 +266,4 @@ EXPORTS = ("gamma_2d_create", "gamma_2d_layout", "gamma_2d_set_params", "gamma_2
            "gamma_2d_step",
            "gamma_2d_download", "gamma_2d_prepare", "gamma_2d_download_fluxes", "gamma_2d_stream",
            "gamma_2d_last_error", "gamma_2d_destroy", "gamma_2d_print_cols", "gamma_2d_save", "gamma_2d_load",
-           "gamma_text2d_write", "gamma_text2d_read")
+           "gamma_text2d_write", "gamma_text2d_read", "gamma_2d_use_graphs", "gamma_2d_prepare_stage")

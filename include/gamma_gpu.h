@@ -42,8 +42,9 @@ extern "C" {
 #define GAMMA_ERR_NEG_DT (-30)     /* a CFL candidate was negative: the reference exit(30)s (cell.cpp:70-73) */
 
 enum { GAMMA_GEOM_SPHERICAL1D = 0, GAMMA_GEOM_CARTESIAN = 1 };
-enum { GAMMA_HYDRO_REL_SPH = 0, GAMMA_HYDRO_REL_CART = 1 };
+enum { GAMMA_HYDRO_REL_SPH = 0, GAMMA_HYDRO_REL_CART = 1, GAMMA_HYDRO_REL_CYL = 2 };
 enum { GAMMA_EOS_IDEAL = 0, GAMMA_EOS_SYNGE = 1 };
+/* built-in problem modules; others by name through gamma_gpu_problem_id */
 enum { GAMMA_PROBLEM_BM1D = 0, GAMMA_PROBLEM_TUBE = 1 };
 /* the Timestep module: Grid::evolve of src/Timestep/rk3.cpp (SSP-RK3, three
  * stages) or of src/Timestep/euler.cpp (one forward-Euler Grid::update) */
@@ -51,9 +52,10 @@ enum { GAMMA_TS_RK3 = 0, GAMMA_TS_EULER = 1 };
 
 /* Module selection and switches (Makefile GEOMETRY/HYDRO/RADIATION/INITIAL,
  * environment.h GAMMA_, EOS_, CFL_, VI, SHOCK_DETECTION_, LOCAL_SYNCHROTRON_).
- * Supported combinations:
- *   spherical1D + rel_sph + shock detection + local synchrotron (nq = 10), BM1D hooks
- *   cartesian   + rel_cart, no shock detection, no synchrotron   (nq = 6),  no hooks */
+ * Supported combinations, each with any problem module built for it:
+ *   spherical1D + rel_sph + shock detection + local synchrotron (nq = 10)
+ *   cartesian   + rel_cart, no shock detection, no synchrotron   (nq = 6)
+ *   cartesian   + rel_cyl (Hydro/rel_cyl.cpp), the same switches  (nq = 6) */
 typedef struct {
   int geometry;
   int hydro;
@@ -95,6 +97,7 @@ typedef struct {
   int c2p_max_iters;
   int status;                        /* 0 or the first failing run's GAMMA_ERR_* */
   float device_ms;                   /* device time of the step launch(es) */
+  unsigned long long c2p_guesses;    /* calls started from the learned guess (gamma_gpu_set_guess) */
 } gamma_step_stats_t;
 
 typedef struct gamma_ctx gamma_ctx_t;
@@ -107,8 +110,35 @@ int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *capacity, 
 /* offsets[r] of each run in the pooled arrays and the total length. */
 int gamma_gpu_layout(const gamma_ctx_t *ctx, long long *offsets, long long *total);
 
-/* Problem parameters, one record per run. */
+/* Problem parameters, one record per run: the BM1D module's record
+ * (gamma_run_params_t), the words of its first fields. */
 int gamma_gpu_set_params(gamma_ctx_t *ctx, const gamma_run_params_t *params);
+
+/* ---- Problem modules (the reference's INITIAL files) ------------------------
+ * A problem module is a set of user hooks (include/gamma_problem.h) compiled
+ * into this library: the built-in "bm1d" (GAMMA_PROBLEM_BM1D), "tube"
+ * (GAMMA_PROBLEM_TUBE) and "isen1d", and any named by
+ * `make -C gamma_b200/csrc INITIAL=...` (the reference links one with
+ * INITIAL = Tests/<name>, Makefile:1).  gamma_config_t.problem holds the id. */
+
+/* The id of the module registered under name, or -1. */
+int gamma_gpu_problem_id(const char *name);
+
+/* The module's parameter words of every run: words[r * nwords + k], nwords <=
+ * 32 (gamma_problem::PARAM_WORDS; the rest are zero).  Replaces the file-static
+ * constants of an Initial file (e.g. src/Initial/Tests/isen1D.cpp:13-24). */
+int gamma_gpu_set_params_words(gamma_ctx_t *ctx, const double *words, int nwords);
+
+/* Simu::initialise of one run on the HOST (src/simu.cpp:24-38): the module's
+ * loadParams, Grid::initialGeometry and Grid::initialValues, then
+ * Grid::prepForRun (1d.cpp:844-856, 931-951), radiation_initGammas and the
+ * first updateGhosts with the module's userBoundaries.  Outputs are host
+ * arrays of cap cells (prim [nq][cap]); ntrack and t take the run's cell count
+ * (ghosts included) and start time.  Needs no GPU.  GAMMA_ERR_INVALID for a
+ * module whose set-up runs elsewhere (bm1d and tube are set up by
+ * gamma_b200/problems.py), GAMMA_ERR_CAPACITY if nmax + 2 ngst > cap. */
+int gamma_gpu_initial_state(const gamma_config_t *cfg, const double *params, int nwords, int cap, int *ntrack,
+                            double *t, double *prim, double *x, double *dx, double *xI, double *dt_loc);
 
 /* Host -> device state of every run (mpi_distribute + prepForRun leave this
  * state in the reference, 1d.cpp:956-969, grid.cpp:20-26).  t[r], it[r]:
@@ -292,6 +322,11 @@ int gamma_2d_upload(gamma_2d_t *ctx, const int *ntrack, const double *prim, cons
  * graph launch each.  With stats == NULL the call only enqueues the work. */
 int gamma_2d_step(gamma_2d_t *ctx, int nsteps, gamma_step_stats_t *stats);
 
+/* No counterpart in the reference.  on = 1 (default): each step is one
+ * replay of a captured CUDA graph; 0: the step's kernels are launched one by
+ * one from the host (the plain form the benchmark compares against). */
+int gamma_2d_use_graphs(gamma_2d_t *ctx, int on);
+
 /* Device -> host state; any pointer may be NULL. */
 int gamma_2d_download(gamma_2d_t *ctx, int *ntrack, double *t, double *dt, long long *it, int *status,
                       double *prim, double *x, double *dx, double *dt_loc, double *xI, double *grad_mv,
@@ -305,6 +340,10 @@ int gamma_2d_download(gamma_2d_t *ctx, int *ntrack, double *t, double *dt, long 
  * grad_f1 (per cell, [NUM_Q][NJ*cap]).  Continuing with gamma_2d_step after it
  * is not a reference step. */
 int gamma_2d_prepare(gamma_2d_t *ctx);
+/* The same up to stage `stage` of Grid::evolve (rk3.cpp:99-194): the stages
+ * before it complete (updates and combines), then that stage's updateGhosts
+ * and prepForUpdate.  stage 1 is gamma_2d_prepare. */
+int gamma_2d_prepare_stage(gamma_2d_t *ctx, int stage);
 int gamma_2d_download_fluxes(gamma_2d_t *ctx, double *v, double *lL, double *lR, double *flux, double *f1lo,
                              double *f1hi, double *grad_f1_stage);
 

@@ -104,7 +104,10 @@ static double g_epsrel_override = 0.0;
 void oracle_brent_override_epsrel(double epsrel) { g_epsrel_override = epsrel; }
 
 int oracle_brent_continue(double lo, double hi, double epsabs, double epsrel) {
-  if (g_epsrel_override > 0.0) epsrel = g_epsrel_override;
+  if (g_epsrel_override > 0.0) {  // converge: the relative tolerance only
+    epsrel = g_epsrel_override;
+    epsabs = 0.0;
+  }
   double min_abs;
   if ((lo > 0.0 && hi > 0.0) || (lo < 0.0 && hi < 0.0))
     min_abs = fmin(fabs(lo), fabs(hi));

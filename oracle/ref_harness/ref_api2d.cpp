@@ -185,6 +185,36 @@ REF_API int ref_partial(int what) {
     s.grid.copyState0();
     s.grid.update(s.dt);
   }
+  // the later stages of rk3.cpp:107-192 up to their fluxes: what = 4 stops
+  // after stage 2's prepForUpdate, 5 after stage 3's (the stage bodies are the
+  // reference's, in its order; the combines restate its loops)
+  for (int st = 2; st <= 3 && what >= st + 2; ++st) {
+    Grid &g = s.grid;
+    if (st == 3) {
+      g.update(s.dt);
+      for (int j = g.jLbnd + 1; j <= g.jRbnd - 1; ++j)
+        for (int i = g.iLbnd[j] + 1; i <= g.iRbnd[j] - 1; ++i) {
+          Cell *c = &g.Ctot[j][i];
+          double dV = c->G.dV, dV0 = c->G0.dV;
+          for (int q = 0; q < NUM_Q; ++q) c->S.cons[q] = 3. / 4. * c->S0.cons[q] * dV0 + 1. / 4. * c->S.cons[q] * dV;
+        }
+      for (int j = g.jLbnd + 1; j <= g.jRbnd - 1; ++j)
+        for (int i = g.iLbnd[j]; i <= g.iRbnd[j] - 1; ++i) {
+          Interface *I = &g.Itot[j][i];
+          I->x[MV] = 3. / 4. * I->x0[MV] + 1. / 4. * I->x[MV];
+          I->computedA();
+        }
+      g.CellGeomFromInterfacePos();
+      for (int j = g.jLbnd + 1; j <= g.jRbnd - 1; ++j)
+        for (int i = g.iLbnd[j] + 1; i <= g.iRbnd[j] - 1; ++i) {
+          Cell *c = &g.Ctot[j][i];
+          for (int q = 0; q < NUM_Q; ++q) c->S.cons[q] /= c->G.dV;
+          c->S.cons2prim(c->G.x[r_]);
+        }
+    }
+    g.updateGhosts(s.it, s.t);
+    g.prepForUpdate(s.it, s.t);
+  }
   return 0;
 }
 
