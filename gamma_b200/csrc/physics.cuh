@@ -59,12 +59,13 @@ constexpr double DT_INF = 1.e15;
 //      move at the ulp level, which the reference's own cold-gas conditioning
 //      amplifies beyond the parity bars (lambda* from a near-cancelling
 //      quadratic; f(p) of cons2prim cancelling to eps*E).
-//   2 (default): the shared reciprocals of 1 everywhere except in those two
-//      places, which keep the reference's order: the wave speeds and the
-//      contact speed lambda* (FAST_RIEMANN), and f(p) of the cons2prim root
-//      search with the primitive recovery after it (FAST_ROOT).  It meets every
-//      parity bar that 0 meets, with the same cell counts and regrid
-//      decisions, and runs the tube step 25% faster.
+//   2 (default): the shared reciprocals of 1 everywhere except where the
+//      reference's results hinge on exact values, which keep its order: the
+//      wave speeds and the contact speed lambda*, the PLM pair gradients whose
+//      minmod returns 0 on a tie (FAST_RIEMANN), and f(p) of the cons2prim
+//      root search with the primitive recovery after it (FAST_ROOT).  It meets
+//      every parity bar that 0 meets, with the same cell counts and regrid
+//      decisions, and runs the tube step ~20% faster.
 #ifndef GB_FAST_ARITH
 #define GB_FAST_ARITH 2
 #endif

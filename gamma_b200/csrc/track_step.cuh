@@ -298,7 +298,10 @@ struct TrackStep {
         for (int k = tid; k < NC - 1; k += BS) {
           if ((a > 0 || k > 0) && a + k < n) {  // slots k and k+1 both hold cells
             const double d = sm.cen[k + 1] - sm.cen[k];
-            if (Cfg::FAST) {
+            // in the reference's order unless every formula may move (FAST_RIEMANN):
+            // minmod of two equal slopes is 0 (1d.cpp:250-260), and a split's two
+            // halves make such ties on purpose (their pair gradient is the split's)
+            if (Cfg::FAST_RIEMANN) {
               const double rd = 1. / d;
 #pragma unroll
               for (int s = 0; s < NQS; ++s) sm.gp[s][k] = (sm.cp[s][k + 1] - sm.cp[s][k]) * rd;

@@ -160,9 +160,11 @@ def test_c2_wedge_200_steps(gpu_available, refs):
 def test_2d_wedge_1000_steps(gpu_available, refs):
     """One continuous 1,000-step run from the reference's state after two
     steps, compared every 100 steps while the cell counts stay identical:
-    L1 <= 1e-8, or 3x the reference's own movement under its root finder's
-    tolerance change at that step (the shock detector and the tracers it
-    re-injects cross thresholds)."""
+    L1 <= 1e-8, or 10x the reference's own movement under its root finder's
+    tolerance change at that step (the 1D tests' per-cell allowance: that
+    change is a lower bound on how far any second implementation's rounding
+    moves this thin wedge, where r dtheta ~ dr couples the cold lateral gas to
+    the shock within a step)."""
     from gamma_b200 import gpu2d
     _, _, (r, d), (alt, _) = refs
     th, dth = theta_of(r[2])
@@ -177,8 +179,8 @@ def test_2d_wedge_1000_steps(gpu_available, refs):
             break
         l1 = l1_by_quantity(got, r[k], qs=HYDRO + TRACERS)
         self_l1 = _l1_ref(alt[k], r[k], HYDRO + TRACERS)
-        worst = max(l1[q] / max(1e-8, 3 * self_l1[q]) for q in HYDRO + TRACERS)
-        record(f"step {k}: max over slots of L1 / max(1e-8, 3 x reference self-sensitivity)", worst, 1.)
+        worst = max(l1[q] / max(1e-8, 10 * self_l1[q]) for q in HYDRO + TRACERS)
+        record(f"step {k}: max over slots of L1 / max(1e-8, 10 x reference self-sensitivity)", worst, 1.)
         assert worst <= 1., (k, l1, self_l1)
         same_until = k - 2
     g.close()

@@ -136,6 +136,7 @@ def _ref_every_step(P, n):
     s = RefSim("hooked_tube")
     s.set_params(**P)
     s.init()
+    s.set_c2p_epsrel(1e-16)  # converged: cold-gas lambda* amplifies Brent's 1e-13 bracket
     out = [s.snapshot()]
     for _ in range(n):
         s.step(1)
@@ -167,7 +168,8 @@ def test_hooked_module_matches_reference_hooks(gpu_available):
     for k in range(n):
         a, b = got[k], ref[k + 1]
         assert a.ntrack == b.ntrack, k
-        assert np.array_equal(a.x, b.x) or l1_rel(a.x, b.x) <= 1e-14, k  # the same cells split and merge
+        # the same cells split and merge, and the interfaces move alike
+        assert np.max(np.abs(a.x - b.x) / np.abs(b.x)) <= 1e-12, k
         s = slice(2, a.ntrack - 2)
         worst = max(worst, max(l1_rel(a.prim[q, s], b.prim[q, s]) for q in (0, 1, 2, 4)))
         assert np.min(a.prim[1, s]) >= HOOKED["p_floor"]  # cons2prim_user's floor

@@ -56,5 +56,7 @@ def test_rel_cyl_tubes_match_reference(gpu_available):
             bar = 1e-12 if k == 1 else 1e-8
             record(f"tube{s.ncell} step {k} L1 max over slots", l1, bar)
             assert l1 <= bar, (s.ncell, k, l1)
-            assert abs(got.t - ref[k].t) <= 1e-12 * ref[k].t
+            # the time steps are CFL minima over the cold right state's wave speeds
+            record(f"tube{s.ncell} step {k} relative time difference", abs(got.t - ref[k].t) / ref[k].t, 1e-10)
+            assert abs(got.t - ref[k].t) <= 1e-10 * ref[k].t
         g.close()
