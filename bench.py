@@ -212,6 +212,9 @@ def run_reference_arm(args):
 
 
 JET2D = dict(ntheta=512, ncell=12000, nmax=12000)  # tracks settle at ~3,000-4,000 cells after the first regrid
+# the sweep workload's large 2D case: slow cells merge only below 0.3 of the
+# target spacing, so the tracks keep ~8,000 cells (~33 M zones)
+JET2D_C4 = dict(ntheta=4096, ncell=8000, nmax=8400, merge_DR_slow=0.3)
 
 
 def _jet2d_cpu_worker(args):
@@ -231,10 +234,11 @@ def _jet2d_cpu_worker(args):
     return steps * 0.5 * (n0 + n1), dt
 
 
-def _jet2d_run(s, steps, warmup, guess_ptr=0, dev_index=None, after=None):
+def _jet2d_run(s, steps, warmup, guess_ptr=0, dev_index=None, after=None, graphs=True):
     """Fresh 2D grid from the initial state: warm-up steps, one step with
-    statistics, then `steps` timed graph launches (statistics over them);
-    after(grid) runs before the grid is released."""
+    statistics, then `steps` timed steps (statistics over them), each one graph
+    launch (graphs) or its kernels launched one by one; after(grid) runs
+    before the grid is released."""
     import torch
 
     from gamma_b200 import gpu2d
@@ -242,6 +246,7 @@ def _jet2d_run(s, steps, warmup, guess_ptr=0, dev_index=None, after=None):
     g = gpu2d.Grid2DGPU(s.ntheta, s.nmax, th, dth)
     g.set_params(s.params())
     g.set_guess(guess_ptr)
+    g.use_graphs(graphs)
     g.upload(s.initial_state(), run_ghosts=True)
     for _ in range(max(warmup, 3)):
         g.step(1, stats=False)
@@ -351,6 +356,13 @@ def jet2d_arm(args, dev_index, host_work=True):
     res["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                        "peak_source": peak_kind, "bytes_per_zone_update": B_ZU_NQ10,
                        "note": "whole step (43 launches); per-kernel shares in the ncu launch list"}
+    # the plain form: the same step with its kernels launched one by one (no
+    # graph) and the reference's warm start, from the same initial state
+    ms_p, st_p, out_p, _ = _jet2d_run(s, args.steps, args.warmup, 0, graphs=False)
+    res["plain"] = {"value": st_p["zone_updates"] / (ms_p / 1e3), "ms_per_step": ms_p / args.steps,
+                    "same_cell_counts": bool(np.array_equal(out_p.ntrack, out.ntrack)),
+                    "note": "43 kernel launches per step from the host, no CUDA graph, warm start"}
+    res["batched_over_plain"] = res["value"] / res["plain"]["value"]
     if not args.no_learned:
         # training states: the run's active cells, as 1D states of the same |u| (cons2prim sees |S| only)
         live = _active_cells(out)
@@ -372,12 +384,15 @@ def jet2d_arm(args, dev_index, host_work=True):
             "mean_newton_iters": st_l["c2p_iters"] / max(st_l["c2p_calls"], 1),
             "max_newton_iters": st_l["c2p_max_iters"], "fallbacks": st_l["c2p_fallbacks"],
             "fallback_rate": st_l["c2p_fallbacks"] / max(st_l["c2p_calls"], 1),
+            "guess_rate": st_l["c2p_guesses"] / max(st_l["c2p_calls"], 1),
             "plain_mean_newton_iters": res["c2p"]["mean_newton_iters"],
             "plain_max_newton_iters": res["c2p"]["max_newton_iters"],
             "same_cell_counts": same, "l1_vs_plain": l1, "steps_compared": max(args.warmup, 3) + 1 + args.steps,
             "training": train,
-            "note": "the network's pressure starts every cons2prim of the cell updates (regrid merges keep the "
-                    "warm start); Newton still converges to the reference tolerance"}
+            "note": "cons2prim evaluates f at the previous pressure first and starts from the network's pressure "
+                    "only where |f| > 1e-4 E there (guess_rate); regrid merges keep the warm start; Newton still "
+                    "converges to the reference tolerance"}
+        res["learned_over_plain"] = res["learned_guess"]["value"] / res["plain"]["value"]
         del P
     lib = os.path.join(ROOT, "oracle", "_ref", "libref_jet2d.so")
     if host_work and os.path.exists(lib):
@@ -411,6 +426,65 @@ def jet2d_arm(args, dev_index, host_work=True):
     return res
 
 
+def jet2d_c4_arm(args, dev_index):
+    """The sweep workload's large 2D case: 4,096 theta tracks of ~8,000 cells
+    over [0, 0.2] rad (~33 M zones), the jet set-up of the 2D workload, batched
+    (one graph per step), device-resident."""
+    import torch
+
+    from gamma_b200 import problems
+    s = problems.Jet2dSetup(**dict(JET2D_C4, ntheta=args.c4_ntheta))
+    free0 = torch.cuda.mem_get_info()[0]
+    mem = []
+    ms, st, out, clk = _jet2d_run(s, args.steps, args.warmup, 0, dev_index,
+                                  after=lambda g: mem.append(torch.cuda.mem_get_info()[0]))
+    zones = st["zone_updates"]
+    n = out.ntrack[2:-2]
+    peak, peak_kind = measured_peak_hbm()
+    achieved = B_ZU_NQ10 * zones / (ms / 1e3) / 1e9
+    return {"workload": f"{s.ntheta} theta tracks over [{s.th_min}, {s.th_max}] rad, BM cap below {s.th_jet} rad, "
+                        f"{s.ncell} initial cells per track, slow cells merged below {s.merge_DR_slow} of the target "
+                        "spacing, NUM_Q=10, regrid + shock detection + synchrotron on",
+            "value": zones / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / args.steps,
+            "zones_per_step": zones / args.steps, "cells_per_track": [int(n.min()), int(n.max())],
+            "device_state_gb": (free0 - mem[0]) / 1e9 if mem else None,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "bytes_per_zone_update": B_ZU_NQ10},
+            "clocks": clk, "gpu_launches": 43 * args.steps}
+
+
+def summary_of(line):
+    """Short top-level figures of every workload, placed last in the JSON line."""
+    def get(d, *path):
+        for k in path:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+
+    def r(v):
+        return None if v is None else float(f"{v:.4g}")
+    out = {"tubes_value": get(line, "value"), "tubes_e2e": get(line, "e2e", "value"),
+           "tubes_frac": get(line, "roofline", "frac"), "tubes_learned_value": get(line, "learned_guess", "value")}
+    for w in ("jet2d", "sweep"):
+        out[f"{w}_value"] = get(line, w, "value")
+        out[f"{w}_plain_value"] = get(line, w, "plain", "value")
+        out[f"{w}_learned_value"] = get(line, w, "learned_guess", "value")
+        out[f"{w}_batched_over_plain"] = get(line, w, "batched_over_plain")
+        out[f"{w}_learned_over_plain"] = get(line, w, "learned_over_plain")
+        out[f"{w}_learned_guess_rate"] = get(line, w, "learned_guess", "guess_rate")
+        out[f"{w}_frac"] = get(line, w, "roofline", "frac")
+    out["c4_2d_value"] = get(line, "sweep2d", "value")
+    out["c4_2d_zones_per_step"] = get(line, "sweep2d", "zones_per_step")
+    out["c4_2d_frac"] = get(line, "sweep2d", "roofline", "frac")
+    out["c2p_plain_value"] = get(line, "c2p", "plain", "value")
+    out["c2p_learned_value"] = get(line, "c2p", "learned", "value")
+    out["c2p_learned_over_plain"] = get(line, "c2p", "speedup_learned")
+    tl = out["tubes_learned_value"]
+    out["tubes_learned_over_batched"] = tl / out["tubes_value"] if tl and out["tubes_value"] else None
+    return {k: r(v) for k, v in out.items() if v is not None}
+
+
 def autotune(g, args):
     """The step kernel's launch shape picked on the live state (gamma_gpu_autotune:
     3 one-step launches per shape, state restored), outside the timed region."""
@@ -428,21 +502,25 @@ def autotune(g, args):
                                zip(ms, (gpu.variant_info(k) for k in range(gpu.N_VARIANTS)))}}
 
 
+TRAIN_PAIRS = 10_000_000  # the learned guess's training set (half from solution states where there are enough)
+
+
 def train_guess(cfg, prim, rows_live, seed):
     """Train the learned cons2prim starting pressure on device.
 
-    Training pairs: up to 1M primitive states picked from the columns
-    `rows_live` of `prim` [nq][N] (host array) plus 1M drawn states.  Returns
-    the device parameter tensor and a summary."""
+    Training pairs: 10 M, half of them (or all the run has, if fewer) primitive
+    states picked from the columns `rows_live` of `prim` [nq][N] (host array),
+    the rest drawn.  Returns the device parameter tensor and a summary."""
     import torch
 
     from gamma_b200 import gpu
     dev = torch.device("cuda", torch.cuda.current_device())
     t0 = time.perf_counter()
     rng = np.random.default_rng(seed)
-    pick = np.sort(rng.choice(rows_live, size=min(1_000_000, rows_live.size), replace=False))
+    pick = np.sort(rng.choice(rows_live, size=min(TRAIN_PAIRS // 2, rows_live.size), replace=False))
     states = torch.tensor(np.ascontiguousarray(prim[:, pick]), device=dev)
-    ns, nu = states.shape[1], 1_000_000
+    ns = states.shape[1]
+    nu = TRAIN_PAIRS - ns
     x = torch.zeros((ns + nu, 3), dtype=torch.float32, device=dev)
     y = torch.zeros((ns + nu, 2), dtype=torch.float32, device=dev)
     gpu.mlp_pairs(cfg, states.data_ptr(), ns, nu, seed, x.data_ptr(), y.data_ptr())
@@ -504,11 +582,13 @@ def learned_arm(args, g, cfg, upload, stream, plain_out, rows, max_over_ranks, b
     return {
         "value": ws * zones / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / args.steps,
         "mean_newton_iters": st["c2p_iters"] / max(st["c2p_calls"], 1), "max_newton_iters": st["c2p_max_iters"],
-        "fallbacks": st["c2p_fallbacks"],
+        "fallbacks": st["c2p_fallbacks"], "fallback_rate": st["c2p_fallbacks"] / max(st["c2p_calls"], 1),
+        "guess_rate": st["c2p_guesses"] / max(st["c2p_calls"], 1),
         "plain_mean_newton_iters": plain_stats["c2p_iters"] / max(plain_stats["c2p_calls"], 1),
         "l1_vs_plain": l1, "same_cell_counts": same, "steps_compared": args.steps, "training": train,
-        "note": "network start replaces the previous-step pressure in every cons2prim of the step; "
-                "Newton still converges to the reference tolerance",
+        "note": "cons2prim evaluates f at the previous pressure first and starts from the network's pressure only "
+                "where |f| > 1e-4 E there (guess_rate of the calls); Newton still converges to the reference "
+                "tolerance",
     }
 
 
@@ -681,6 +761,53 @@ def sweep_cpu_baseline(kws, cores, warmup, steps=3):
                       f"warm-up steps, {cores} processes; value = sample zone-updates / slowest process"}
 
 
+def sweep_plain(args, kws, states):
+    """The plain drop-in form of the sweep: every run in a context of its own
+    (one Simu each, as separate GAMMA jobs would be), default launch shape, no
+    CUDA graph, no tuner, warm start.  A step is one gamma_gpu_step per
+    context, each on its context's own stream.  The same steps from the same
+    initial states as the batched arm: warm-up, one more, then K timed, which
+    take the same zone-updates (checked through the final cell counts)."""
+    import torch
+
+    from gamma_b200 import gpu, problems
+    cfg = gpu.config_sph()
+    ctxs = []
+    for kw, st in zip(kws, states):
+        s = problems.Bm1dSetup(**kw)
+        g = gpu.GammaGPU(cfg, [s.capacity])
+        g.set_params([s.run_params()])
+        g.use_graphs(False)
+        pk = problems.pack([st], g.offsets, g.total, 10)
+        g.upload(pk["ntrack"], pk["prim"], pk["x"], pk["dx"], pk["xI"], pk["dt_loc"], pk["t"], pk["it"])
+        ctxs.append(g)
+    for _ in range(max(args.warmup, 3) + 1):
+        for g in ctxs:
+            g.step(1, stats=False)
+    torch.cuda.synchronize()
+    side = torch.cuda.Stream()
+    streams = [torch.cuda.ExternalStream(g.stream) for g in ctxs]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ends = [torch.cuda.Event() for _ in ctxs]
+    e0.record(side)
+    for st in streams:
+        st.wait_event(e0)
+    for _ in range(args.steps):
+        for g in ctxs:
+            g.step(1, stats=False)
+    for ev, st in zip(ends, streams):
+        ev.record(st)
+    for ev in ends:
+        side.wait_event(ev)
+    e1.record(side)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    nt = np.array([int(g.download()["ntrack"][0]) for g in ctxs])
+    for g in ctxs:
+        g.close()
+    return ms, nt
+
+
 def sweep_arm(args, dev_index, max_over_ranks, barrier, ws):
     """C4: independent BM1D runs of uneven size and parameters, one persistent
     launch per step (one CTA per run, work queue longest-first), regrid, shock
@@ -730,6 +857,7 @@ def sweep_arm(args, dev_index, max_over_ranks, barrier, ws):
     barrier()
     per_launch = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     ms = max_over_ranks(sum(per_launch))
+    nt_timed = g.download()["ntrack"].copy()
     # end to end from pinned host memory: upload, K steps, download of the
     # primitives.  These K steps start from the initial state, whose first
     # regrids merge most cells one run at a time and want many resident runs,
@@ -773,6 +901,16 @@ def sweep_arm(args, dev_index, max_over_ranks, barrier, ws):
         res["learned_guess"] = learned_arm(args, g, cfg, upload, stream, plain_out, (0, 1, 2, 4, 5, 6, 7, 8, 9),
                                            max_over_ranks, barrier, ws, stats0)
     g.close()
+    if not args.no_plain:
+        ms_p, nt_p = sweep_plain(args, kws, states)
+        ms_p = max_over_ranks(ms_p)
+        res["plain"] = {"value": ws * zones / (ms_p / 1e3), "ms_per_step": ms_p / args.steps,
+                        "same_cell_counts": bool(np.array_equal(nt_p, nt_timed)),
+                        "note": "one context per run (1,024 gamma_gpu_step calls per step, each one CTA on its "
+                                "own stream), default launch shape, no graph, no tuner"}
+        res["batched_over_plain"] = res["value"] / res["plain"]["value"]
+        if "learned_guess" in res:
+            res["learned_over_plain"] = res["learned_guess"]["value"] / res["plain"]["value"]
     if not args.no_cpu_baseline and ws == 1 and os.path.exists(os.path.join(ROOT, "oracle", "_ref",
                                                                             "libref_bm1d.so")):
         res["cpu_baseline"] = sweep_cpu_baseline(kws, os.cpu_count() or 1, max(args.warmup, 3))
@@ -818,6 +956,8 @@ def run_gpu_arm(args):
             res = sweep_arm(args, local, max_over_ranks, barrier, ws)
         elif args.workload == "c2p":
             res = c2p_arm(args, local)
+        elif args.workload == "sweep2d":
+            res = jet2d_c4_arm(args, local)
         if args.workload != "tubes":
             if rank == 0:
                 print(json.dumps(dict({"metric": METRIC, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -918,6 +1058,8 @@ def run_gpu_arm(args):
         line["jet2d"] = jet2d_arm(args, local, host_work=(ws == 1 and rank == 0))
     if not args.no_sweep and args.workload == "all":
         line["sweep"] = sweep_arm(args, local, max_over_ranks, barrier, ws)
+    if not args.no_c4_2d and args.workload == "all":
+        line["sweep2d"] = jet2d_c4_arm(args, local)
     if not args.no_c2p and args.workload == "all" and rank == 0:
         line["c2p"] = c2p_arm(args, local, host_work=(ws == 1))
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -926,6 +1068,7 @@ def run_gpu_arm(args):
         v, info, _ = cpu_run(setups_cpu, 50, 2, sample=max(64, cores * 2), cores=cores,
                              budget_zones=float(os.environ.get("GAMMA_CPU_ZONES", 3.0e7)))
         line["cpu_baseline"] = dict(info, value=v, unit="zone-updates/s")
+    line["summary"] = summary_of(line)
     if rank == 0:
         print(json.dumps(line))
     if ws > 1:
@@ -945,13 +1088,16 @@ def main():
     ap.add_argument("--no-dump", action="store_true", help="skip the 2D text dump and resume timing")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape of the 1D step")
     ap.add_argument("--variant", type=int, default=None, help="a fixed launch shape of the 1D step (no tuning)")
-    ap.add_argument("--workload", default="all", choices=["all", "tubes", "jet2d", "sweep", "c2p"],
+    ap.add_argument("--workload", default="all", choices=["all", "tubes", "jet2d", "sweep", "sweep2d", "c2p"],
                     help="one workload alone (profiling captures); 'all' prints the tube line with the others nested")
     ap.add_argument("--ntubes", type=int, default=NTUBES, help="smaller batches for profiling captures")
     ap.add_argument("--ntheta", type=int, default=JET2D["ntheta"], help="theta tracks of the 2D workload")
     ap.add_argument("--sweep-runs", type=int, default=SWEEP_RUNS, help="runs of the BM1D sweep")
     ap.add_argument("--c2p-states", type=int, default=C2P_STATES, help="states of the cons2prim batch")
     ap.add_argument("--no-c2p", action="store_true", help="skip the cons2prim batch")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain (one context per run) sweep arm")
+    ap.add_argument("--no-c4-2d", action="store_true", help="skip the large 2D case of the sweep workload")
+    ap.add_argument("--c4-ntheta", type=int, default=JET2D_C4["ntheta"], help="theta tracks of the large 2D case")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
