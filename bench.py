@@ -385,13 +385,14 @@ def jet2d_arm(args, dev_index, host_work=True):
             "max_newton_iters": st_l["c2p_max_iters"], "fallbacks": st_l["c2p_fallbacks"],
             "fallback_rate": st_l["c2p_fallbacks"] / max(st_l["c2p_calls"], 1),
             "guess_rate": st_l["c2p_guesses"] / max(st_l["c2p_calls"], 1),
+            "poor_warm_start_rate": st_l["c2p_poor"] / max(st_l["c2p_calls"], 1),
+            "steps_with_guess": st_l["learned_steps"], "steps_timed": args.steps,
             "plain_mean_newton_iters": res["c2p"]["mean_newton_iters"],
             "plain_max_newton_iters": res["c2p"]["max_newton_iters"],
             "same_cell_counts": same, "l1_vs_plain": l1, "steps_compared": max(args.warmup, 3) + 1 + args.steps,
             "training": train,
-            "note": "cons2prim evaluates f at the previous pressure first and starts from the network's pressure "
-                    "only where |f| > 1e-4 E there (guess_rate); regrid merges keep the warm start; Newton still "
-                    "converges to the reference tolerance"}
+            "note": GATE_NOTE + " (guess_rate); regrid merges keep the warm start; Newton still converges to the "
+                    "reference tolerance"}
         res["learned_over_plain"] = res["learned_guess"]["value"] / res["plain"]["value"]
         del P
     lib = os.path.join(ROOT, "oracle", "_ref", "libref_jet2d.so")
@@ -473,6 +474,8 @@ def summary_of(line):
         out[f"{w}_batched_over_plain"] = get(line, w, "batched_over_plain")
         out[f"{w}_learned_over_plain"] = get(line, w, "learned_over_plain")
         out[f"{w}_learned_guess_rate"] = get(line, w, "learned_guess", "guess_rate")
+        lv, bv = out[f"{w}_learned_value"], out[f"{w}_value"]
+        out[f"{w}_learned_over_batched"] = lv / bv if lv and bv else None
         out[f"{w}_frac"] = get(line, w, "roofline", "frac")
     out["c4_2d_value"] = get(line, "sweep2d", "value")
     out["c4_2d_zones_per_step"] = get(line, "sweep2d", "zones_per_step")
@@ -501,6 +504,11 @@ def autotune(g, args):
             "ms_per_3_steps": {f"{a}x{b}": round(m, 3) for m, (a, b) in
                                zip(ms, (gpu.variant_info(k) for k in range(gpu.N_VARIANTS)))}}
 
+
+GATE_NOTE = ("a step runs the kernel with the network only if the previous step found poor warm starts (first "
+             "Newton correction above 3% of the previous pressure) in more than a quarter of its cons2prim calls "
+             "(steps_with_guess of steps_timed); there, cells with a poor warm start search again from the network's "
+             "pressure")
 
 TRAIN_PAIRS = 10_000_000  # the learned guess's training set (half from solution states where there are enough)
 
@@ -555,6 +563,9 @@ def learned_arm(args, g, cfg, upload, stream, plain_out, rows, max_over_ranks, b
     out = g.download()
     P, train = train_guess(cfg, out["prim"], live_cells(g.offsets, out["ntrack"]), SEED)
     g.set_guess(P.data_ptr())
+    # the launch shape of the step with the guess, tuned like the plain step's
+    plain_variant = g.variant
+    tune = autotune(g, args)
     # results: K steps from the initial state, against the plain run's K steps
     upload()
     g.step(args.steps, stats=False)
@@ -566,29 +577,34 @@ def learned_arm(args, g, cfg, upload, stream, plain_out, rows, max_over_ranks, b
     for _ in range(args.warmup):
         g.step(1, stats=False)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    zones = 0
+    zones = learned = poor = calls = 0
     barrier()
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
         ev[0].record(stream)
         for k in range(args.steps):
-            zones += g.step(1)["zone_updates"]
+            s1 = g.step(1)
+            zones += s1["zone_updates"]
+            learned += s1["learned_steps"]
+            poor += s1["c2p_poor"]
+            calls += s1["c2p_calls"]
             ev[k + 1].record(stream)
     torch.cuda.synchronize()
     barrier()
     ms = max_over_ranks(sum(ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)))
     st = g.step(1)
     g.set_guess(0)
+    g.set_variant(plain_variant)
     return {
         "value": ws * zones / (ms / 1e3), "unit": "zone-updates/s", "ms_per_step": ms / args.steps,
         "mean_newton_iters": st["c2p_iters"] / max(st["c2p_calls"], 1), "max_newton_iters": st["c2p_max_iters"],
         "fallbacks": st["c2p_fallbacks"], "fallback_rate": st["c2p_fallbacks"] / max(st["c2p_calls"], 1),
         "guess_rate": st["c2p_guesses"] / max(st["c2p_calls"], 1),
+        "poor_warm_start_rate": poor / max(calls, 1), "steps_with_guess": learned, "steps_timed": args.steps,
         "plain_mean_newton_iters": plain_stats["c2p_iters"] / max(plain_stats["c2p_calls"], 1),
         "l1_vs_plain": l1, "same_cell_counts": same, "steps_compared": args.steps, "training": train,
-        "note": "cons2prim evaluates f at the previous pressure first and starts from the network's pressure only "
-                "where |f| > 1e-4 E there (guess_rate of the calls); Newton still converges to the reference "
-                "tolerance",
+        "launch_shape": tune,
+        "note": GATE_NOTE + " (guess_rate of the calls); Newton still converges to the reference tolerance",
     }
 
 

@@ -51,16 +51,37 @@ constexpr int kThreads = 256;
 
 struct Stats2 {
   unsigned long long c2p_calls, c2p_iters, c2p_fallbacks, c2p_max_iters, splits, merges, zone_updates;
-  unsigned long long c2p_guesses;
+  unsigned long long c2p_guesses, c2p_poor, learned_steps;
 };
 
+// The choice between the cell update and the cell update with the learned
+// guess (use_guess, nonzero: the guess), made at the start of every step from
+// the previous step's cell updates: their cons2prim calls and those whose
+// warm start was poor (mlp::kGuessPolicy).  With no previous step (after
+// gamma_2d_set_guess or an upload) the choice stays.
+struct Policy2 {
+  int use_guess;
+  unsigned long long calls, poor;
+};
+
+__global__ void k_guess_policy2(Policy2 *pol, Stats2 *S) {
+  if (pol->calls) pol->use_guess = (double)pol->poor > mlp::kGuessPolicy * (double)pol->calls ? 1 : 0;
+  pol->calls = 0;
+  pol->poor = 0;
+  if (pol->use_guess) S->learned_steps += 1;
+}
+
+// A warp's cons2prim statistics into the launch totals (and, with pol, into
+// the learned-guess choice's counts).
 __device__ void add_stats(Stats2 *S, unsigned long long calls, unsigned long long iters, unsigned long long fb,
-                          unsigned long long mx, unsigned long long guesses = 0) {
+                          unsigned long long mx, unsigned long long guesses, unsigned long long poor,
+                          Policy2 *pol) {
   for (int o = 16; o > 0; o >>= 1) {
     calls += __shfl_xor_sync(0xffffffffu, calls, o);
     iters += __shfl_xor_sync(0xffffffffu, iters, o);
     fb += __shfl_xor_sync(0xffffffffu, fb, o);
     guesses += __shfl_xor_sync(0xffffffffu, guesses, o);
+    poor += __shfl_xor_sync(0xffffffffu, poor, o);
     const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, mx, o);
     mx = m2 > mx ? m2 : mx;
   }
@@ -69,7 +90,12 @@ __device__ void add_stats(Stats2 *S, unsigned long long calls, unsigned long lon
     atomicAdd(&S->c2p_iters, iters);
     if (fb) atomicAdd(&S->c2p_fallbacks, fb);
     if (guesses) atomicAdd(&S->c2p_guesses, guesses);
+    if (poor) atomicAdd(&S->c2p_poor, poor);
     atomicMax(&S->c2p_max_iters, mx);
+    if (pol) {
+      atomicAdd(&pol->calls, calls);
+      if (poor) atomicAdd(&pol->poor, poor);
+    }
   }
 }
 
@@ -240,39 +266,17 @@ __global__ void k_iface(Grid2 G, int stage) {
   FOR_LIVE_CELLS(G, j, i) iface_move(G, j, i, stage);
 }
 
-// Learned cons2prim starting pressure for the 32 cells of a warp (BF16 tensor
-// cores, mlp.cuh).  The network sees |S| = sqrt(S_r^2 + (S_theta / r)^2), the
-// momentum magnitude cons2prim solves with; a non-finite or non-positive
-// guess keeps the warm start.
-// The learned start of the 2D cell update: f at the warm start first; the
-// network's pressure replaces the warm start only where |f| exceeds
-// mlp::kGuessGate of E (c2p[4] counts those calls), and runs only when a lane
-// of the warp needs it.
+// The learned start of the 2D cell update (BF16 tensor cores, mlp.cuh): the
+// network's pressure for the warp's cells whose warm start was poor.  It sees
+// |S| = sqrt(S_r^2 + (S_theta / r)^2), the momentum magnitude cons2prim solves
+// with.
 struct LearnedStart {
+  static constexpr bool ON = true;
   const mlp::InferSmem *inf;
-  __device__ const C2PStart *operator()(const Phys &ph, const double *cons, double *prim, bool upd, double r,
-                                        C2PStart &wbuf, unsigned long long *c2p) const {
-    bool need = false;
-    if (upd) {
-      const C2PInput2 in = c2p_input(cons, prim, r);
-      wbuf = c2p_start<Cfg2>(ph, in.D, in.S, in.S2, in.E, in.pCand);
-      need = !(fabs(wbuf.f) <= mlp::kGuessGate * in.E);
-    }
-    if (__any_sync(0xffffffffu, need)) {
-      float f[3] = {0.f, 0.f, 0.f}, o[2] = {0.f, 0.f};
-      if (need) {
-        const double s1 = cons[SS1], s2 = cons[SS2] / r;
-        mlp::features(cons[DEN], cons[TAU], sqrt(s1 * s1 + s2 * s2), f);
-      }
-      __syncwarp();
-      mlp::infer_warp(*inf, f, o);
-      if (need) {
-        const double pg = mlp::guess_pressure(cons[DEN], o[0]);
-        if (isfinite(pg) && pg > 0.) prim[PPP] = pg;
-        c2p[4] += 1;
-      }
-    }
-    return need ? nullptr : &wbuf;
+  __device__ bool any(bool need) const { return __any_sync(0xffffffffu, need); }
+  __device__ double operator()(const double *cons, double r, bool need) const {
+    const double s1 = cons[SS1], s2 = cons[SS2] / r;
+    return mlp::warp_guess_pressure(*inf, cons[DEN], cons[TAU], sqrt(s1 * s1 + s2 * s2), need);
   }
 };
 
@@ -280,10 +284,14 @@ struct LearnedStart {
 // parameters of the network), the loop runs warp-uniform so that every lane
 // takes part in the tensor-core inference; the weights are staged in shared
 // memory once per block.
+// With pol (a learned guess set), both variants are launched and the one
+// k_guess_policy2 did not choose returns at once.
 template <bool GUESS>
 __global__ void __launch_bounds__(kThreads, GB2_MINB_UP)
-    k_update(Phys ph, Params2 P, Grid2 G, int stage, Stats2 *S, const float *guess) {
-  unsigned long long c2p[5] = {0, 0, 0, 0, 0};  // calls, iterations, fallbacks, max, learned starts
+    k_update(Phys ph, Params2 P, Grid2 G, int stage, Stats2 *S, const float *guess, Policy2 *pol) {
+  if (pol && ((pol->use_guess != 0) != GUESS)) return;
+  // calls, iterations, fallbacks, max, learned starts, poor warm starts
+  unsigned long long c2p[6] = {0, 0, 0, 0, 0, 0};
   if (!GUESS) {
     FOR_LIVE_CELLS(G, j, i) update_cell(ph, P, G, j, i, stage, c2p, true, WarmStart{});
   } else {
@@ -301,7 +309,7 @@ __global__ void __launch_bounds__(kThreads, GB2_MINB_UP)
       update_cell(ph, P, G, j, i, stage, c2p, live, ls);
     }
   }
-  add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3], c2p[4]);
+  add_stats(S, c2p[0], c2p[1], c2p[2], c2p[3], c2p[4], c2p[5], pol);
 }
 
 // Grid::printCols' side effect with shock detection (text2d.cpp:147-153):
@@ -337,6 +345,7 @@ struct gamma_2d {
   Stats2 *d_stats = nullptr;
   const float *guess = nullptr;  // learned cons2prim start (device parameters), or none
   int *d_flags = nullptr;  // [NJ] regrid flags
+  Policy2 *d_policy = nullptr;  // the learned guess's choice (k_guess_policy2)
   std::vector<double> tg;  // host copy of the per-track factors
   std::vector<double> theta, dtheta;  // of the active tracks, as given at creation
   std::string err;
@@ -405,6 +414,7 @@ int enqueue_step_until(gamma_2d *c, int upto) {
   const Grid2 &G = c->G;
   cudaStream_t s = c->stream;
   const int nb = cell_blocks(c);
+  if (c->guess) k_guess_policy2<<<1, 1, 0, s>>>(c->d_policy, c->d_stats);
   k_regrid_check<<<1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst);
   k_regrid<<<1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst, 1);
   if (c->cfg.ntheta > 1) {
@@ -432,11 +442,10 @@ int enqueue_step_until(gamma_2d *c, int upto) {
       k_dtfinal<<<1, kThreads, 0, s>>>(G, nb, c->cfg.cfl);
     }
     k_iface<<<nb, kThreads, 0, s>>>(G, stage);
-    if (c->guess) {
-      k_update<true><<<nb, kThreads, sizeof(mlp::InferSmem), s>>>(ph, P, G, stage, c->d_stats, c->guess);
-    } else {
-      k_update<false><<<nb, kThreads, 0, s>>>(ph, P, G, stage, c->d_stats, nullptr);
-    }
+    Policy2 *pol = c->guess ? c->d_policy : nullptr;
+    k_update<false><<<nb, kThreads, 0, s>>>(ph, P, G, stage, c->d_stats, nullptr, pol);
+    if (c->guess)
+      k_update<true><<<nb, kThreads, sizeof(mlp::InferSmem), s>>>(ph, P, G, stage, c->d_stats, c->guess, pol);
   }
   k_advance<<<1, 32, 0, s>>>(G, c->d_stats);
   G2_CUDA(c, cudaGetLastError());
@@ -570,6 +579,7 @@ GAMMA_API int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta,
   G2_ALLOC(G.rnbr2, 4 * NC * sizeof(int));
   G2_ALLOC(c->d_stats, sizeof(Stats2));
   G2_ALLOC(c->d_flags, (size_t)c->NJ * sizeof(int) + 4 * d + 8);
+  G2_ALLOC(c->d_policy, sizeof(Policy2));
 #undef G2_ALLOC
   if ((e = cudaMemcpyAsync(tg_d, c->tg.data(), c->tg.size() * d, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
     return bail(e, "copy track factors");
@@ -602,8 +612,22 @@ GAMMA_API int gamma_2d_set_params(gamma_2d_t *ctx, const gamma_2d_params_t *para
   return GAMMA_OK;
 }
 
+namespace {
+// the next step with a learned guess set starts with it (k_guess_policy2)
+int reset_policy(gamma_2d *c) {
+  const Policy2 p{1, 0ull, 0ull};
+  G2_CUDA(c, cudaMemcpyAsync(c->d_policy, &p, sizeof(p), cudaMemcpyHostToDevice, c->stream));
+  G2_CUDA(c, cudaStreamSynchronize(c->stream));  // p is a stack buffer
+  return GAMMA_OK;
+}
+}  // namespace
+
 GAMMA_API int gamma_2d_set_guess(gamma_2d_t *ctx, const float *params) {
   if (!ctx) return GAMMA_ERR_INVALID;
+  if (params && !ctx->guess) {
+    const int rc = reset_policy(ctx);
+    if (rc != GAMMA_OK) return rc;
+  }
   ctx->guess = params;
   drop_graph(ctx);
   return GAMMA_OK;
@@ -657,7 +681,7 @@ GAMMA_API int gamma_2d_upload(gamma_2d_t *ctx, const int *ntrack, const double *
     G2_CUDA(c, cudaGetLastError());
   }
   G2_CUDA(c, cudaStreamSynchronize(s));  // host staging vectors go out of scope
-  return GAMMA_OK;
+  return reset_policy(c);  // a new state: no step has measured its warm starts
 }
 
 GAMMA_API int gamma_2d_use_graphs(gamma_2d_t *ctx, int on) {
@@ -709,6 +733,8 @@ GAMMA_API int gamma_2d_step(gamma_2d_t *ctx, int nsteps, gamma_step_stats_t *sta
     stats->status = status == 30 ? GAMMA_ERR_NEG_DT : (status ? GAMMA_ERR_INVALID : GAMMA_OK);
     stats->device_ms = ms;
     stats->c2p_guesses = h.c2p_guesses;
+    stats->c2p_poor = h.c2p_poor;
+    stats->learned_steps = h.learned_steps;
   }
   return GAMMA_OK;
 }

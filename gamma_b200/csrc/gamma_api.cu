@@ -93,17 +93,16 @@ struct gamma_ctx {
   int *d_order = nullptr;
   int *d_queue = nullptr;
   gb::StepStats *d_stats = nullptr;
-  int grid = 0;
-  size_t smem = 0;
-  int grid_guess = 0;  // launch shape of the kernel with the learned guess
-  size_t smem_guess = 0;
+  int *d_use_guess = nullptr;  // k_guess_policy's choice for the next call
   bool graphs = true;  // steps replayed from a captured CUDA graph
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   long long gkey[4] = {-1, -1, -1, -1};  // nsteps, variant, guess pointer, regrid_only of the graph
   int variant = 0;     // step-kernel launch shape (tune.h); 0 = the default kernel
-  int vgrid[gb::tune::kVariants] = {};
-  size_t vsmem[gb::tune::kVariants] = {};
+  // grid and shared memory of each launch shape, without [0] and with [1] the
+  // learned guess (grid 0: not configured yet)
+  int vgrid[2][gb::tune::kVariants] = {};
+  size_t vsmem[2][gb::tune::kVariants] = {};
   std::string err;
 };
 
@@ -163,7 +162,17 @@ gb::Phys phys_of(const gamma_config_t &c) {
   return p;
 }
 
-// Launch shape v (with the learned guess: v = 0) of the context's step kernel.
+// The choice between the step kernel and the step kernel with the learned
+// guess for the next call (*use_guess, nonzero: the guess): with the guess
+// where the previous call that stepped found poor warm starts in more than
+// gb::mlp::kGuessPolicy of its cons2prim calls.  A call that did not step (a
+// regrid alone, or none since the upload) keeps the choice.
+__global__ void k_guess_policy(const gb::StepStats *prev, int *use_guess) {
+  if (prev->zone_updates == 0) return;
+  *use_guess = (double)prev->c2p_poor > gb::mlp::kGuessPolicy * (double)prev->c2p_calls ? 1 : 0;
+}
+
+// Launch shape v of the context's step kernel, without or with the learned guess.
 int configure_launch(gamma_ctx *c, int v, bool guess, int *grid, size_t *smem) {
   GB_CUDA(c, c->prob->configure(v, guess, c->nruns, c->max_cap, grid, smem));
   return GAMMA_OK;
@@ -321,6 +330,7 @@ GAMMA_API int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *
   GB_ALLOC(c->d_order, nruns * sizeof(int));
   GB_ALLOC(c->d_queue, sizeof(int));
   GB_ALLOC(c->d_stats, sizeof(gb::StepStats));
+  GB_ALLOC(c->d_use_guess, sizeof(int));
 #undef GB_ALLOC
   T.off = d_off;
   T.cap = d_cap;
@@ -333,7 +343,7 @@ GAMMA_API int gamma_gpu_create(const gamma_config_t *cfg, int nruns, const int *
       cudaSuccess)
     return fail(e, "copy capacities");
   if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return fail(e, "sync");
-  int rc = configure_launch(c, 0, false, &c->grid, &c->smem);
+  int rc = configure_launch(c, 0, false, &c->vgrid[0][0], &c->vsmem[0][0]);
   if (rc != GAMMA_OK) {
     gamma_gpu_destroy(c);
     return rc;
@@ -419,6 +429,10 @@ GAMMA_API int gamma_gpu_upload(gamma_ctx_t *ctx, const int *ntrack, const double
   }
   GB_CUDA(ctx, cudaMemcpyAsync(T.run, rs.data(), R * sizeof(gb::RunState), cudaMemcpyHostToDevice, ctx->stream));
   GB_CUDA(ctx, cudaMemcpyAsync(ctx->d_order, order.data(), R * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  // a new state: no step has measured its warm starts, so the next step with
+  // a learned guess set starts from it (k_guess_policy keeps the choice)
+  GB_CUDA(ctx, cudaMemsetAsync(ctx->d_stats, 0, sizeof(gb::StepStats), ctx->stream));
+  GB_CUDA(ctx, cudaMemsetAsync(ctx->d_use_guess, 0xff, sizeof(int), ctx->stream));
   GB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // rs/order are stack buffers
   return GAMMA_OK;
 }
@@ -433,18 +447,25 @@ void drop_graph(gamma_ctx_t *ctx) {
 }
 
 // The launches of one call: queue and statistics reset, then the step kernel.
+// With a learned guess set, k_guess_policy first reads the previous call's
+// statistics, and both step kernels are launched: the one it chose runs, the
+// other returns at once.
 int enqueue_steps(gamma_ctx_t *ctx, int nsteps, int regrid_only) {
+  const bool guess = ctx->T.mlp != nullptr && !regrid_only;
+  if (guess) {
+    k_guess_policy<<<1, 1, 0, ctx->stream>>>(ctx->d_stats, ctx->d_use_guess);
+    GB_CUDA(ctx, cudaGetLastError());
+  }
   GB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(int), ctx->stream));
   GB_CUDA(ctx, cudaMemsetAsync(ctx->d_stats, 0, sizeof(gb::StepStats), ctx->stream));
-  const bool guess = ctx->T.mlp != nullptr && !regrid_only;
-  // the learned guess has the default shape only; the plain kernel the tuned one
-  const int v = guess ? 0 : ctx->variant;
-  const int grid = guess ? ctx->grid_guess : (v > 0 ? ctx->vgrid[v] : ctx->grid);
-  const size_t smem = guess ? ctx->smem_guess : (v > 0 ? ctx->vsmem[v] : ctx->smem);
-  const cudaError_t e = ctx->prob->launch(v, guess, grid, smem, ctx->stream, ctx->T, phys_of(ctx->cfg), nsteps,
-                                          ctx->d_order, ctx->nruns, ctx->d_queue, ctx->d_stats, regrid_only,
-                                          ctx->max_cap);
-  if (e != cudaSuccess) return fail_cuda(ctx, e, "step launch");
+  const int v = ctx->variant;
+  for (int k = 0; k <= (guess ? 1 : 0); ++k) {
+    const cudaError_t e = ctx->prob->launch(v, k == 1, ctx->vgrid[k][v], ctx->vsmem[k][v], ctx->stream, ctx->T,
+                                            phys_of(ctx->cfg), nsteps, ctx->d_order, ctx->nruns, ctx->d_queue,
+                                            ctx->d_stats, regrid_only, ctx->max_cap,
+                                            guess ? ctx->d_use_guess : nullptr);
+    if (e != cudaSuccess) return fail_cuda(ctx, e, "step launch");
+  }
   return GAMMA_OK;
 }
 
@@ -490,6 +511,8 @@ int run_steps(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *stats, int regri
     stats->merges = h.merges;
     stats->c2p_max_iters = h.c2p_max_iters;
     stats->c2p_guesses = h.c2p_guesses;
+    stats->c2p_poor = h.c2p_poor;
+    stats->learned_steps = h.learned ? (unsigned long long)nsteps : 0ull;
     stats->status = h.status == 30 ? GAMMA_ERR_NEG_DT : (h.status ? GAMMA_ERR_INVALID : GAMMA_OK);
     stats->device_ms = ms;
   }
@@ -503,9 +526,13 @@ GAMMA_API int gamma_gpu_step(gamma_ctx_t *ctx, int nsteps, gamma_step_stats_t *s
 
 GAMMA_API int gamma_gpu_set_guess(gamma_ctx_t *ctx, const float *params) {
   if (!ctx) return GAMMA_ERR_INVALID;
-  if (params && !ctx->grid_guess) {
-    int rc = configure_launch(ctx, 0, true, &ctx->grid_guess, &ctx->smem_guess);
+  if (params && !ctx->vgrid[1][ctx->variant]) {
+    int rc = configure_launch(ctx, ctx->variant, true, &ctx->vgrid[1][ctx->variant], &ctx->vsmem[1][ctx->variant]);
     if (rc != GAMMA_OK) return rc;
+  }
+  if (params && !ctx->T.mlp) {  // the next step starts with the guess (k_guess_policy)
+    GB_CUDA(ctx, cudaMemsetAsync(ctx->d_stats, 0, sizeof(gb::StepStats), ctx->stream));
+    GB_CUDA(ctx, cudaMemsetAsync(ctx->d_use_guess, 0xff, sizeof(int), ctx->stream));
   }
   ctx->T.mlp = params;
   return GAMMA_OK;
@@ -695,8 +722,9 @@ GAMMA_API int gamma_gpu_variant_info(int variant, int *threads, int *cells_per_t
 
 GAMMA_API int gamma_gpu_set_variant(gamma_ctx_t *ctx, int variant) {
   if (!ctx || variant < 0 || variant >= gb::tune::kVariants) return GAMMA_ERR_INVALID;
-  if (variant > 0 && ctx->vgrid[variant] == 0) {
-    const int rc = configure_launch(ctx, variant, false, &ctx->vgrid[variant], &ctx->vsmem[variant]);
+  for (int guess = 0; guess < 2; ++guess) {
+    if (ctx->vgrid[guess][variant] != 0 || (guess && !ctx->T.mlp)) continue;
+    const int rc = configure_launch(ctx, variant, guess != 0, &ctx->vgrid[guess][variant], &ctx->vsmem[guess][variant]);
     if (rc != GAMMA_OK) return rc;
   }
   ctx->variant = variant;
@@ -709,7 +737,6 @@ GAMMA_API int gamma_gpu_get_variant(const gamma_ctx_t *ctx) { return ctx ? ctx->
 // state back after each, and keeps the fastest.
 GAMMA_API int gamma_gpu_autotune(gamma_ctx_t *ctx, int nsteps, float *ms, int *chosen) {
   if (!ctx || nsteps < 1) return GAMMA_ERR_INVALID;
-  if (ctx->T.mlp) return GAMMA_ERR_INVALID;  // the learned-guess kernel has one shape
   const gb::Tracks &T = ctx->T;
   const size_t N = (size_t)ctx->N, d = sizeof(double), R = (size_t)ctx->nruns;
   struct Arr {

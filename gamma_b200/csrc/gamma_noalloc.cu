@@ -145,7 +145,7 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
   auto *qs = reinterpret_cast<int *>(ws + off_queue);
   auto *st = reinterpret_cast<gb::StepStats *>(ws + off_stats);
   if (tube->launch(0, false, grid, smem, s, T, ph, nsteps, reinterpret_cast<const int *>(ws + off_order), nruns, qs,
-                   st, 0, 0) != cudaSuccess)
+                   st, 0, 0, nullptr) != cudaSuccess)
     return GAMMA_ERR_CUDA;
 
   if (stats) {
@@ -160,6 +160,8 @@ extern "C" GAMMA_API int gamma_gpu_step_tubes_noalloc(const gamma_config_t *cfg,
     stats->merges = h.merges;
     stats->c2p_max_iters = h.c2p_max_iters;
     stats->c2p_guesses = h.c2p_guesses;
+    stats->c2p_poor = h.c2p_poor;
+    stats->learned_steps = 0;
     stats->status = h.status == 30 ? GAMMA_ERR_NEG_DT : (h.status ? GAMMA_ERR_INVALID : GAMMA_OK);
     stats->device_ms = 0.f;
   }

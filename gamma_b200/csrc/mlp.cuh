@@ -64,9 +64,14 @@ __device__ __forceinline__ double guess_pressure(double D, float y0) {
 }
 
 // Inside a time step the previous pressure is the better start almost
-// everywhere (Newton stops after one or two iterations).  The network starts
-// cons2prim only where f at that warm start exceeds this fraction of E = D + tau.
-constexpr double kGuessGate = 1e-4;
+// everywhere (Newton stops after one or two iterations from it), so the steps
+// start cons2prim from the network only where that warm start is poor
+// (c2p_warm_start_poor in physics.cuh), and only in steps whose previous step
+// found more than this fraction of its searches with a poor warm start (or
+// that follow no step): the step with the guess carries the network's weights,
+// its call sites and the waits of a warp's neighbours for it, which cost more
+// than it saves where poor warm starts are rare.
+constexpr double kGuessPolicy = 0.25;
 
 // FP32 forward of one sample; optional pre-activations and activations for
 // the backward pass (h1, h2 may be strided rows of shared memory)
@@ -211,6 +216,21 @@ __device__ __forceinline__ void infer_warp(const InferSmem &s, const float f[3],
       out[1] = ((r & 8) ? hi1 : lo1) + s.b3[1];
     }
   }
+}
+
+// The network's starting pressure for the cells of a warp from their
+// conserved D, tau and momentum magnitude S: every lane calls, lanes with
+// on = false only take part in the tensor-core tiles (their result is 0).
+// Out of line, with scalar arguments: inlined into a step's loop, the
+// fragments took registers from it, which then spilled on every cell, guessed
+// or not.
+static __device__ __noinline__ double warp_guess_pressure(const InferSmem &s, double D, double tau, double S,
+                                                          bool on) {
+  float f[3] = {0.f, 0.f, 0.f}, o[2] = {0.f, 0.f};
+  if (on) features(D, tau, S, f);
+  __syncwarp();
+  infer_warp(s, f, o);
+  return on ? guess_pressure(D, o[0]) : 0.;
 }
 
 }  // namespace mlp

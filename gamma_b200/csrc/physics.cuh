@@ -314,7 +314,20 @@ GB_HD void state2flux(const double *prim, const double *cons, double *flux) {
 struct C2PStats {
   int iters;     // f evaluations after the bracket set-up
   int fallback;  // 1 if the iteration cap was hit (bisection-limited)
+  int deferred;  // 1 if a deferring search stopped at a poor warm start (c2p_pressure_body)
+  int poor;      // 1 if a search was needed and its warm start was poor (c2p_warm_start_poor)
 };
+
+// A warm start is poor where the first Newton correction from it, |f/f'|,
+// exceeds this fraction of the pressure: worse than the learned guess's own
+// starting error of a few per cent.  (A build may set another fraction with
+// -DGB_GUESS_GATE=...)
+#ifndef GB_GUESS_GATE
+#define GB_GUESS_GATE 3e-2
+#endif
+constexpr double kGuessGate = GB_GUESS_GATE;
+
+GB_HD bool c2p_warm_start_poor(double f, double df, double p) { return !(fabs(f) <= kGuessGate * fabs(df) * p); }
 
 // f(p) = E + p - D lfac - k p lfac^2 with lfac = (1 - S^2/(E+p)^2)^(-1/2)
 // (rel_sph.cpp:191-210 takes |1 - S^2/W^2|, rel_cart.cpp:108-123 does not).
@@ -390,22 +403,6 @@ GB_HD double c2p_f_ref(const Phys &ph, double p, double D, double S, double E, d
   return f;
 }
 
-// f(p) of the cons2prim root search at its starting pressure, with the slope
-// and Lorentz factor the search reuses (c2p_start below).
-struct C2PStart {
-  double f, df, l2, lf;
-};
-
-// The root search's first evaluation, f at the starting pressure pCand.
-template <class Cfg>
-GB_HD C2PStart c2p_start(const Phys &ph, double D, double S, double S2, double E, double pCand) {
-  C2PStart w;
-  w.lf = -1.;
-  w.f = Cfg::FAST_ROOT ? c2p_f<Cfg>(ph, pCand, D, S2, E, &w.df, &w.l2)
-                       : c2p_f_ref<Cfg>(ph, pCand, D, S, E, &w.df, &w.l2, &w.lf);
-  return w;
-}
-
 // Pressure root of the cons2prim driver (rel_sph.cpp:243-286): the bracket,
 // its no-solution tests and the warm start pCand are the reference's; the
 // Brent search is replaced by safeguarded Newton-Raphson.  Returns the
@@ -415,11 +412,12 @@ GB_HD C2PStart c2p_start(const Phys &ph, double D, double S, double S2, double E
 // returned pressure when the search evaluated f there (the same rounding as
 // f's), else -1.
 //
-// start (optional): f at pCand with its slope, as c2p_start evaluated it for
-// the same pCand; the search then does not evaluate it again.
+// defer (with st): where a search is needed and the warm start is poor
+// (c2p_warm_start_poor), stop before it and set st->deferred; the caller then
+// starts the search again from a better pressure (the learned guess).
 template <class Cfg>
 GB_HD double c2p_pressure_body(const Phys &ph, double D, double S, double S2, double E, double pCand,
-                               C2PStats *st, double *lfac_at, const C2PStart *start) {
+                               C2PStats *st, double *lfac_at, bool defer) {
   auto fval = [&](double p, double *df, double *l2, double *lf, bool p_may_be_zero = false) -> double {
     return Cfg::FAST_ROOT ? c2p_f<Cfg>(ph, p, D, S2, E, df, l2)
                      : c2p_f_ref<Cfg>(ph, p, D, S, E, df, l2, lf, p_may_be_zero);
@@ -428,18 +426,19 @@ GB_HD double c2p_pressure_body(const Phys &ph, double D, double S, double S2, do
   // f at the warm start, with its slope: the search starts there when the
   // warm start lies in the bracket (f does not depend on whether df is asked for)
   double df0, l20, lf0 = -1.;
-  double f_init;
-  if (start) {
-    f_init = start->f;
-    df0 = start->df;
-    l20 = start->l2;
-    lf0 = start->lf;
-  } else {
-    f_init = fval(pCand, &df0, &l20, &lf0);
-  }
+  const double f_init = fval(pCand, &df0, &l20, &lf0);
   if (lfac_at) *lfac_at = lf0;
   // rel_cyl.cpp:161 searches only where |f| exceeds 1e-13 (rel_sph, rel_cart: 0)
+  int poor = 0;
   if (fabs(f_init) > (Cfg::CYL ? 1.e-13 : 0.)) {
+    poor = c2p_warm_start_poor(f_init, df0, pCand);
+    if (defer && st && poor) {
+      st->iters = 0;
+      st->fallback = 0;
+      st->deferred = 1;
+      st->poor = 1;
+      return pCand;
+    }
     double p_lo = fmax(0., (1. + 1e-13) * S - E);
     bool find_p = true;
     if (fval(p_lo, nullptr, nullptr, nullptr, true) < 0) find_p = false;
@@ -496,25 +495,28 @@ GB_HD double c2p_pressure_body(const Phys &ph, double D, double S, double S2, do
   if (st) {
     st->iters = iters;
     st->fallback = fallback;
+    st->deferred = 0;
+    st->poor = poor;
   }
   return pCand;
 }
 
 template <class Cfg>
 GB_HD_OUTLINE double c2p_pressure_outline(const Phys &ph, double D, double S, double S2, double E, double pCand,
-                                          C2PStats *st, double *lfac_at, const C2PStart *start) {
-  return c2p_pressure_body<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at, start);
+                                          C2PStats *st, double *lfac_at, bool defer) {
+  return c2p_pressure_body<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at, defer);
 }
 
 // The cartesian step calls the search from one out-of-line copy: inlined at
 // every call site of the fused step kernel it crowds the instruction cache
 // (3% slower).  The spherical kernels, the 2D passes and the batch cons2prim
-// keep it inline, which is as fast or faster there.
-template <class Cfg>
+// keep it inline, which is as fast or faster there.  OUTLINE forces the
+// out-of-line copy (a second, rarely taken call site).
+template <class Cfg, bool OUTLINE = !Cfg::SPH>
 GB_HD double c2p_pressure(const Phys &ph, double D, double S, double S2, double E, double pCand, C2PStats *st,
-                          double *lfac_at = nullptr, const C2PStart *start = nullptr) {
-  if (Cfg::SPH) return c2p_pressure_body<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at, start);
-  return c2p_pressure_outline<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at, start);
+                          double *lfac_at = nullptr, bool defer = false) {
+  if (!OUTLINE) return c2p_pressure_body<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at, defer);
+  return c2p_pressure_outline<Cfg>(ph, D, S, S2, E, pCand, st, lfac_at, defer);
 }
 
 // What cons2prim's root search is given: D, E = D + tau, S and S^2 of the
@@ -544,14 +546,18 @@ GB_HD C2PInput c2p_input(const double *cons, const double *prim) {
 // Hooks::cons2prim_user (the problem module's FluidState::cons2prim_user,
 // rel_sph.cpp:304) sees rho, p and u before the pressure floor; par is the
 // run's parameter words.
-// start (optional): c2p_start at this state's starting pressure.
-template <class Cfg, class Hooks = gamma_problem::Problem>
+// defer (with st): where the warm start is poor the search stops before it
+// (st->deferred, c2p_pressure_body) and prim and cons are left as they were,
+// for a second call from a better starting pressure.  OUTLINE: the search's
+// out-of-line copy (c2p_pressure).
+template <class Cfg, class Hooks = gamma_problem::Problem, bool OUTLINE = !Cfg::SPH>
 GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, C2PStats *st, const double *par = nullptr,
-                     const C2PStart *start = nullptr) {
+                     bool defer = false) {
   const C2PInput in = c2p_input<Cfg>(cons, prim);
   const double D = in.D, E = in.E, ss = in.ss, S2 = in.S2, S = in.S;
   double lf_root = -1.;
-  const double pCand = c2p_pressure<Cfg>(ph, D, S, S2, E, in.pCand, st, &lf_root, start);
+  const double pCand = c2p_pressure<Cfg, OUTLINE>(ph, D, S, S2, E, in.pCand, st, &lf_root, defer);
+  if (defer && st && st->deferred) return;
 
   double p = pCand;
   double rho, uu;

@@ -295,17 +295,18 @@ GB_HD C2PInput2 c2p_input(const double *cons, const double *prim, double r) {
 }
 
 // FluidState::cons2prim (rel_sph.cpp:213-320) at radius r: warm start from
-// prim[PPP]; cons is rewritten by the closing prim2cons(r).  start
-// (optional): c2p_start at this state's starting pressure.
-GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, double r, C2PStats *st,
-                     const C2PStart *start = nullptr) {
+// prim[PPP]; cons is rewritten by the closing prim2cons(r).  defer, OUTLINE:
+// as in the 1D cons2prim (physics.cuh).
+template <bool OUTLINE = false>
+GB_HD void cons2prim(const Phys &ph, double *cons, double *prim, double r, C2PStats *st, bool defer = false) {
   const C2PInput2 in = c2p_input(cons, prim, r);
   double D = in.D;
   double E = in.E;
   double ss[2] = {in.ss[0], in.ss[1]};
   double S2 = in.S2;
   double S = in.S;
-  double p = c2p_pressure<Cfg2>(ph, D, S, S2, E, in.pCand, st, nullptr, start);
+  double p = c2p_pressure<Cfg2, OUTLINE>(ph, D, S, S2, E, in.pCand, st, nullptr, defer);
+  if (defer && st && st->deferred) return;
   double Ep2 = (E + p) * (E + p);
   double v2 = qdiv(S2, Ep2);
   double lf = 1. / sqrt(fabs(1. - v2));

@@ -3,7 +3,7 @@
 // A module (include/gamma_problem.h) is a struct of hooks plus the module set
 // it runs with.  GAMMA_PROBLEM_MODULE(name, Hooks, modules, id) at the end of
 // its file instantiates the 1D step kernel for it in every launch shape of the
-// autotuner (tune.h) and with the learned cons2prim guess, and adds an entry
+// autotuner (tune.h), without and with the learned cons2prim guess, and adds an entry
 // to the library's registry (gamma_api.cu), through which the C ABI configures
 // and launches it.  The set-up hooks run on the host (initial_state below).
 #pragma once
@@ -23,11 +23,12 @@ struct ProblemEntry {
   int id;       // a fixed id (the built-in GAMMA_PROBLEM_* values), or -1
   int modules;  // gamma_problem::MODULES_*
   bool regrid;  // Hooks::REGRID
-  // launch shape v of the step kernel (with the learned guess: v = 0 only)
+  // launch shape v of the step kernel, without or with the learned guess
   cudaError_t (*configure)(int v, bool guess, int nruns, int max_cap, int *grid, size_t *smem);
+  // gate: nullptr, or the step kernels' choice (track_step_kernel)
   cudaError_t (*launch)(int v, bool guess, int grid, size_t smem, cudaStream_t s, const Tracks &T, const Phys &ph,
                         int nsteps, const int *order, int nruns, int *queue, StepStats *stats, int regrid_only,
-                        int max_cap);
+                        int max_cap, const int *gate);
   // Simu::initialise of one run on the host (prim [NQ][cap])
   int (*initial_state)(const Phys &ph, const double *par, int cap, int *ntrack, double *t, double *prim, double *x,
                        double *dx, double *xI, double *dt_loc);
@@ -84,9 +85,10 @@ struct ModuleKernel {
     return cudaSuccess;
   }
   static cudaError_t launch(int grid, size_t sm, cudaStream_t s, const Tracks &T, const Phys &ph, int nsteps,
-                            const int *order, int nruns, int *queue, StepStats *stats, int regrid_only, int max_cap) {
+                            const int *order, int nruns, int *queue, StepStats *stats, int regrid_only, int max_cap,
+                            const int *gate) {
     fn<<<grid, BS, sm, s>>>(T, ph, nsteps, order, nruns, queue, stats, regrid_only,
-                            module_words_bytes<Hooks>(max_cap));
+                            module_words_bytes<Hooks>(max_cap), gate);
     return cudaGetLastError();
   }
 };
@@ -96,13 +98,11 @@ static_assert(tune::kVariants == 8, "GB_MODULE_SHAPES lists every launch shape")
 
 template <class C, class Hooks>
 cudaError_t module_configure(int v, bool guess, int nruns, int max_cap, int *grid, size_t *smem) {
-  if (guess) {
-    if (v != 0) return cudaErrorInvalidValue;
-    return ModuleKernel<C, Hooks, 0, true>::configure(nruns, max_cap, grid, smem);
-  }
   switch (v) {
-#define GB_CASE(k) \
-  case k: return ModuleKernel<C, Hooks, k, false>::configure(nruns, max_cap, grid, smem);
+#define GB_CASE(k)                                                                       \
+  case k:                                                                                \
+    return guess ? ModuleKernel<C, Hooks, k, true>::configure(nruns, max_cap, grid, smem) \
+                 : ModuleKernel<C, Hooks, k, false>::configure(nruns, max_cap, grid, smem);
     GB_MODULE_SHAPES(GB_CASE)
 #undef GB_CASE
   }
@@ -112,17 +112,14 @@ cudaError_t module_configure(int v, bool guess, int nruns, int max_cap, int *gri
 template <class C, class Hooks>
 cudaError_t module_launch(int v, bool guess, int grid, size_t smem, cudaStream_t s, const Tracks &T, const Phys &ph,
                           int nsteps, const int *order, int nruns, int *queue, StepStats *stats, int regrid_only,
-                          int max_cap) {
-  if (guess) {
-    if (v != 0) return cudaErrorInvalidValue;
-    return ModuleKernel<C, Hooks, 0, true>::launch(grid, smem, s, T, ph, nsteps, order, nruns, queue, stats,
-                                                   regrid_only, max_cap);
-  }
+                          int max_cap, const int *gate) {
   switch (v) {
-#define GB_CASE(k)                                                                                       \
-  case k:                                                                                                \
-    return ModuleKernel<C, Hooks, k, false>::launch(grid, smem, s, T, ph, nsteps, order, nruns, queue, stats, \
-                                                    regrid_only, max_cap);
+#define GB_CASE(k)                                                                                             \
+  case k:                                                                                                      \
+    return guess ? ModuleKernel<C, Hooks, k, true>::launch(grid, smem, s, T, ph, nsteps, order, nruns, queue,  \
+                                                           stats, regrid_only, max_cap, gate)                  \
+                 : ModuleKernel<C, Hooks, k, false>::launch(grid, smem, s, T, ph, nsteps, order, nruns, queue, \
+                                                            stats, regrid_only, max_cap, gate);
     GB_MODULE_SHAPES(GB_CASE)
 #undef GB_CASE
   }

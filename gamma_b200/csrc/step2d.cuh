@@ -654,18 +654,46 @@ GB_HD void iface_move(const Grid2 &G, int j, int i, int stage) {
 // injection of every cell (run after evolve by Simu::run).  Every cell copies this stage's grad_f1 into the
 // persistent one.
 // The starting pressure of cons2prim: the cell's previous pressure (the
-// reference's warm start).  A learned guess replaces it through `guess`, which
-// is called the same number of times (1 in stage 1, 2 after) by every lane of a
-// warp whether or not the lane's cell is updated (`upd`), so that it may work
-// across the warp; `r` is the radius cons2prim divides S_theta by.  It returns
-// the root search's first evaluation when it kept the warm start and made it
-// (into wbuf), else nullptr.
+// reference's warm start).  With a learned guess (Guess::ON), cons2prim stops
+// at a poor warm start (C2PStats::deferred) and those cells search again from
+// guess(cons, r, need), the network's pressure; every lane of a warp calls it
+// together whether or not its cell is updated, so that it may work across the
+// warp, and only when a lane of the warp needs it (Guess::any).  `r` is the
+// radius cons2prim divides S_theta by.
 struct WarmStart {
-  GB_HD const C2PStart *operator()(const Phys &, const double *, double *, bool, double, C2PStart &,
-                                   unsigned long long *) const {
-    return nullptr;
-  }
+  static constexpr bool ON = false;
+  GB_HD bool any(bool) const { return false; }
+  GB_HD double operator()(const double *, double, bool) const { return 0.; }
 };
+
+// cons2prim of one cell at radius r, with its statistics in c2p (calls,
+// iterations, fallbacks, max iterations, starts from the learned guess, poor
+// warm starts)
+template <class Guess>
+GB_HD void cell_cons2prim(const Phys &ph, double *cons, double *prim, double r, bool upd, unsigned long long *c2p,
+                          const Guess &guess) {
+  C2PStats cs;
+  if (upd) cons2prim(ph, cons, prim, r, &cs, Guess::ON);
+  const int poor = upd ? cs.poor : 0;
+  if (Guess::ON) {
+    const bool need = upd && cs.deferred;
+    if (guess.any(need)) {
+      const double pg = guess(cons, r, need);
+      if (need) {
+        if (isfinite(pg) && pg > 0.) prim[PPP] = pg;  // else the warm start stays
+        cons2prim<true>(ph, cons, prim, r, &cs);
+        c2p[4] += 1;
+      }
+    }
+  }
+  if (upd) {
+    c2p[0] += 1;
+    c2p[1] += cs.iters;
+    c2p[2] += cs.fallback;
+    if ((unsigned long long)cs.iters > c2p[3]) c2p[3] = cs.iters;
+    c2p[5] += poor;
+  }
+}
 
 // `live` = false: a lane without a cell (the learned guess' warp-uniform loop).
 template <class Guess>
@@ -716,16 +744,7 @@ GB_HD void update_cell(const Phys &ph, const Params2 &P, const Grid2 &G, int j, 
     xn = G1.r;
     dxn = G1.dr;
   }
-  C2PStart wbuf;
-  const C2PStart *w = guess(ph, cons, prim, upd, r1, wbuf, c2p);
-  C2PStats cs;
-  if (upd) {
-    cons2prim(ph, cons, prim, r1, &cs, w);
-    c2p[0] += 1;
-    c2p[1] += cs.iters;
-    c2p[2] += cs.fallback;
-    if ((unsigned long long)cs.iters > c2p[3]) c2p[3] = cs.iters;
-  }
+  cell_cons2prim(ph, cons, prim, r1, upd, c2p, guess);
   if (stage > 1) {
     if (upd) {
       const double w0 = stage == 2 ? 3. / 4. : 1. / 3.;
@@ -740,14 +759,7 @@ GB_HD void update_cell(const Phys &ph, const Params2 &P, const Grid2 &G, int j, 
       xn = G2.r;
       dxn = G2.dr;
     }
-    const C2PStart *w2 = guess(ph, cons, prim, upd, r2, wbuf, c2p);
-    if (upd) {
-      cons2prim(ph, cons, prim, r2, &cs, w2);
-      c2p[0] += 1;
-      c2p[1] += cs.iters;
-      c2p[2] += cs.fallback;
-      if ((unsigned long long)cs.iters > c2p[3]) c2p[3] = cs.iters;
-    }
+    cell_cons2prim(ph, cons, prim, r2, upd, c2p, guess);
   }
   if (!live) return;
   if (upd) {

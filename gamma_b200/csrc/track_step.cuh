@@ -68,7 +68,10 @@ struct StepStats {
   int c2p_max_iters;
   int status;
   unsigned long long c2p_guesses;  // cons2prim calls started from the learned guess
+  unsigned long long c2p_poor;     // cons2prim calls whose warm start was poor (c2p_warm_start_poor)
+  unsigned long long learned;      // launches of the step with the learned guess that ran
 };
+
 
 // BS threads advance one run; each sweep chunk holds CPT cells per thread
 // (CH = BS * CPT), which a thread takes in turn.  Hooks: the problem module
@@ -220,44 +223,37 @@ struct TrackStep {
     return !(*cand < 0);
   }
 
-  __device__ static void count_c2p(StepStats &st, const C2PStats &cs) {
+  __device__ static void count_c2p(StepStats &st, const C2PStats &cs, int poor) {
     st.c2p_calls++;
+    st.c2p_poor += poor;
     st.c2p_iters += cs.iters;
     st.c2p_fallbacks += cs.fallback;
     st.c2p_max_iters = max(st.c2p_max_iters, cs.iters);
   }
 
-  // Learned cons2prim starting pressure for the cells of this warp (all 32
-  // lanes call; lanes with on = false only take part in the tensor-core tiles).
-  // A non-finite or non-positive guess keeps the warm start.
-  __device__ static void learned_guess(const mlp::InferSmem &inf, const double *cons, double *prim, bool on) {
-    float f[3] = {0.f, 0.f, 0.f}, o[2] = {0.f, 0.f};
-    if (on) mlp::features(cons[DEN], cons[TAU], cons[SS1], f);
-    __syncwarp();
-    mlp::infer_warp(inf, f, o);
-    if (on) {
-      const double pg = mlp::guess_pressure(cons[DEN], o[0]);
-      if (isfinite(pg) && pg > 0.) prim[PPP] = pg;
+  // cons2prim of one cell, with the learned guess (GUESS): the search stops at
+  // a poor warm start (C2PStats::deferred) and those cells search again from
+  // the network's pressure (a non-finite or non-positive guess keeps the warm
+  // one).  Every lane of the warp calls (upd = false: no cell); the network
+  // runs only when a lane of the warp needs it, and the second search is the
+  // out-of-line copy, so that the step's own loop stays as without the guess.
+  __device__ static void cell_cons2prim(const mlp::InferSmem *inf, const Phys &ph, double *cons, double *prim,
+                                        bool upd, StepStats &st, const double *par) {
+    C2PStats cs;
+    if (upd) cons2prim<Cfg, Hooks>(ph, cons, prim, &cs, par, GUESS);
+    const int poor = upd ? cs.poor : 0;
+    if (GUESS) {
+      const bool need = upd && cs.deferred;
+      if (__any_sync(0xffffffffu, need)) {
+        const double pg = mlp::warp_guess_pressure(*inf, cons[DEN], cons[TAU], cons[SS1], need);
+        if (need) {
+          if (isfinite(pg) && pg > 0.) prim[PPP] = pg;
+          cons2prim<Cfg, Hooks, true>(ph, cons, prim, &cs, par);
+          st.c2p_guesses++;
+        }
+      }
     }
-  }
-
-  // The starting pressure of one cons2prim with the learned guess: f at the
-  // warm start first; where it is within mlp::kGuessGate of E the warm start
-  // stays and its evaluation is handed to the search (returned pointer, into
-  // wbuf), elsewhere the network's pressure replaces it (nullptr).  Every lane
-  // of the warp calls (upd = false: no cell); the network runs only when a lane
-  // of the warp needs it.
-  __device__ static const C2PStart *guessed_start(const mlp::InferSmem &inf, const Phys &ph, const double *cons,
-                                                  double *prim, bool upd, StepStats &st, C2PStart &wbuf) {
-    bool need = false;
-    if (upd) {
-      const C2PInput in = c2p_input<Cfg>(cons, prim);
-      wbuf = c2p_start<Cfg>(ph, in.D, in.S, in.S2, in.E, in.pCand);
-      need = !(fabs(wbuf.f) <= mlp::kGuessGate * in.E);
-    }
-    if (__any_sync(0xffffffffu, need)) learned_guess(inf, cons, prim, need);
-    if (need) st.c2p_guesses++;
-    return need ? nullptr : &wbuf;
+    if (upd) count_c2p(st, cs, poor);
   }
 
   // --- one stage sweep ------------------------------------------------------
@@ -422,8 +418,6 @@ struct TrackStep {
         const long long g = off + i;
         double prim[NQ], cons[NQ];
         Geom G1;
-        C2PStats cs;
-        C2PStart wbuf;
         if (upd) {
 #pragma unroll
           for (int s = 0; s < NQS; ++s) prim[Slots<Cfg>::q_of(s)] = sm.cp[s][c];
@@ -468,11 +462,7 @@ struct TrackStep {
           }
         }
         // every lane of the warp meets here (the network works across it)
-        const C2PStart *w = GUESS ? guessed_start(*inf, ph, cons, prim, upd, st, wbuf) : nullptr;
-        if (upd) {
-          cons2prim<Cfg, Hooks>(ph, cons, prim, &cs, A.par, w);
-          count_c2p(st, cs);
-        }
+        cell_cons2prim(inf, ph, cons, prim, upd, st, A.par);
         if (stage > 1) {
           if (upd) {  // RK3 combine (rk3.cpp:27-55, 63-92)
 #pragma unroll
@@ -490,11 +480,7 @@ struct TrackStep {
               for (int q = 0; q < NQ; ++q) cons[q] = q <= TAU ? cons[q] / G2.dV : qdiv(cons[q], G2.dV);
             }
           }
-          const C2PStart *w2 = GUESS ? guessed_start(*inf, ph, cons, prim, upd, st, wbuf) : nullptr;
-          if (upd) {
-            cons2prim<Cfg, Hooks>(ph, cons, prim, &cs, A.par, w2);
-            count_c2p(st, cs);
-          }
+          cell_cons2prim(inf, ph, cons, prim, upd, st, A.par);
         }
         if (upd) {
           if (Cfg::SYNCH && stage == (ph.euler ? 1 : 3)) {  // radiation_injectParticles, active cells
@@ -649,10 +635,13 @@ struct TrackStep {
 
 // Dynamic shared memory: TrackStep::Smem, the regrid bit words (words_bytes),
 // then, with GUESS, the tensor-core weights of the learned guess.
+// gate (or nullptr): the launch returns at once unless *gate (k_guess_policy)
+// chose this kernel, the one with (nonzero) or without (0) the learned guess.
 template <class Cfg, class Hooks, int BS, bool GUESS = false, int CPT = 1, int MINB = Cfg::MIN_BLOCKS>
 __global__ void __launch_bounds__(BS, MINB)
     track_step_kernel(Tracks T, Phys ph, int nsteps, const int *order, int nruns, int *queue, StepStats *stats,
-                      int regrid_only, unsigned words_bytes) {
+                      int regrid_only, unsigned words_bytes, const int *gate) {
+  if (gate && ((*gate != 0) != GUESS)) return;
   using TS = TrackStep<Cfg, Hooks, BS, GUESS, CPT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typename TS::Smem &sm = *reinterpret_cast<typename TS::Smem *>(smem_raw);
@@ -685,6 +674,8 @@ __global__ void __launch_bounds__(BS, MINB)
   // fold the per-thread statistics into the launch totals
   __syncthreads();
   if (st.c2p_guesses) atomicAdd(&stats->c2p_guesses, st.c2p_guesses);
+  if (st.c2p_poor) atomicAdd(&stats->c2p_poor, st.c2p_poor);
+  if (GUESS && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&stats->learned, 1ull);
   if (st.c2p_calls) {
     atomicAdd(&stats->c2p_calls, st.c2p_calls);
     atomicAdd(&stats->c2p_iters, st.c2p_iters);

@@ -72,7 +72,8 @@ class StepStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_ulonglong) for n in ("c2p_calls", "c2p_iters", "c2p_fallbacks", "zone_updates",
                                                   "splits", "merges")] + \
                [("c2p_max_iters", ctypes.c_int), ("status", ctypes.c_int), ("device_ms", ctypes.c_float),
-                ("c2p_guesses", ctypes.c_ulonglong)]
+                ("c2p_guesses", ctypes.c_ulonglong), ("c2p_poor", ctypes.c_ulonglong),
+                ("learned_steps", ctypes.c_ulonglong)]
 
     def as_dict(self) -> dict:
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
@@ -228,6 +229,7 @@ class GammaGPU:
         if rc != GAMMA_OK:
             raise GammaError(rc)
         self.h = h
+        self._destroy = lib().gamma_gpu_destroy  # bound now: module globals may be gone when __del__ runs
         offs = np.zeros(self.nruns, dtype=np.int64)
         tot = ctypes.c_longlong()
         lib().gamma_gpu_layout(self.h, _p(offs, _lp), ctypes.byref(tot))
@@ -240,7 +242,7 @@ class GammaGPU:
 
     def close(self):
         if getattr(self, "h", None):
-            lib().gamma_gpu_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     def __del__(self):

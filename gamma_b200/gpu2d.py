@@ -127,6 +127,7 @@ class Grid2DGPU:
         if rc != gpu.GAMMA_OK:
             raise gpu.GammaError(rc)
         self.h = h
+        self._destroy = lib().gamma_2d_destroy  # bound now: module globals may be gone when __del__ runs
         nj, cap = ctypes.c_int(), ctypes.c_int()
         lib().gamma_2d_layout(self.h, ctypes.byref(nj), ctypes.byref(cap))
         self.NJ, self.cap = nj.value, cap.value
@@ -138,7 +139,7 @@ class Grid2DGPU:
 
     def close(self):
         if getattr(self, "h", None):
-            lib().gamma_2d_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -98,6 +98,9 @@ typedef struct {
   int status;                        /* 0 or the first failing run's GAMMA_ERR_* */
   float device_ms;                   /* device time of the step launch(es) */
   unsigned long long c2p_guesses;    /* calls started from the learned guess (gamma_gpu_set_guess) */
+  unsigned long long c2p_poor;       /* calls whose warm start was poor: the first Newton correction
+                                        from the previous pressure above 3% of it */
+  unsigned long long learned_steps;  /* steps that ran the step with the learned guess */
 } gamma_step_stats_t;
 
 typedef struct gamma_ctx gamma_ctx_t;
@@ -254,9 +257,16 @@ int gamma_mlp_forward(const float *params, const float *x, long long n, float *o
 int gamma_gpu_cons2prim_guess(const gamma_config_t *cfg, double *cons, double *prim, int n, int *iters,
                               const float *params, void *stream);
 
-/* Use the network's starting pressure in every cons2prim of gamma_gpu_step
- * (params: device pointer that stays valid while in use), or NULL for the
- * reference's warm start.  Merges during regrid keep the warm start. */
+/* Let cons2prim in gamma_gpu_step start from the network's pressure (params:
+ * device pointer that stays valid while in use), or NULL for the reference's
+ * warm start alone.  With a network set, a step call runs one of two step
+ * kernels, chosen on the device from the previous stepping call's statistics:
+ * the plain one where poor warm starts (c2p_poor) were at most a quarter of
+ * the cons2prim calls, else the one with the guess, in which the cells whose
+ * warm start is poor start from the network (c2p_guesses) and the others keep
+ * the warm start.  The first call after this one or after an upload takes the
+ * guess.  Merges during regrid keep the warm start.  Newton converges to the
+ * same tolerance from either start. */
 int gamma_gpu_set_guess(gamma_ctx_t *ctx, const float *params);
 
 /* ---- 2D runs (r, theta): NUM_D = 2, spherical, rel_sph, shock detection and
@@ -360,13 +370,15 @@ void *gamma_gpu_stream(gamma_ctx_t *ctx);
  * each thread takes per sweep chunk; variant 0 is the default (128 threads,
  * one cell).  Every variant computes every cell the same way, so results are
  * identical; only the speed depends on the batch (track lengths, run count).
- * The learned-guess step always uses variant 0. */
+ * The step with the learned guess (gamma_gpu_set_guess) has every variant too;
+ * the context's variant applies to whichever step runs. */
 int gamma_gpu_variant_info(int variant, int *threads, int *cells_per_thread);
 int gamma_gpu_set_variant(gamma_ctx_t *ctx, int variant);
 int gamma_gpu_get_variant(const gamma_ctx_t *ctx);
 
 /* Times nsteps launches of one step each with every variant on the context's
- * current state (ms[v], may be NULL), restores that state after each, and
+ * current state (ms[v], may be NULL; with a learned guess set, the step with
+ * the guess), restores that state after each, and
  * keeps the fastest (*chosen); another variant must beat variant 0 by 3%.
  * Allocates a copy of the state for the duration of the call. */
 int gamma_gpu_autotune(gamma_ctx_t *ctx, int nsteps, float *ms, int *chosen);

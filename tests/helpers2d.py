@@ -70,6 +70,20 @@ def l1_by_quantity(got, ref, qs=(0, 1, 2, 3, 4, 6, 7, 9), ngst=2):
     return out
 
 
+def l1_between_snapshots(a, b, qs, ngst=2):
+    """L1 of reference snapshot a against reference snapshot b (the same cell
+    counts), per quantity, over the active cells of the active tracks"""
+    out = {}
+    for q in qs:
+        num = den = 0.
+        for j in range(ngst, len(b.tracks) - ngst):
+            s = slice(ngst, b.tracks[j].ntrack - ngst)
+            num += np.sum(np.abs(a.tracks[j].prim[q][s] - b.tracks[j].prim[q][s]))
+            den += np.sum(np.abs(b.tracks[j].prim[q][s]))
+        out[q] = num / den if den > 0 else num
+    return out
+
+
 def cell_errors(got, ref, q, ngst=2):
     """relative errors of quantity q over the active cells: pressures against
     max(|p|, 1e-2 E), velocities with a floor of 1e-6 of their largest value"""

@@ -23,7 +23,8 @@ import numpy as np
 import pytest
 
 from conftest import ref_available
-from helpers2d import cell_errors, l1_by_quantity, params_of, state_from_reference, theta_of
+from helpers import record
+from helpers2d import cell_errors, l1_between_snapshots, l1_by_quantity, params_of, state_from_reference, theta_of
 
 pytestmark = pytest.mark.gpu
 
@@ -186,8 +187,15 @@ def test_2d_heavy_regrid_matches_reference(gpu_available):
     cold cell's pressure is a root of f(p) that is flat to within eps*E there,
     so the two root finders settle at different points of that band: 1e-10
     against 1.00000008e-10).  That difference then reaches the shock front, so
-    the steps after it are held to L1 <= 1e-7; restarting from the reference's
-    own post-regrid state brings one step back to L1 ~2e-11 (pressure)."""
+    the steps after it are held to L1 <= 1e-7 (1e-6 for the synchrotron
+    tracers, which are re-injected wherever the shock detector fires); measured
+    9.4e-9 (rho), 2.3e-8 (p), 1.6e-8 (u_r) after one step.  The reference's own
+    movement when only its root finder's tolerance changes (1e-15 against
+    4e-16) is recorded beside each figure: ~1e-12, because Brent from the same
+    bracket stops at the same point of the band at any tight tolerance, so it
+    does not measure which point of the band a second root finder stops at.
+    Restarting from the reference's own post-regrid state brings one step back
+    to L1 ~2e-11 (pressure)."""
     if not ref_available("jet2d"):
         pytest.skip("oracle/_ref/libref_jet2d.so not built")
     from oracle.refsim2d import run_isolated
@@ -218,6 +226,7 @@ def test_2d_heavy_regrid_matches_reference(gpu_available):
     g.close()
     # then whole steps
     snaps = run_isolated(p, snap_at=(0, 1, 4), c2p_epsrel=EPS_CONVERGED)
+    alt = run_isolated(p, snap_at=(0, 1, 4), c2p_epsrel=1e-15)
     g = gpu2d.Grid2DGPU(len(th), p["nmax"], th, dth)
     g.set_params(params_of(p, d))
     g.upload(state_from_reference(snaps[0]))
@@ -226,9 +235,11 @@ def test_2d_heavy_regrid_matches_reference(gpu_available):
         got = g.download()
         assert st["status"] == 0
         assert _same_counts(got, snaps[k])
-        l1 = l1_by_quantity(got, snaps[k], qs=(0, 1, 2, 4, 6, 7))
-        # the synchrotron tracers are re-injected wherever the shock detector
-        # fires, so they inherit the hydro differences near its threshold
-        assert all(l1[q] <= 1e-7 for q in (0, 1, 2, 4)), (k, l1)
-        assert all(l1[q] <= 1e-6 for q in (6, 7)), (k, l1)
+        qs = (0, 1, 2, 4, 6, 7)
+        bar = {q: 1e-6 if q in (6, 7) else 1e-7 for q in qs}
+        l1 = l1_by_quantity(got, snaps[k], qs=qs)
+        self_l1 = l1_between_snapshots(alt[k], snaps[k], qs)
+        for q in qs:
+            record(f"step {k} L1 slot {q} (reference tolerance sensitivity {self_l1[q]:.2e})", l1[q], bar[q])
+        assert all(l1[q] <= bar[q] for q in qs), (k, l1, self_l1)
     g.close()

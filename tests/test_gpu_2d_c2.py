@@ -47,7 +47,7 @@ import pytest
 
 from conftest import ref_available
 from helpers import record
-from helpers2d import cell_errors, l1_by_quantity, params_of, state_from_reference, theta_of
+from helpers2d import cell_errors, l1_between_snapshots, l1_by_quantity, params_of, state_from_reference, theta_of
 
 pytestmark = pytest.mark.gpu
 
@@ -108,19 +108,6 @@ def _counts(got, ref):
     return [int(got.ntrack[j]) for j in range(len(ref.tracks))] == [t.ntrack for t in ref.tracks]
 
 
-def _l1_ref(a, b, qs):
-    """L1 of reference snapshot a against reference snapshot b"""
-    out = {}
-    for q in qs:
-        num = den = 0.
-        for j in range(2, len(b.tracks) - 2):
-            s = slice(2, b.tracks[j].ntrack - 2)
-            num += np.sum(np.abs(a.tracks[j].prim[q][s] - b.tracks[j].prim[q][s]))
-            den += np.sum(np.abs(b.tracks[j].prim[q][s]))
-        out[q] = num / den if den > 0 else num
-    return out
-
-
 def test_c2_wedge_settles_at_the_workload_resolution(refs):
     (r, _), _, _, _ = refs
     n = [t.ntrack - 4 for t in r[2].tracks[2:-2]]
@@ -151,7 +138,7 @@ def test_c2_wedge_200_steps(gpu_available, refs):
     assert _counts(got, ref)
     assert abs(got.t - ref.t) <= 1e-11 * ref.t
     l1 = l1_by_quantity(got, ref, qs=HYDRO + TRACERS)
-    self_l1 = _l1_ref(alt[202], ref, HYDRO + TRACERS)
+    self_l1 = l1_between_snapshots(alt[202], ref, HYDRO + TRACERS)
     for q in HYDRO + TRACERS:
         record(f"L1 slot {q} (reference self-sensitivity {self_l1[q]:.2e})", l1[q], max(1e-8, 3 * self_l1[q]))
     assert all(l1[q] <= max(1e-8, 3 * self_l1[q]) for q in HYDRO + TRACERS), (l1, self_l1)
@@ -178,7 +165,7 @@ def test_2d_wedge_1000_steps(gpu_available, refs):
         if not _counts(got, r[k]):
             break
         l1 = l1_by_quantity(got, r[k], qs=HYDRO + TRACERS)
-        self_l1 = _l1_ref(alt[k], r[k], HYDRO + TRACERS)
+        self_l1 = l1_between_snapshots(alt[k], r[k], HYDRO + TRACERS)
         worst = max(l1[q] / max(1e-8, 10 * self_l1[q]) for q in HYDRO + TRACERS)
         record(f"step {k}: max over slots of L1 / max(1e-8, 10 x reference self-sensitivity)", worst, 1.)
         assert worst <= 1., (k, l1, self_l1)

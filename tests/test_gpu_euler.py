@@ -16,8 +16,8 @@ import numpy as np
 import pytest
 
 from conftest import ref_available
-from helpers import l1_rel
-from helpers2d import l1_by_quantity, params_of, state_from_reference, theta_of
+from helpers import l1_rel, record
+from helpers2d import l1_between_snapshots, l1_by_quantity, params_of, state_from_reference, theta_of
 
 pytestmark = pytest.mark.gpu
 
@@ -140,13 +140,18 @@ def test_euler_2d_matches_reference(gpu_available):
     comes out of a cancellation in tau) grows them step by step.  The reference
     itself, compiled with FMA contraction, differs from its plain build by L1 ~1e-4
     in density after 30 steps.  The bars are L1 <= 3e-8 (1e-6 for u_theta, ~0
-    away from the jet edge; measured 7.9e-9 in density and 3.8e-7 in u_theta)
-    with identical cell counts and t within 1e-10."""
+    away from the jet edge), with identical cell counts and t within 1e-10;
+    measured 7.9e-9 (rho), 1.1e-8 (p), 5.5e-9 (u_r), 3.8e-7 (u_theta),
+    1.6e-8 (gamma_min tracer).  The reference's movement when only its root
+    finder's tolerance changes (1e-15 against 4e-16) is recorded beside each
+    figure (2.9e-9 in rho, 1e-10 in u_theta): it does not measure which point
+    of the cold cells' flat f(p) band a second root finder stops at."""
     if not ref_available("jet2d_euler"):
         pytest.skip("oracle/_ref/libref_jet2d_euler.so not built")
     from gamma_b200 import gpu, gpu2d
     from oracle.refsim2d import run_isolated
     snaps = run_isolated(CFG2, snap_at=(0, 1, 2, 4, 5, 30), c2p_epsrel=4e-16, euler=True)
+    alt = run_isolated(CFG2, snap_at=(30,), c2p_epsrel=1e-15, euler=True)
     with mp.get_context("spawn").Pool(1) as pool:
         d = pool.apply(_derived, (CFG2,))
     th, dth = theta_of(snaps[0])
@@ -179,4 +184,8 @@ def test_euler_2d_matches_reference(gpu_available):
     got, ref = run(0, 30)
     assert abs(got.t - ref.t) <= 1e-10 * ref.t
     l1 = l1_by_quantity(got, ref)
-    assert all(v <= (1e-6 if q == 3 else 3e-8) for q, v in l1.items()), l1
+    self_l1 = l1_between_snapshots(alt[30], ref, tuple(l1))
+    bar = {q: 1e-6 if q == 3 else 3e-8 for q in l1}
+    for q, v in l1.items():
+        record(f"30 steps L1 slot {q} (reference tolerance sensitivity {self_l1[q]:.2e})", v, bar[q])
+    assert all(v <= bar[q] for q, v in l1.items()), (l1, self_l1)

@@ -271,6 +271,7 @@ def test_step_with_guess_matches_plain_step(trained):
             g.set_guess(P.data_ptr())
         st = g.step(50)
         assert st["status"] == 0 and st["c2p_fallbacks"] == 0
+        assert (st["c2p_guesses"] > 0) == use  # the first steps' shock cells start from the network
         outs.append([problems.unpack(g.download(), r, g.offsets) for r in range(len(setups))])
         stats.append(st)
         g.close()
@@ -283,6 +284,85 @@ def test_step_with_guess_matches_plain_step(trained):
         for q in (0, 1, 2, 4):
             assert l1_rel(b.prim[q, s], a.prim[q, s]) <= 1e-10, q
         assert l1_rel(b.xI, a.xI) <= 1e-10
+
+
+def test_step_with_guess_same_bits_in_every_launch_shape(trained):
+    """The step with the learned guess exists in every launch shape, chosen
+    before or after the guess is set; every shape gives the same bits, and the
+    autotuner times the step with the guess and puts the state back."""
+    from gamma_b200 import gpu, problems
+    P, _ = trained
+    setups = [problems.TubeSetup(ncell=n, vL=v, vR=v, rhoL=r) for n, v, r in
+              ((300, 0.1, 10.0), (777, -0.3, 9.5), (1500, 0.45, 10.5))]
+    outs = []
+    for v in range(gpu.N_VARIANTS):
+        g = gpu.GammaGPU(gpu.config_cart(), [s.capacity for s in setups])
+        pk = problems.pack([s.initial_state() for s in setups], g.offsets, g.total, 6)
+        g.upload(pk["ntrack"], pk["prim"], pk["x"], pk["dx"], pk["xI"], pk["dt_loc"], pk["t"], pk["it"])
+        if v % 2:
+            g.set_variant(v)
+            g.set_guess(P.data_ptr())
+        else:
+            g.set_guess(P.data_ptr())
+            g.set_variant(v)
+        st = g.step(20)
+        assert st["status"] == 0 and st["c2p_guesses"] > 0 and g.variant == v
+        outs.append((g.download(), st["zone_updates"], st["c2p_guesses"]))
+        if v == 0:
+            before = g.download()
+            ms, chosen = g.autotune(2)
+            after = g.download()
+            assert g.variant == chosen and all(m > 0 for m in ms)
+            for k in ("ntrack", "t", "prim", "x", "xI", "dt_loc"):
+                assert np.array_equal(before[k], after[k]), k
+        offsets = g.offsets
+        g.close()
+    a = outs[0]
+    for b in outs[1:]:
+        assert b[1] == a[1] and b[2] == a[2]
+        assert np.array_equal(a[0]["ntrack"], b[0]["ntrack"])
+        for o, n in zip(offsets, a[0]["ntrack"]):
+            assert np.array_equal(a[0]["prim"][:, o:o + n], b[0]["prim"][:, o:o + n])
+            assert np.array_equal(a[0]["xI"][o:o + n - 1], b[0]["xI"][o:o + n - 1])
+
+
+def test_guess_policy_follows_poor_warm_starts(trained):
+    """With a network set, the first step call after the upload runs the step
+    with the guess; the calls after it run the plain step kernel while poor warm
+    starts stay below a quarter of the cons2prim calls (the tubes' are a few per
+    thousand), with the plain kernel's bits; an upload starts over with the
+    guess."""
+    from gamma_b200 import gpu, problems
+    P, _ = trained
+    setups = [problems.TubeSetup(ncell=n, vL=v, vR=v, rhoL=r) for n, v, r in
+              ((300, 0.1, 10.0), (777, -0.3, 9.5), (1500, 0.45, 10.5))]
+    outs = []
+    for keep in (True, False):
+        g = gpu.GammaGPU(gpu.config_cart(), [s.capacity for s in setups])
+        pk = problems.pack([s.initial_state() for s in setups], g.offsets, g.total, 6)
+
+        def upload():
+            g.upload(pk["ntrack"], pk["prim"], pk["x"], pk["dx"], pk["xI"], pk["dt_loc"], pk["t"], pk["it"])
+
+        upload()
+        g.set_guess(P.data_ptr())
+        s1 = g.step(1)
+        assert s1["learned_steps"] == 1 and s1["c2p_guesses"] > 0
+        assert 0 < s1["c2p_poor"] < 0.25 * s1["c2p_calls"]
+        if not keep:
+            g.set_guess(0)  # the plain step kernel by hand
+        s2 = g.step(5)
+        assert s2["status"] == 0 and s2["learned_steps"] == 0 and s2["c2p_guesses"] == 0
+        outs.append(g.download())
+        if keep:
+            upload()
+            assert g.step(1)["learned_steps"] == 1
+        g.close()
+    a, b = outs
+    assert np.array_equal(a["ntrack"], b["ntrack"]) and np.array_equal(a["t"], b["t"])
+    for o, n in zip(g.offsets, a["ntrack"]):
+        assert np.array_equal(a["prim"][:, o:o + n], b["prim"][:, o:o + n])
+        assert np.array_equal(a["xI"][o:o + n - 1], b["xI"][o:o + n - 1])
 
 
 def test_bm1d_step_with_guess_matches_plain_step(trained):
