@@ -861,14 +861,16 @@ template <class Cfg>
 GB_HD void inject_particles(const Phys &ph, const SynchConst &sc, double *prim, bool shocked, double pspec) {
   double lfac = lfac_of(prim[UU1]);
   double rho = prim[RHO];
-  double lim = lfac * pow(rho, 4. / 3.) / (lfac * rho);
   if (shocked) {
     if (pspec > prim[PSN] || isnan(prim[PSN])) prim[PSN] = pspec;
     prim[GMX] = gammae2trac<Cfg>(GAMMA_MAX_INIT, prim) / (lfac * rho);
     prim[GMN] = gammae2trac<Cfg>(gamma_min_init<Cfg>(ph, sc, prim), prim) / (lfac * rho);
   }
-  if (isnan(prim[GMX])) prim[GMX] = lim;
-  if (isnan(prim[GMN])) prim[GMN] = lim;
+  if (isnan(prim[GMX]) || isnan(prim[GMN])) {  // lim only where it is used
+    const double lim = lfac * pow(rho, 4. / 3.) / (lfac * rho);
+    if (isnan(prim[GMX])) prim[GMX] = lim;
+    if (isnan(prim[GMN])) prim[GMN] = lim;
+  }
 }
 
 // Cell::radiativeSourceTerms: returns the increment of cons[GMX] and cons[GMN]

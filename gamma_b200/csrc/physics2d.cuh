@@ -437,14 +437,16 @@ GB_HD double gammae2trac(double gme, const double *prim) {
 GB_HD void inject_particles(const Phys &ph, const SynchConst &sc, double *prim, bool shocked, double pspec) {
   double lf = lfac(prim);
   double rho = prim[RHO];
-  double lim = lf * pow(rho, 4. / 3.) / (lf * rho);
   if (shocked) {
     if (pspec > prim[PSN] || isnan(prim[PSN])) prim[PSN] = pspec;
     prim[GMX] = gammae2trac(GAMMA_MAX_INIT, prim) / (lf * rho);
     prim[GMN] = gammae2trac(gamma_min_init<Cfg2>(ph, sc, prim), prim) / (lf * rho);
   }
-  if (isnan(prim[GMX])) prim[GMX] = lim;
-  if (isnan(prim[GMN])) prim[GMN] = lim;
+  if (isnan(prim[GMX]) || isnan(prim[GMN])) {  // lim only where it is used
+    const double lim = lf * pow(rho, 4. / 3.) / (lf * rho);
+    if (isnan(prim[GMX])) prim[GMX] = lim;
+    if (isnan(prim[GMN])) prim[GMN] = lim;
+  }
 }
 
 }  // namespace d2
