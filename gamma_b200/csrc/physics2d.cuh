@@ -211,32 +211,41 @@ GB_HD void hllc_flux(const St &L, const St &R, const Waves &w, double v, double 
 
 // compute_Sd (radiation_sph.cpp:41-158) along dim, S1 upstream.  Returns false
 // where the reference returns -1 before reaching the spectral index.
-GB_HD bool compute_Sd(const Phys &ph, const St &S1, const St &S2, int dim, bool reverse, double *Sd) {
+// What compute_Sd reads of one side along dim: pressure, density, the
+// 4-velocity along dim (ux) and across it (ut), the Lorentz factor.
+struct SdSide {
+  double p, rho, ux, ut, lfac;
+};
+
+GB_HD SdSide sd_side(const St &S, int dim) {
+  return SdSide{S.prim[PPP], S.prim[RHO], S.prim[UU1 + dim], S.prim[UU2 - dim], S.lfac};
+}
+
+GB_HD bool compute_Sd(const Phys &ph, const SdSide &S1, const SdSide &S2, bool reverse, double *Sd) {
   // with eos_ws, the upstream state's Gamma_eff throughout
-  const double G = ph.eos_ws ? eos_gamma(ph, S1.prim[RHO], S1.prim[PPP]) : ph.gamma_ad;
-  const int uux = UU1 + dim, uut = UU2 - dim;
+  const double G = ph.eos_ws ? eos_gamma(ph, S1.rho, S1.p) : ph.gamma_ad;
   const int n_evals = 10;
   const double chi = 0.5;
-  double p1 = S1.prim[PPP];
-  double p2 = S2.prim[PPP];
+  double p1 = S1.p;
+  double p2 = S2.p;
   if (fabs(qdiv(p1 - p2, p1)) < 1.e-10 || p1 < p2) {
     *Sd = -1;
     return false;
   }
   double delta_p = p2 - p1;
   double dp = delta_p / (double)n_evals;
-  double rho1 = S1.prim[RHO];
-  double rho2 = S2.prim[RHO];
+  double rho1 = S1.rho;
+  double rho2 = S2.rho;
   double h1 = 1 + p1 * G / (G - 1.) / rho1;
   double h2 = 1 + p2 * G / (G - 1.) / rho2;
   double lfac2 = S2.lfac;
-  double vx1 = qdiv(S1.prim[uux], S1.lfac);
-  double vx2 = qdiv(S2.prim[uux], lfac2);
+  double vx1 = qdiv(S1.ux, S1.lfac);
+  double vx2 = qdiv(S2.ux, lfac2);
   if (reverse) {
     vx1 *= -1;
     vx2 *= -1;
   }
-  double ut1 = S1.prim[uut];
+  double ut1 = S1.ut;
   double v12 = qdiv(vx1 - vx2, 1 - vx1 * vx2);
   double A1 = h1 * ut1;
   double I = 0;

@@ -249,7 +249,7 @@ GB_HD void mv_interface(const Phys &ph, const Params2 &P, const Grid2 &G, int j,
   for (int q = 0; q < NQ; ++q) G.flx[q * G.NC + g] = fl[q];
   // measureShock, moving direction: forward shocks only, into the left cell
   double Sd;
-  if (compute_Sd(ph, L, R, MV, false, &Sd)) {
+  if (compute_Sd(ph, sd_side(L, MV), sd_side(R, MV), false, &Sd)) {
     if (P_SPEC > G.pspec[g]) G.pspec[g] = P_SPEC;
   }
   G.sd[g] = fmax(G.sd[g], Sd);
@@ -457,8 +457,22 @@ GB_HD void f1_interface(const Phys &ph, const Grid2 &G, int j, long long g0, lon
   }
   const Waves wv = compute_lambda(ph, L, R, F1, xm);
   hllc_flux(L, R, wv, 0., dA, F1, xm, out.flux);
-  out.have_fwd = compute_Sd(ph, L, R, F1, false, &out.sd_fwd);
-  out.have_rev = compute_Sd(ph, R, L, F1, true, &out.sd_rev);
+  // measureShock across the tracks (radiation_sph.cpp:160-175): the forward
+  // test (L upstream) and the reverse one (R upstream).  compute_Sd passes its
+  // pressure test only where the upstream pressure is the larger, so at most
+  // one of the two evaluates the isentrope integral: one call, with the
+  // upstream side chosen per lane, gives both results and runs the integral
+  // once per warp instead of twice.  Where a pressure is NaN both tests pass
+  // and both results are NaN, which the one call also gives.
+  const SdSide sL = sd_side(L, F1), sR = sd_side(R, F1);
+  const bool fw = sL.p > sR.p;
+  const bool nan_p = isnan(sL.p) || isnan(sR.p);
+  double sd;
+  const bool have = compute_Sd(ph, fw ? sL : sR, fw ? sR : sL, !fw, &sd);
+  out.have_fwd = (fw || nan_p) && have;
+  out.sd_fwd = (fw || nan_p) ? sd : -1.;
+  out.have_rev = !fw && have;
+  out.sd_rev = fw ? -1. : sd;
 }
 
 // c0's side: flux[1][F1] and forward shocks, over c0's upper neighbours in order

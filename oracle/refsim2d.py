@@ -63,11 +63,13 @@ class RefJet2D:
     (libref_jet2d_io.so): printCols then writes ../results/Last/phys*.out
     relative to the working directory, and resume() reads it back."""
 
-    def __init__(self, io: bool = False, euler: bool = False):
-        assert not (io and euler)
+    def __init__(self, io: bool = False, euler: bool = False, synge: bool = False):
+        assert io + euler + synge <= 1
         path = LIB.replace("libref_jet2d.so", "libref_jet2d_io.so") if io else LIB
         if euler:
             path = LIB.replace("libref_jet2d.so", "libref_jet2d_euler.so")
+        if synge:  # EOS_ = SYNGE_EOS_, GAMMA_ = 5/3
+            path = LIB.replace("libref_jet2d.so", "libref_jet2d_synge.so")
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
         lib = ctypes.CDLL(path, mode=os.RTLD_LOCAL)
@@ -166,8 +168,8 @@ class RefJet2D:
 
 
 def _worker(args):
-    params, snap_at, nsteps, epsrel, euler = args
-    sim = RefJet2D(euler=euler)
+    params, snap_at, nsteps, epsrel, euler, synge = args
+    sim = RefJet2D(euler=euler, synge=synge)
     sim.set_params(**params)
     sim.init()
     if epsrel:
@@ -184,12 +186,14 @@ def _worker(args):
     return out
 
 
-def run_isolated(params: dict, snap_at=(0,), nsteps: int = 0, c2p_epsrel: float = 0., euler: bool = False):
+def run_isolated(params: dict, snap_at=(0,), nsteps: int = 0, c2p_epsrel: float = 0., euler: bool = False,
+                 synge: bool = False):
     """Run one configuration in a fresh spawned process; returns {step: Grid2D}.
     c2p_epsrel > 0 replaces the reference's cons2prim stopping tolerance after
-    the initial state is built.  euler: the build with Timestep/euler.cpp."""
+    the initial state is built.  euler: the build with Timestep/euler.cpp;
+    synge: the build with the Synge EOS and GAMMA_ = 5/3."""
     import multiprocessing as mp
 
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
-        return pool.apply(_worker, ((params, tuple(snap_at), nsteps, c2p_epsrel, euler),))
+        return pool.apply(_worker, ((params, tuple(snap_at), nsteps, c2p_epsrel, euler, synge),))

@@ -20,6 +20,18 @@ def energy_scale(prim, gamma_ad):
     return rho * lfac * h * lfac - p
 
 
+EPS = 2.220446049250313e-16
+# f(p) = E + p - D lfac - k p lfac^2 is rounded to a few ulp of E, so where p
+# is far below E (cold gas) any root finder leaves p uncertain by ~eps * E:
+# pressures are held to max(rtol |p|, P_EPS_E * eps * E)
+P_EPS_E = 16.0
+
+
+def pressure_scale(p, E, rtol):
+    """The scale s with |dp| <= rtol * s  <=>  |dp| <= max(rtol |p|, P_EPS_E eps E)."""
+    return np.maximum(np.abs(p), P_EPS_E * EPS * np.abs(E) / rtol)
+
+
 def rel_err(a, b, floor):
     """max |a-b| / max(|b|, floor)"""
     d = np.abs(a - b) / np.maximum(np.abs(b), floor)
@@ -76,14 +88,15 @@ def solver_sensitivity(run, eps_list=(1e-13, 1e-14, 1e-15), converged=1e-16):
 def within_sensitivity(got, ref, sens, gamma_ad, rtol=1e-12, k=4.0, qs=(0, 1, 2)):
     """Per-cell check |got - ref| <= rtol * scale + k * sensitivity.
 
-    scale is |ref| (pressure: max(|p|, 1e-2 E)).  Returns the worst ratio
+    scale is |ref| (pressure: pressure_scale, i.e. rtol * scale is at least
+    P_EPS_E eps E).  Returns the worst ratio
     |got - ref| / bound per field (<= 1 passes) and the fraction of cells that
     are within rtol alone."""
     E = energy_scale(ref.prim, gamma_ad)
     worst, frac = {}, {}
     for q in qs:
         b = ref.prim[q]
-        scale = np.maximum(np.abs(b), 1e-2 * np.abs(E)) if q == 1 else np.abs(b)
+        scale = pressure_scale(b, E, rtol) if q == 1 else np.abs(b)
         if q >= 2:
             # velocities and tracers vanish in parts of a track: below 1e-4 of
             # the field's largest magnitude (or of one for a track at rest)
