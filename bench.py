@@ -211,6 +211,9 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+# kernel launches of one 2D step (gamma_2d.cu enqueue_step_until): 4 regrid,
+# 14 per RK3 stage, collect_dt's 2 in stage 1, the advance
+LAUNCHES_2D = 4 + 3 * 14 + 2 + 1
 JET2D = dict(ntheta=512, ncell=12000, nmax=12000)  # tracks settle at ~3,000-4,000 cells after the first regrid
 # the sweep workload's large 2D case: slow cells merge only below 0.3 of the
 # target spacing, so the tracks keep ~8,000 cells (~33 M zones)
@@ -350,18 +353,18 @@ def jet2d_arm(args, dev_index, host_work=True):
            "zones_per_step": zones / args.steps, "cells_per_track": [int(n.min()), int(n.max())],
            "c2p": {"mean_newton_iters": st["c2p_iters"] / max(st["c2p_calls"], 1),
                    "max_newton_iters": st["c2p_max_iters"], "fallbacks": st["c2p_fallbacks"]},
-           "clocks": clk, "gpu_launches": 43 * args.steps}
+           "clocks": clk, "gpu_launches": LAUNCHES_2D * args.steps}
     peak, peak_kind = measured_peak_hbm()
     achieved = B_ZU_NQ10 * zones / (ms / 1e3) / 1e9
     res["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                        "peak_source": peak_kind, "bytes_per_zone_update": B_ZU_NQ10,
-                       "note": "whole step (43 launches); per-kernel shares in the ncu launch list"}
+                       "note": f"whole step ({LAUNCHES_2D} launches); per-kernel shares in the ncu launch list"}
     # the plain form: the same step with its kernels launched one by one (no
     # graph) and the reference's warm start, from the same initial state
     ms_p, st_p, out_p, _ = _jet2d_run(s, args.steps, args.warmup, 0, graphs=False)
     res["plain"] = {"value": st_p["zone_updates"] / (ms_p / 1e3), "ms_per_step": ms_p / args.steps,
                     "same_cell_counts": bool(np.array_equal(out_p.ntrack, out.ntrack)),
-                    "note": "43 kernel launches per step from the host, no CUDA graph, warm start"}
+                    "note": f"{LAUNCHES_2D} kernel launches per step from the host, no CUDA graph, warm start"}
     res["batched_over_plain"] = res["value"] / res["plain"]["value"]
     if not args.no_learned:
         # training states: the run's active cells, as 1D states of the same |u| (cons2prim sees |S| only)
@@ -451,7 +454,7 @@ def jet2d_c4_arm(args, dev_index):
             "device_state_gb": (free0 - mem[0]) / 1e9 if mem else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "bytes_per_zone_update": B_ZU_NQ10},
-            "clocks": clk, "gpu_launches": 43 * args.steps}
+            "clocks": clk, "gpu_launches": LAUNCHES_2D * args.steps}
 
 
 def summary_of(line):

@@ -227,8 +227,80 @@ __global__ void __launch_bounds__(kThreads, GB2_MINB_TG) k_tgrad(Grid2 G) {
   FOR_LIVE_CELLS(G, j, i) trans_grad(G, j, i);
 }
 
-__global__ void __launch_bounds__(kThreads, GB2_MINB_F1) k_f1own(Phys ph, Grid2 G) {
-  FOR_LIVE_CELLS(G, j, i) f1_own(ph, G, j, i);
+// The theta interfaces of track j (one block per track, j <= NJ-2), numbered
+// in cell order: a cell's first interface (if_off) is the upper-list length
+// of the cells before it; if_own names the owner of each; if_tot counts them.
+__global__ void k_if_scan(Grid2 G) {
+  __shared__ int part[kThreads];
+  const int j = blockIdx.x, n = G.ntrack[j];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int chunk = (n + nt - 1) / nt;
+  const int i0 = min(n, t * chunk), i1 = min(n, i0 + chunk);
+  const long long o = (long long)j * G.cap;
+  int sum = 0;
+  for (int i = i0; i < i1; ++i) sum += max(G.nbr[3 * G.NC + o + i], 0);
+  part[t] = sum;
+  __syncthreads();
+  for (int off = 1; off < nt; off <<= 1) {  // inclusive scan
+    const int v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  const long long IC = if_cap(G), base = (long long)j * IC;
+  int run = part[t] - sum;
+  for (int i = i0; i < i1; ++i) {
+    const int cnt = max(G.nbr[3 * G.NC + o + i], 0);
+    G.if_off[o + i] = run;
+    for (int k = 0; k < cnt; ++k)
+      if (run + k < IC) G.if_own[base + run + k] = i;
+    run += cnt;
+  }
+  if (t == nt - 1) {
+    const int tot = part[t];
+    if (tot > IC) *G.status = 41;
+    G.if_tot[j] = tot > IC ? (int)IC : tot;
+  }
+}
+
+// if_pref: the interfaces of the tracks before j (track NJ-1 owns none)
+__global__ void k_if_pref(Grid2 G) {
+  __shared__ int part[1024];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int chunk = (G.NJ + nt - 1) / nt;
+  const int j0 = t * chunk, j1 = min(G.NJ, j0 + chunk);
+  auto tot = [&](int j) { return j <= G.NJ - 2 ? G.if_tot[j] : 0; };
+  int sum = 0;
+  for (int j = j0; j < j1; ++j) sum += tot(j);
+  part[t] = sum;
+  __syncthreads();
+  for (int off = 1; off < nt; off <<= 1) {
+    const int v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - sum;
+  for (int j = j0; j < j1; ++j) {
+    G.if_pref[j] = run;
+    run += tot(j);
+  }
+  if (t == nt - 1) G.if_pref[G.NJ] = part[t];
+}
+
+// every theta interface, one per thread (f1_if)
+__global__ void __launch_bounds__(kThreads, GB2_MINB_F1) k_f1if(Phys ph, Grid2 G) {
+  const long long n = G.if_pref[G.NJ];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = G.NJ - 1;  // last track with if_pref[track] <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (G.if_pref[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    f1_if(ph, G, lo, (int)(t - G.if_pref[lo]));
+  }
 }
 
 __global__ void __launch_bounds__(kThreads, GB2_MINB_GA) k_f1gather(Phys ph, Grid2 G) {
@@ -431,7 +503,9 @@ int enqueue_step_until(gamma_2d *c, int upto) {
     k_stale_clear<<<(c->NJ + 255) / 256, 256, 0, s>>>(G);
     k_stale<<<(c->NJ + 127) / 128, 128, 0, s>>>(G);
     k_tgrad<<<nb, kThreads, 0, s>>>(G);
-    k_f1own<<<nb, kThreads, 0, s>>>(ph, G);
+    k_if_scan<<<c->NJ - 1, kThreads, 0, s>>>(G);
+    k_if_pref<<<1, 1024, 0, s>>>(G);
+    k_f1if<<<nb, kThreads, 0, s>>>(ph, G);
     k_f1gather<<<nb, kThreads, 0, s>>>(ph, G);
     if (stage == upto) {
       G2_CUDA(c, cudaGetLastError());
@@ -565,7 +639,12 @@ GAMMA_API int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta,
   G2_ALLOC(G.status, sizeof(int));
   G2_ALLOC(G.red, (size_t)blocks_of(NC) * d);
   G2_ALLOC(G.pref, ((size_t)c->NJ + 1) * sizeof(int));
-  G2_ALLOC(G.seg, (size_t)SEG_WORDS * KSEG * NC * d);
+  const size_t IS = (size_t)c->NJ * (size_t)if_cap(G);
+  G2_ALLOC(G.ifs, (size_t)IF_WORDS * IS * d);
+  G2_ALLOC(G.if_off, NC * sizeof(int));
+  G2_ALLOC(G.if_own, IS * sizeof(int));
+  G2_ALLOC(G.if_tot, c->NJ * sizeof(int));
+  G2_ALLOC(G.if_pref, ((size_t)c->NJ + 1) * sizeof(int));
   G2_ALLOC(G.rprim, q * NC * d);
   G2_ALLOC(G.rgmv, q * NC * d);
   G2_ALLOC(G.rgf1, q * NC * d);

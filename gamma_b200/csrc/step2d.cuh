@@ -13,7 +13,7 @@
 //                       computeFlux + measureShock (2d.cpp:436-470, 735-767)
 //     cell_mv           update_dt(MV) and computeNeighbors (2d.cpp:534-606, 769-777)
 //     trans_grad        computeTransGradients (2d.cpp:366-430)
-//     f1_own/f1_gather  the theta-direction fluxes between tracks (2d.cpp:779-839)
+//     f1_if/f1_gather   the theta-direction fluxes between tracks (2d.cpp:779-839)
 //     [stage 1: dt = CFL min dt_loc, detectShock]
 //     iface_move, update_cell   Grid::update + the RK3 combines (2d.cpp:861-882,
 //                       rk3.cpp:98-194)
@@ -38,8 +38,9 @@ namespace gb {
 namespace d2 {
 
 constexpr int KMAX_STALE = 8;  // foreign stale contributors per target track
-constexpr int KSEG = 4;        // theta interfaces kept per cell for the gather (longer lists recompute)
-constexpr int SEG_WORDS = NQ + 2;  // flux[NQ], reverse Sd, flags (1: forward computed, 2: reverse)
+// a theta interface's results: flux[NQ], forward Sd, reverse Sd, flags (1: the
+// forward test reached the spectral index, 2: the reverse one)
+constexpr int IF_WORDS = NQ + 3;
 
 // Problem hooks of the theta-wedge blast wave (src/Initial/Tests/BM.cpp)
 struct Params2 {
@@ -73,10 +74,17 @@ struct Grid2 {
   // run scalars
   double *t, *dt;
   long long *it;
-  int *status;               // 30: negative CFL candidate; 40: stale table overflow
+  int *status;               // 30: negative CFL candidate; 40: stale table overflow;
+                             // 41: a track's theta interfaces exceed if_cap
   double *red;               // partial minima of dt_loc
   int *pref;                 // [NJ+1] cells of tracks before j (the live-cell index)
-  double *seg;               // [SEG_WORDS][KSEG * NC]: theta interfaces of each cell's upper list
+  // theta interfaces, owned by the cells of track j (j <= NJ-2) through their
+  // upper lists, numbered per track in cell order (k_if_scan):
+  double *ifs;               // [IF_WORDS][NJ * if_cap]: interface results, track j from j * if_cap
+  int *if_off;               // [NC]: a cell's first interface within its track
+  int *if_own;               // [NJ * if_cap]: the owning cell (index in its track) of each interface
+  int *if_tot;               // [NJ]: interfaces of each track
+  int *if_pref;              // [NJ+1]: interfaces of the tracks before j
   // regrid scratch (one track of records per track)
   double *rprim, *rgmv, *rgf1;  // [NQ][NC]
   double *rx, *rdx, *rdtl, *rxI;
@@ -86,6 +94,11 @@ struct Grid2 {
   int *rnbr2;                // [4][NC]
   unsigned long long *stats;  // c2p calls, c2p iters, fallbacks, zone updates, splits, merges, max iters
 };
+
+// interfaces one track may own: its upper lists overlap the next track's
+// cells in sorted order, so they hold at most ntrack[j] + ntrack[j+1] entries;
+// the margin covers the copied lists of the edge cells
+__host__ __device__ inline long long if_cap(const Grid2 &G) { return 2LL * G.cap + 64; }
 
 GB_HD int iL_of(const Grid2 &G) { return G.ngst - 1; }
 GB_HD int jL_of(const Grid2 &G) { return G.ngst - 1; }
@@ -475,34 +488,22 @@ GB_HD void f1_interface(const Phys &ph, const Grid2 &G, int j, long long g0, lon
   out.sd_rev = fw ? -1. : sd;
 }
 
-// c0's side: flux[1][F1] and forward shocks, over c0's upper neighbours in order
-GB_HD void f1_own(const Phys &ph, const Grid2 &G, int j, int i) {
-  if (j > G.NJ - 2 || i >= G.ntrack[j]) return;
-  const long long g0 = (long long)j * G.cap + i;
-  const int first = G.nbr[2 * G.NC + g0], cnt = G.nbr[3 * G.NC + g0];
-  double acc[NQ];
+// Interface s of track j's list: upper neighbour k of its owning cell.  Its
+// flux, shock tests and flags are kept for the cell pass (f1_gather).  One
+// interface per thread: a cell's upper list holds one to three of them, and a
+// thread per cell left the lanes of the shorter lists idle.
+GB_HD void f1_if(const Phys &ph, const Grid2 &G, int j, int s) {
+  const long long base = (long long)j * if_cap(G), sl = base + s;
+  const long long g0 = (long long)j * G.cap + G.if_own[sl];
+  const int k = s - G.if_off[g0];
+  F1Result r;
+  f1_interface(ph, G, j, g0, G.nbr[2 * G.NC + g0] + k, r);
+  const long long IS = (long long)G.NJ * if_cap(G);
 #pragma unroll
-  for (int q = 0; q < NQ; ++q) acc[q] = 0.;
-  double sd = G.sd[g0], ps = G.pspec[g0];
-  for (int k = 0; k < cnt; ++k) {
-    F1Result r;
-    f1_interface(ph, G, j, g0, first + k, r);
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) acc[q] += r.flux[q];
-    sd = fmax(sd, r.sd_fwd);
-    if (r.have_fwd && P_SPEC > ps) ps = P_SPEC;
-    if (k < KSEG && G.seg) {  // kept for the upper cell's gather
-      const long long sl = g0 * KSEG + k, SN = G.NC * KSEG;
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) G.seg[q * SN + sl] = r.flux[q];
-      G.seg[NQ * SN + sl] = r.sd_rev;
-      G.seg[(NQ + 1) * SN + sl] = (r.have_fwd ? 1. : 0.) + (r.have_rev ? 2. : 0.);
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) G.f1hi[q * G.NC + g0] = acc[q];
-  G.sd[g0] = sd;
-  G.pspec[g0] = ps;
+  for (int q = 0; q < NQ; ++q) G.ifs[q * IS + sl] = r.flux[q];
+  G.ifs[NQ * IS + sl] = r.sd_fwd;
+  G.ifs[(NQ + 1) * IS + sl] = r.sd_rev;
+  G.ifs[(NQ + 2) * IS + sl] = (r.have_fwd ? 1. : 0.) + (r.have_rev ? 2. : 0.);
 }
 
 // Foreign stale contributors: cells 0 and ntrack-1 whose (copied) upper list
@@ -535,31 +536,48 @@ GB_HD void stale_table(const Grid2 &G) {
   for (int j = 0; j <= G.NJ - 2; ++j) stale_append(G, j);
 }
 
-// cn's side: flux[0][F1] and reverse shocks, summed over the cells whose upper
-// list holds cn, in the reference's (j, i) order.
+// Cell cn after f1_if: its own side (flux[1][F1], forward shocks over its
+// upper list) and its other side (flux[0][F1] and reverse shocks, summed over
+// the cells whose upper list holds cn, in the reference's (j, i) order).
 GB_HD void f1_gather(const Phys &ph, const Grid2 &G, int t, int k) {
+  (void)ph;
   if (k >= G.ntrack[t]) return;
   const long long gn = (long long)t * G.cap + k;
+  const long long IC = if_cap(G), IS = (long long)G.NJ * IC;
+  double sd = G.sd[gn], ps = G.pspec[gn];
+  // the cell's own side: flux[1][F1] and the forward shock tests over its
+  // upper list, in order (tracks 0..NJ-2)
+  if (t <= G.NJ - 2) {
+    const int cnt = G.nbr[3 * G.NC + gn], off = G.if_off[gn];
+    const long long sl0 = (long long)t * IC + off;
+    double hi[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) hi[q] = 0.;
+    for (int m = 0; m < cnt && off + m < IC; ++m) {
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) hi[q] += G.ifs[q * IS + sl0 + m];
+      sd = fmax(sd, G.ifs[NQ * IS + sl0 + m]);
+      if (((int)G.ifs[(NQ + 2) * IS + sl0 + m] & 1) && P_SPEC > ps) ps = P_SPEC;
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) G.f1hi[q * G.NC + gn] = hi[q];
+  }
   double acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) acc[q] = 0.;
-  double sd = G.sd[gn], ps = G.pspec[gn];
   auto add = [&](int j, long long g0) {
     const int first = G.nbr[2 * G.NC + g0], cnt = G.nbr[3 * G.NC + g0];
     if (!(cnt > 0 && gn >= first && gn < (long long)first + cnt)) return;
+    const long long s = G.if_off[g0] + (gn - first);  // solved by f1_if
+    if (s >= IC) return;  // the interface table overflowed (status 41)
+    const long long sl = (long long)j * IC + s;
     F1Result r;
-    const long long k = gn - first;
-    if (k < KSEG && G.seg) {  // solved by the owning cell's pass
-      const long long sl = g0 * KSEG + k, SN = G.NC * KSEG;
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) r.flux[q] = G.seg[q * SN + sl];
-      r.sd_rev = G.seg[NQ * SN + sl];
-      const int fl = (int)G.seg[(NQ + 1) * SN + sl];
-      r.have_fwd = (fl & 1) != 0;
-      r.have_rev = (fl & 2) != 0;
-    } else {
-      f1_interface(ph, G, j, g0, gn, r);
-    }
+    for (int q = 0; q < NQ; ++q) r.flux[q] = G.ifs[q * IS + sl];
+    r.sd_rev = G.ifs[(NQ + 1) * IS + sl];
+    const int fl = (int)G.ifs[(NQ + 2) * IS + sl];
+    r.have_fwd = (fl & 1) != 0;
+    r.have_rev = (fl & 2) != 0;
 #pragma unroll
     for (int q = 0; q < NQ; ++q) acc[q] += r.flux[q];
     sd = fmax(sd, r.sd_rev);
