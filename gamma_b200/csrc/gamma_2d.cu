@@ -48,6 +48,11 @@ constexpr int kThreads = 256;
 #ifndef GB2_MINB_UP
 #define GB2_MINB_UP 4
 #endif
+// waves of resident blocks in the grid of a per-cell pass
+#ifndef GB2_PASS_WAVES
+#define GB2_PASS_WAVES 8
+#endif
+constexpr int kPassWaves = GB2_PASS_WAVES;
 
 struct Stats2 {
   unsigned long long c2p_calls, c2p_iters, c2p_fallbacks, c2p_max_iters, splits, merges, zone_updates;
@@ -418,6 +423,11 @@ struct gamma_2d {
   const float *guess = nullptr;  // learned cons2prim start (device parameters), or none
   int *d_flags = nullptr;  // [NJ] regrid flags
   Policy2 *d_policy = nullptr;  // the learned guess's choice (k_guess_policy2)
+  int nsm = 148;
+  // grid of each per-cell pass (set_pass_grids)
+  struct {
+    int mv, cellmv, tgrad, f1if, f1gather, dtpart, iface, update, update_guess;
+  } grid{};
   std::vector<double> tg;  // host copy of the per-track factors
   std::vector<double> theta, dtheta;  // of the active tracks, as given at creation
   std::string err;
@@ -464,12 +474,28 @@ Params2 params_of(const gamma_2d_params_t &q) {
 
 int blocks_of(long long n) { return (int)((n + kThreads - 1) / kThreads); }
 
-// fixed grid of the per-cell passes (they stride over the live cells)
-int cell_blocks(const gamma_2d *c) {
-  int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  return std::max(1, std::min(blocks_of(c->NC), nsm * 8));
+// Grid of a per-cell pass (they stride over the live cells): whole waves of
+// the kernel's resident blocks on every SM, so that no pass ends on a part
+// wave, and no more blocks than the cell capacity needs.  The cells a thread
+// takes change with the grid, the arithmetic of each cell does not.
+template <class K>
+int pass_blocks(const gamma_2d *c, K kernel, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return (int)std::max(1LL, std::min<long long>(blocks_of(c->NC), (long long)c->nsm * per_sm * kPassWaves));
+}
+
+void set_pass_grids(gamma_2d *c) {
+  c->grid.mv = pass_blocks(c, k_mv, 0);
+  c->grid.cellmv = pass_blocks(c, k_cellmv, 0);
+  c->grid.tgrad = pass_blocks(c, k_tgrad, 0);
+  c->grid.f1if = pass_blocks(c, k_f1if, 0);
+  c->grid.f1gather = pass_blocks(c, k_f1gather, 0);
+  c->grid.dtpart = pass_blocks(c, k_dtpart, 0);
+  c->grid.iface = pass_blocks(c, k_iface, 0);
+  c->grid.update = pass_blocks(c, k_update<false>, 0);
+  c->grid.update_guess = pass_blocks(c, k_update<true>, sizeof(mlp::InferSmem));
 }
 
 int ghost_blocks(const gamma_2d *c, bool reset) {
@@ -485,7 +511,6 @@ int enqueue_step_until(gamma_2d *c, int upto) {
   const Params2 P = params_of(c->par);
   const Grid2 &G = c->G;
   cudaStream_t s = c->stream;
-  const int nb = cell_blocks(c);
   if (c->guess) k_guess_policy2<<<1, 1, 0, s>>>(c->d_policy, c->d_stats);
   k_regrid_check<<<1, kThreads, 0, s>>>(P, G, c->d_flags, c->cfg.ngst);
   k_regrid<<<1, kThreads, 0, s>>>(ph, P, G, c->d_stats, c->d_flags, c->cfg.ngst, 1);
@@ -498,28 +523,28 @@ int enqueue_step_until(gamma_2d *c, int upto) {
     k_ghosts_copy<<<ghost_blocks(c, stage == 1), kThreads, 0, s>>>(G, stage == 1);
     k_ghost_cells<<<c->NJ, 32, 0, s>>>(G);
     k_prefix<<<1, 1024, 0, s>>>(G);
-    k_mv<<<nb, kThreads, 0, s>>>(ph, P, G);
-    k_cellmv<<<nb, kThreads, 0, s>>>(G);
+    k_mv<<<c->grid.mv, kThreads, 0, s>>>(ph, P, G);
+    k_cellmv<<<c->grid.cellmv, kThreads, 0, s>>>(G);
     k_stale_clear<<<(c->NJ + 255) / 256, 256, 0, s>>>(G);
     k_stale<<<(c->NJ + 127) / 128, 128, 0, s>>>(G);
-    k_tgrad<<<nb, kThreads, 0, s>>>(G);
+    k_tgrad<<<c->grid.tgrad, kThreads, 0, s>>>(G);
     k_if_scan<<<c->NJ - 1, kThreads, 0, s>>>(G);
     k_if_pref<<<1, 1024, 0, s>>>(G);
-    k_f1if<<<nb, kThreads, 0, s>>>(ph, G);
-    k_f1gather<<<nb, kThreads, 0, s>>>(ph, G);
+    k_f1if<<<c->grid.f1if, kThreads, 0, s>>>(ph, G);
+    k_f1gather<<<c->grid.f1gather, kThreads, 0, s>>>(ph, G);
     if (stage == upto) {
       G2_CUDA(c, cudaGetLastError());
       return GAMMA_OK;
     }
     if (stage == 1) {
-      k_dtpart<<<nb, kThreads, 0, s>>>(G);
-      k_dtfinal<<<1, kThreads, 0, s>>>(G, nb, c->cfg.cfl);
+      k_dtpart<<<c->grid.dtpart, kThreads, 0, s>>>(G);
+      k_dtfinal<<<1, kThreads, 0, s>>>(G, c->grid.dtpart, c->cfg.cfl);
     }
-    k_iface<<<nb, kThreads, 0, s>>>(G, stage);
+    k_iface<<<c->grid.iface, kThreads, 0, s>>>(G, stage);
     Policy2 *pol = c->guess ? c->d_policy : nullptr;
-    k_update<false><<<nb, kThreads, 0, s>>>(ph, P, G, stage, c->d_stats, nullptr, pol);
+    k_update<false><<<c->grid.update, kThreads, 0, s>>>(ph, P, G, stage, c->d_stats, nullptr, pol);
     if (c->guess)
-      k_update<true><<<nb, kThreads, sizeof(mlp::InferSmem), s>>>(ph, P, G, stage, c->d_stats, c->guess, pol);
+      k_update<true><<<c->grid.update_guess, kThreads, sizeof(mlp::InferSmem), s>>>(ph, P, G, stage, c->d_stats, c->guess, pol);
   }
   k_advance<<<1, 32, 0, s>>>(G, c->d_stats);
   G2_CUDA(c, cudaGetLastError());
@@ -558,6 +583,8 @@ GAMMA_API int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta,
   c->NJ = cfg->ntheta + 2 * ng;
   c->cap = cfg->nmax + 2 * ng;
   c->NC = (long long)c->NJ * c->cap;
+  c->nsm = prop.multiProcessorCount;
+  set_pass_grids(c);
   const long long NC = c->NC;
   // per-track angular factors; ghost tracks as updateGhosts shifts them
   // (2d.cpp:259-287: by the first active track's dtheta below, the last's above)
