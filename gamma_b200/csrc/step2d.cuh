@@ -344,25 +344,39 @@ GB_HD void overlap(const Grid2 &G, long long g0, long long gn, double *xm, doubl
   *w = fmax(0., fmin(xR0, xRn) - fmax(xL0, xLn));
 }
 
-// The gradient towards neighbour gn, (qR - qL) / dcen, of every slot.
-GB_HD void neighbour_grad(const Grid2 &G, long long gn, double xm, double cr0, double ct0, const double *p0,
-                          const double *m0, double *grad) {
-  const int jn = track_of(G, gn);
-  const double dxmL = xm - cr0;
-  const double dxmR = xm - cen_r(G.x[gn], G.dx[gn]);
-  const double dcen = tgeo(G, jn).cen_t - ct0;
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    const double qL = p0[q] + m0[q] * dxmL;
-    const double qR = G.prim[q * G.NC + gn] + G.gmv[q * G.NC + gn] * dxmR;
-    grad[q] = qdiv(qR - qL, dcen);
-  }
+// Geometry of the gradient towards neighbour gn, the same for every slot:
+// the offsets of the overlap's centre from both cell centres, the theta
+// distance, and the overlap's area.
+struct NbrGeo {
+  double dxmL, dxmR, dcen, dA;
+};
+
+GB_HD NbrGeo neighbour_geo(const Grid2 &G, long long g0, long long gn, double cr0, double ct0, double s) {
+  double xm, w;
+  overlap(G, g0, gn, &xm, &w);
+  NbrGeo n;
+  n.dxmL = xm - cr0;
+  n.dxmR = xm - cen_r(G.x[gn], G.dx[gn]);
+  n.dcen = tgeo(G, track_of(G, gn)).cen_t - ct0;
+  n.dA = dA_t(xm, w, s);
+  return n;
+}
+
+// The gradient of slot q towards neighbour gn, (qR - qL) / dcen.
+GB_HD double neighbour_grad(const Grid2 &G, int q, long long gn, const NbrGeo &n, double p0, double m0) {
+  const double qL = p0 + m0 * n.dxmL;
+  const double qR = G.prim[q * G.NC + gn] + G.gmv[q * G.NC + gn] * n.dxmR;
+  return qdiv(qR - qL, n.dcen);
 }
 
 // Pass 1 forms the dA-weighted average; pass 2 folds in minmod with each
 // neighbour's gradient in the reference's order (an order-dependent chain:
-// minmod(x, x) = 0).  The first KGRAD gradients of pass 1 are kept for pass 2.
-constexpr int KGRAD = 4;
+// minmod(x, x) = 0).  Every slot's chain uses its own gradients only, so the
+// slots run one after another over geometry formed once: the first KGEO
+// neighbours' geometry and one slot's gradients stay in registers, and
+// neighbours past KGEO recompute theirs for each slot.  Per slot the
+// operations and their order are those of the reference's loops.
+constexpr int KGEO = 4;
 
 GB_HD void trans_grad(const Grid2 &G, int j, int i) {
   const int n = G.ntrack[j];
@@ -376,56 +390,48 @@ GB_HD void trans_grad(const Grid2 &G, int j, int i) {
   const double cr0 = cen_r(G.x[g0], G.dx[g0]);
   const TrackGeo t0 = tgeo(G, j);
   const double ct0 = t0.cen_t;
-  double p0[NQ], m0[NQ], avg[NQ], grad[NQ], kept[KGRAD][NQ];
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    p0[q] = G.prim[q * G.NC + g0];
-    m0[q] = G.gmv[q * G.NC + g0];
-    avg[q] = 0.;
-  }
   const int f0 = G.nbr[0 * G.NC + g0], c0 = G.nbr[1 * G.NC + g0];
   const int f1 = G.nbr[2 * G.NC + g0], c1 = G.nbr[3 * G.NC + g0];
+  const int nn = c0 + c1;
+  // neighbour kn: the lower list's cells, then the upper list's; the theta of
+  // the interface is th - dth/2 below and th (unmoved) above
+#define TG_NBR(kn) ((kn) < c0 ? (long long)f0 + (kn) : (long long)f1 + ((kn) - c0))
+#define TG_S(kn) ((kn) < c0 ? t0.s_lo : t0.s_mid)
+  NbrGeo geo[KGEO];
   double dAtot = 0.;
-  int kn = 0;
-  for (int d = 0; d < 2; ++d) {
-    const int first = d == 0 ? f0 : f1, cnt = d == 0 ? c0 : c1;
-    for (int k = 0; k < cnt; ++k, ++kn) {
-      const long long gn = first + k;
-      double xm, w;
-      overlap(G, g0, gn, &xm, &w);
-      // theta of the interface: th - dth/2 below, th (unmoved) above
-      const double dA = dA_t(xm, w, d == 0 ? t0.s_lo : t0.s_mid);
-      dAtot += dA;
-      neighbour_grad(G, gn, xm, cr0, ct0, p0, m0, grad);
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) avg[q] += grad[q] * dA;
-      if (kn < KGRAD) {
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) kept[kn][q] = grad[q];
-      }
+  for (int kn = 0; kn < KGEO; ++kn)
+    if (kn < nn) {
+      geo[kn] = neighbour_geo(G, g0, TG_NBR(kn), cr0, ct0, TG_S(kn));
+      dAtot += geo[kn].dA;
     }
-  }
+  for (int kn = KGEO; kn < nn; ++kn) dAtot += neighbour_geo(G, g0, TG_NBR(kn), cr0, ct0, TG_S(kn)).dA;
+#pragma unroll 1
+  for (int q = 0; q < NQ; ++q) {
+    const double p0 = G.prim[q * G.NC + g0], m0 = G.gmv[q * G.NC + g0];
+    double avg = 0., kept[KGEO];
 #pragma unroll
-  for (int q = 0; q < NQ; ++q) avg[q] = qdiv(avg[q], dAtot);
-  kn = 0;
-  for (int d = 0; d < 2; ++d) {
-    const int first = d == 0 ? f0 : f1, cnt = d == 0 ? c0 : c1;
-    for (int k = 0; k < cnt; ++k, ++kn) {
-      if (kn < KGRAD) {
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) avg[q] = minmod(avg[q], kept[kn][q]);
-      } else {
-        const long long gn = first + k;
-        double xm, w;
-        overlap(G, g0, gn, &xm, &w);
-        neighbour_grad(G, gn, xm, cr0, ct0, p0, m0, grad);
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) avg[q] = minmod(avg[q], grad[q]);
+    for (int kn = 0; kn < KGEO; ++kn)
+      if (kn < nn) {
+        kept[kn] = neighbour_grad(G, q, TG_NBR(kn), geo[kn], p0, m0);
+        avg += kept[kn] * geo[kn].dA;
       }
+    for (int kn = KGEO; kn < nn; ++kn) {
+      const NbrGeo e = neighbour_geo(G, g0, TG_NBR(kn), cr0, ct0, TG_S(kn));
+      avg += neighbour_grad(G, q, TG_NBR(kn), e, p0, m0) * e.dA;
     }
-  }
+    avg = qdiv(avg, dAtot);
 #pragma unroll
-  for (int q = 0; q < NQ; ++q) G.gf1n[q * G.NC + g0] = avg[q];
+    for (int kn = 0; kn < KGEO; ++kn)
+      if (kn < nn) avg = minmod(avg, kept[kn]);
+    for (int kn = KGEO; kn < nn; ++kn) {
+      const NbrGeo e = neighbour_geo(G, g0, TG_NBR(kn), cr0, ct0, TG_S(kn));
+      avg = minmod(avg, neighbour_grad(G, q, TG_NBR(kn), e, p0, m0));
+    }
+    G.gf1n[q * G.NC + g0] = avg;
+  }
+#undef TG_NBR
+#undef TG_S
 }
 
 // ---------------------------------------------------------------------------
