@@ -28,19 +28,17 @@ namespace {
 constexpr int kThreads = 256;
 // resident blocks per SM asked of the heavy per-cell passes: their FP64 and
 // load latency needs warps more than registers (measured per pass at 512
-// tracks: 3 for the r interfaces and the transverse gradients, 4 for the
-// theta gather and the cell update, 2 for the theta interfaces)
-#ifndef GB2_MINB
-#define GB2_MINB 2
-#endif
+// tracks with grids of whole waves: 3 for the theta interfaces and the
+// transverse gradients, 4 for the r interfaces, the theta gather and the cell
+// update)
 #ifndef GB2_MINB_MV
-#define GB2_MINB_MV 3
+#define GB2_MINB_MV 4
 #endif
 #ifndef GB2_MINB_TG
 #define GB2_MINB_TG 3
 #endif
 #ifndef GB2_MINB_F1
-#define GB2_MINB_F1 GB2_MINB
+#define GB2_MINB_F1 3
 #endif
 #ifndef GB2_MINB_GA
 #define GB2_MINB_GA 4
@@ -479,11 +477,11 @@ int blocks_of(long long n) { return (int)((n + kThreads - 1) / kThreads); }
 // wave, and no more blocks than the cell capacity needs.  The cells a thread
 // takes change with the grid, the arithmetic of each cell does not.
 template <class K>
-int pass_blocks(const gamma_2d *c, K kernel, size_t smem) {
+int pass_blocks(const gamma_2d *c, K kernel, size_t smem, int waves = kPassWaves) {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
-  return (int)std::max(1LL, std::min<long long>(blocks_of(c->NC), (long long)c->nsm * per_sm * kPassWaves));
+  return (int)std::max(1LL, std::min<long long>(blocks_of(c->NC), (long long)c->nsm * per_sm * waves));
 }
 
 void set_pass_grids(gamma_2d *c) {
@@ -492,7 +490,9 @@ void set_pass_grids(gamma_2d *c) {
   c->grid.tgrad = pass_blocks(c, k_tgrad, 0);
   c->grid.f1if = pass_blocks(c, k_f1if, 0);
   c->grid.f1gather = pass_blocks(c, k_f1gather, 0);
-  c->grid.dtpart = pass_blocks(c, k_dtpart, 0);
+  // one wave: every block ends in a block reduction, and k_dtfinal reads
+  // one partial per block
+  c->grid.dtpart = pass_blocks(c, k_dtpart, 0, 1);
   c->grid.iface = pass_blocks(c, k_iface, 0);
   c->grid.update = pass_blocks(c, k_update<false>, 0);
   c->grid.update_guess = pass_blocks(c, k_update<true>, sizeof(mlp::InferSmem));
