@@ -301,7 +301,11 @@ GB_HD void neighbour_list(const Grid2 &G, int j, int i, int jn, int *first, int 
   }
   const int b = (X[s] > xjL && s > 0) ? s - 1 : s;
   if (X[b] < xjR) {
-    int e = lower_bound(X, np - 1, xjR) - 1;
+    // LB(xjR) - 1: with X[b] < xjR and X sorted, LB(xjR) > b, so a scan from
+    // b + 1 finds it in (list length + 1) loads
+    int e = b + 1;
+    while (e < np - 1 && X[e] < xjR) ++e;
+    --e;
     if (e > np - 2) e = np - 2;
     *first = jn * G.cap + b + 1;
     *count = e - b + 1;
