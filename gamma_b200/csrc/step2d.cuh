@@ -277,14 +277,41 @@ GB_HD void mv_interface(const Phys &ph, const Params2 &P, const Grid2 &G, int j,
 // i is min(LB(x_{i-1} + dx_{i-1}/2), n'-2) (LB: first interface >= the value),
 // which gives every list without the scan.
 
-GB_HD int lower_bound(const double *X, int n, double v) {  // first k in [0, n) with X[k] >= v, or n
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (X[mid] < v) lo = mid + 1;
+// The first k in [lo0, hi0) where pred(k) is false, or hi0, for a pred that
+// is true up to some k and false after it: searched outwards from the hint h
+// (clamped into the range) in steps 1, 2, 4, ..., then by bisection.  Any h
+// gives the binary search's k; a hint within d of k takes about 2 log2(d)
+// tests instead of log2(hi0 - lo0).
+template <class Pred>
+GB_HD int partition_from(int lo0, int hi0, long long h, Pred pred) {
+  if (hi0 <= lo0) return lo0;
+  const int c = (int)(h < lo0 ? lo0 : (h >= hi0 ? hi0 - 1 : h));
+  int lo, hi;  // pred(lo) true or lo = lo0 - 1; pred(hi) false or hi = hi0
+  if (pred(c)) {
+    lo = c;
+    int step = 1;
+    hi = c + 1;
+    while (hi < hi0 && pred(hi)) {
+      lo = hi;
+      step <<= 1;
+      hi = (hi0 - lo > step) ? lo + step : hi0;
+    }
+  } else {
+    hi = c;
+    int step = 1;
+    lo = c - 1;
+    while (lo >= lo0 && !pred(lo)) {
+      hi = lo;
+      step <<= 1;
+      lo = (hi - lo0 >= step) ? hi - step : lo0 - 1;
+    }
+  }
+  while (hi - lo > 1) {
+    const int mid = lo + ((hi - lo) >> 1);
+    if (pred(mid)) lo = mid;
     else hi = mid;
   }
-  return lo;
+  return hi;
 }
 
 GB_HD void neighbour_list(const Grid2 &G, int j, int i, int jn, int *first, int *count) {
@@ -295,8 +322,11 @@ GB_HD void neighbour_list(const Grid2 &G, int j, int i, int jn, int *first, int 
   const double xjR = G.x[g] + G.dx[g] / 2.;
   int s = 0;
   if (i > 1) {
+    // LB(xpR), from the start of this list in the previous stage (nbr still
+    // holds it; a regrid or an upload only makes the hint worse)
     const double xpR = G.x[g - 1] + G.dx[g - 1] / 2.;
-    s = lower_bound(X, np - 1, xpR);
+    const long long hint = (long long)G.nbr[(jn < j ? 0 : 2) * G.NC + g] - (long long)jn * G.cap;
+    s = partition_from(0, np - 1, hint, [&](int k) { return X[k] < xpR; });
     if (s > np - 2) s = np - 2;
   }
   const int b = (X[s] > xjL && s > 0) ? s - 1 : s;
@@ -620,17 +650,10 @@ GB_HD void f1_gather(const Phys &ph, const Grid2 &G, int t, int k) {
     add(j, o);  // cell 0 (its list may be stale)
     // fresh lists of cells 1..n-2: starts are non-decreasing, so the cells
     // holding gn end at the last start <= gn and form a run downwards
-    int lo = 1, hi = n - 2;  // last i in [1, n-2] with first_i <= gn
-    int last = 0;
-    while (lo <= hi) {
-      const int mid = (lo + hi) >> 1;
-      if (G.nbr[2 * G.NC + o + mid] <= gn) {
-        last = mid;
-        lo = mid + 1;
-      } else {
-        hi = mid - 1;
-      }
-    }
+    // last i in [1, n-2] with first_i <= gn, or 0; searched from the end of
+    // gn's own list into track t-1 (the cells it overlaps)
+    const long long hint = (long long)G.nbr[0 * G.NC + gn] + G.nbr[1 * G.NC + gn] - o;
+    const int last = partition_from(1, n - 1, hint, [&](int k) { return G.nbr[2 * G.NC + o + k] <= gn; }) - 1;
     // (list ends are non-decreasing too; empty lists only occur at the start)
     int begin = last;
     while (begin >= 1) {
