@@ -212,8 +212,8 @@ def run_reference_arm(args):
 
 
 # kernel launches of one 2D step (gamma_2d.cu enqueue_step_until): 4 regrid,
-# 14 per RK3 stage, collect_dt's 2 in stage 1, the advance
-LAUNCHES_2D = 4 + 3 * 14 + 2 + 1
+# 16 per RK3 stage, collect_dt's 2 in stage 1, the advance
+LAUNCHES_2D = 4 + 3 * 16 + 2 + 1
 JET2D = dict(ntheta=512, ncell=12000, nmax=12000)  # tracks settle at ~3,000-4,000 cells after the first regrid
 # the sweep workload's large 2D case: slow cells merge only below 0.3 of the
 # target spacing, so the tracks keep ~8,000 cells (~33 M zones)

@@ -192,15 +192,38 @@ __global__ void k_prefix(Grid2 G) {
   if (t == nt - 1) G.pref[G.NJ] = part[t];
 }
 
-__device__ __forceinline__ void cell_at(const Grid2 &G, long long g, int *j, int *i) {
-  int lo = 0, hi = G.NJ - 1;  // last track with pref[track] <= g
+// the last track j in [0, NJ-1] with pref[j] <= g (pref: a prefix over tracks)
+__device__ __forceinline__ int track_at(const int *pref, int NJ, long long g) {
+  int lo = 0, hi = NJ - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (G.pref[mid] <= g) lo = mid;
+    if (pref[mid] <= g) lo = mid;
     else hi = mid - 1;
   }
-  *j = lo;
-  *i = (int)(g - G.pref[lo]);
+  return lo;
+}
+
+// track_at of every 32nd element (live cell, theta interface), after the
+// prefix is formed: an element's track is then at most a few steps past its
+// group's (one step per track that starts inside the group)
+__global__ void k_group_tracks(const int *pref, int NJ, int *grp) {
+  const long long n = pref[NJ];
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; 32 * k < n; k += (long long)gridDim.x * blockDim.x)
+    grp[k] = track_at(pref, NJ, 32 * k);
+}
+
+// track_at(pref, NJ, g) from the group table
+__device__ __forceinline__ int track_from(const int *pref, const int *grp, int NJ, long long g) {
+  int t = grp[g >> 5];
+  while (t < NJ - 1 && pref[t + 1] <= g) ++t;
+  return t;
+}
+
+// (track, index) of live cell g
+__device__ __forceinline__ void cell_at(const Grid2 &G, long long g, int *j, int *i) {
+  const int t = track_from(G.pref, G.gtrk, G.NJ, g);
+  *j = t;
+  *i = (int)(g - G.pref[t]);
 }
 
 #define FOR_LIVE_CELLS(G, j, i)                                                                     \
@@ -296,13 +319,8 @@ __global__ void __launch_bounds__(kThreads, GB2_MINB_F1) k_f1if(Phys ph, Grid2 G
   const long long n = G.if_pref[G.NJ];
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
-    int lo = 0, hi = G.NJ - 1;  // last track with if_pref[track] <= t
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (G.if_pref[mid] <= t) lo = mid;
-      else hi = mid - 1;
-    }
-    f1_if(ph, G, lo, (int)(t - G.if_pref[lo]));
+    const int j = track_from(G.if_pref, G.iftrk, G.NJ, t);
+    f1_if(ph, G, j, (int)(t - G.if_pref[j]));
   }
 }
 
@@ -424,7 +442,7 @@ struct gamma_2d {
   int nsm = 148;
   // grid of each per-cell pass (set_pass_grids)
   struct {
-    int mv, cellmv, tgrad, f1if, f1gather, dtpart, iface, update, update_guess;
+    int mv, cellmv, tgrad, f1if, f1gather, dtpart, iface, update, update_guess, groups, if_groups;
   } grid{};
   std::vector<double> tg;  // host copy of the per-track factors
   std::vector<double> theta, dtheta;  // of the active tracks, as given at creation
@@ -484,6 +502,10 @@ int pass_blocks(const gamma_2d *c, K kernel, size_t smem, int waves = kPassWaves
   return (int)std::max(1LL, std::min<long long>(blocks_of(c->NC), (long long)c->nsm * per_sm * waves));
 }
 
+// entries of the theta interfaces' group table: the interfaces are at most
+// if_cap per owning track (status 41 past that)
+long long if_groups(const gamma_2d *c) { return ((long long)(c->NJ - 1) * (2LL * c->cap + 64)) / 32 + 2; }
+
 void set_pass_grids(gamma_2d *c) {
   c->grid.mv = pass_blocks(c, k_mv, 0);
   c->grid.cellmv = pass_blocks(c, k_cellmv, 0);
@@ -496,6 +518,8 @@ void set_pass_grids(gamma_2d *c) {
   c->grid.iface = pass_blocks(c, k_iface, 0);
   c->grid.update = pass_blocks(c, k_update<false>, 0);
   c->grid.update_guess = pass_blocks(c, k_update<true>, sizeof(mlp::InferSmem));
+  c->grid.groups = std::max(1, std::min(blocks_of(c->NC / 32 + 1), c->nsm * 8));
+  c->grid.if_groups = std::max(1, std::min(blocks_of(if_groups(c)), c->nsm * 8));
 }
 
 int ghost_blocks(const gamma_2d *c, bool reset) {
@@ -523,6 +547,7 @@ int enqueue_step_until(gamma_2d *c, int upto) {
     k_ghosts_copy<<<ghost_blocks(c, stage == 1), kThreads, 0, s>>>(G, stage == 1);
     k_ghost_cells<<<c->NJ, 32, 0, s>>>(G);
     k_prefix<<<1, 1024, 0, s>>>(G);
+    k_group_tracks<<<c->grid.groups, kThreads, 0, s>>>(G.pref, G.NJ, G.gtrk);
     k_mv<<<c->grid.mv, kThreads, 0, s>>>(ph, P, G);
     k_cellmv<<<c->grid.cellmv, kThreads, 0, s>>>(G);
     k_stale_clear<<<(c->NJ + 255) / 256, 256, 0, s>>>(G);
@@ -530,6 +555,7 @@ int enqueue_step_until(gamma_2d *c, int upto) {
     k_tgrad<<<c->grid.tgrad, kThreads, 0, s>>>(G);
     k_if_scan<<<c->NJ - 1, kThreads, 0, s>>>(G);
     k_if_pref<<<1, 1024, 0, s>>>(G);
+    k_group_tracks<<<c->grid.if_groups, kThreads, 0, s>>>(G.if_pref, G.NJ, G.iftrk);
     k_f1if<<<c->grid.f1if, kThreads, 0, s>>>(ph, G);
     k_f1gather<<<c->grid.f1gather, kThreads, 0, s>>>(ph, G);
     if (stage == upto) {
@@ -666,12 +692,14 @@ GAMMA_API int gamma_2d_create(const gamma_2d_config_t *cfg, const double *theta,
   G2_ALLOC(G.status, sizeof(int));
   G2_ALLOC(G.red, (size_t)blocks_of(NC) * d);
   G2_ALLOC(G.pref, ((size_t)c->NJ + 1) * sizeof(int));
+  G2_ALLOC(G.gtrk, ((size_t)NC / 32 + 2) * sizeof(int));
   const size_t IS = (size_t)c->NJ * (size_t)if_cap(G);
   G2_ALLOC(G.ifs, (size_t)IF_WORDS * IS * d);
   G2_ALLOC(G.if_off, NC * sizeof(int));
   G2_ALLOC(G.if_own, IS * sizeof(int));
   G2_ALLOC(G.if_tot, c->NJ * sizeof(int));
   G2_ALLOC(G.if_pref, ((size_t)c->NJ + 1) * sizeof(int));
+  G2_ALLOC(G.iftrk, (size_t)if_groups(c) * sizeof(int));
   G2_ALLOC(G.rprim, q * NC * d);
   G2_ALLOC(G.rgmv, q * NC * d);
   G2_ALLOC(G.rgf1, q * NC * d);

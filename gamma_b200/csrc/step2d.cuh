@@ -78,6 +78,7 @@ struct Grid2 {
                              // 41: a track's theta interfaces exceed if_cap
   double *red;               // partial minima of dt_loc
   int *pref;                 // [NJ+1] cells of tracks before j (the live-cell index)
+  int *gtrk;                 // [NC/32+2] track of live cell 32k (k_group_tracks)
   // theta interfaces, owned by the cells of track j (j <= NJ-2) through their
   // upper lists, numbered per track in cell order (k_if_scan):
   double *ifs;               // [IF_WORDS][NJ * if_cap]: interface results, track j from j * if_cap
@@ -85,6 +86,7 @@ struct Grid2 {
   int *if_own;               // [NJ * if_cap]: the owning cell (index in its track) of each interface
   int *if_tot;               // [NJ]: interfaces of each track
   int *if_pref;              // [NJ+1]: interfaces of the tracks before j
+  int *iftrk;                // [(NJ-1) if_cap/32 + 2] track of interface 32k (k_if_group_tracks)
   // regrid scratch (one track of records per track)
   double *rprim, *rgmv, *rgf1;  // [NQ][NC]
   double *rx, *rdx, *rdtl, *rxI;
