@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "physics.cuh"
+#include "search.cuh"
 
 namespace {
 
@@ -62,6 +63,38 @@ __attribute__((visibility("default"))) int gb_selftest_pow_3_4(const double *x, 
   if (e == cudaSuccess) e = cudaMemcpy(libm, d + 2 * (size_t)n, b, cudaMemcpyDeviceToHost);
   cudaFree(d);
   return (int)e;
+}
+
+// gb::d2::partition_from (the 2D passes' searches from a hint) against a
+// linear scan, on the host: `cases` random sorted arrays with ties, keys in
+// and around their range, hints in range and far outside it.  Returns the
+// number of wrong results, or -1 if a probe left [lo0, hi0).
+__attribute__((visibility("default"))) int gb_selftest_partition_from(unsigned seed, int cases) {
+  unsigned long long r = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+  auto next = [&r](unsigned m) {  // LCG, high bits
+    r = r * 6364136223846793005ULL + 1442695040888963407ULL;
+    return (unsigned)((r >> 33) % m);
+  };
+  double X[64];
+  int bad = 0;
+  for (int t = 0; t < cases; ++t) {
+    const int n = (int)next(41), lo0 = (int)next(3), hi0 = lo0 + n;
+    double v = 0.;
+    for (int k = 0; k < hi0 + 2; ++k) X[k] = (v += next(3));
+    const double key = next((unsigned)v + 3);
+    const long long h = next(5) == 0 ? (long long)next(2000001) - 1000000 : lo0 + (long long)next(n + 3) - 1;
+    bool out = false;
+    auto pred = [&](int k) {
+      if (k < lo0 || k >= hi0) out = true;
+      return k >= lo0 && k < hi0 && X[k] < key;
+    };
+    int ref = lo0;
+    while (ref < hi0 && X[ref] < key) ++ref;
+    const int got = gb::d2::partition_from(lo0, hi0, h, pred);
+    if (out) return -1;
+    if (got != ref) ++bad;
+  }
+  return bad;
 }
 
 }  // extern "C"
